@@ -1,0 +1,73 @@
+"""Loader of the engine's CUDA library (fractura_b200/lib/libapeiron_b200.so).
+
+The library is the only compute path.  If it is missing or cannot be loaded,
+every entry point raises ``EngineUnavailable``; nothing falls back to the CPU.
+"""
+import ctypes as C
+import os
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libapeiron_b200.so")
+
+EXPORTS = (
+    "ap_abi_version", "ap_last_error", "ap_render_pass", "ap_resolve_hist_pass",
+    "ap_edge_detect", "ap_histogram_cdf", "ap_colour", "ap_build_bla", "ap_fma_peak_launch",
+)
+
+
+class EngineUnavailable(RuntimeError):
+    """The CUDA engine library is not built or cannot be loaded."""
+
+
+class EngineError(RuntimeError):
+    """A C-ABI call returned an error code."""
+
+
+_lib = None
+
+
+def load():
+    """Load and type the library (once)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise EngineUnavailable(
+            f"{LIB_PATH} is missing; build it with `python -m fractura_b200.build`")
+    try:
+        L = C.CDLL(LIB_PATH)
+    except OSError as e:
+        raise EngineUnavailable(f"cannot load {LIB_PATH}: {e}") from e
+    P = C.POINTER(abi.ApFrameParams)
+    B = C.POINTER(abi.ApFrameBuffers)
+    vp, i32, f32, f64 = C.c_void_p, C.c_int32, C.c_float, C.c_double
+    L.ap_abi_version.restype = C.c_int
+    L.ap_last_error.restype = C.c_char_p
+    L.ap_render_pass.argtypes = [P, B, vp]
+    L.ap_resolve_hist_pass.argtypes = [P, B, vp]
+    L.ap_colour.argtypes = [P, B, vp]
+    L.ap_edge_detect.argtypes = [vp, vp, i32, i32, f32, vp]
+    L.ap_histogram_cdf.argtypes = [vp, i32, i32, i32, i32, vp, vp, vp]
+    L.ap_build_bla.argtypes = [vp, vp, i32, i32, f64, i32, i32, f64, f64, vp, vp]
+    L.ap_fma_peak_launch.argtypes = [i32, i32, i32, vp, C.POINTER(C.c_double), vp]
+    for name in EXPORTS:
+        fn = getattr(L, name)
+        if fn.restype is None or fn.restype is C.c_int:
+            fn.restype = C.c_int
+    if L.ap_abi_version() != abi.AP_ABI_VERSION:
+        raise EngineUnavailable(
+            f"library ABI {L.ap_abi_version()} != expected {abi.AP_ABI_VERSION}")
+    _lib = L
+    return L
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = load().ap_last_error().decode(errors="replace")
+        raise EngineError(f"{what} failed ({rc}): {msg}")
+
+
+def last_error():
+    return load().ap_last_error().decode(errors="replace")

@@ -1,0 +1,163 @@
+// ap_colour.cu -- edge mask, histogram -> CDF, and colouring passes.
+#include "ap_common.cuh"
+
+namespace ap {
+
+// ------------------------------------------------------------------ edges
+// math_core/cuda_kernels.py:1587-1611: a pixel is an edge when any of its
+// 8 neighbours differs in interior-ness or by more than the threshold
+// (float32 difference against the float32 threshold).
+__global__ void __launch_bounds__(256) edge_kernel(const float* __restrict__ it,
+                                                   uint8_t* __restrict__ edge, int W, int H,
+                                                   float thr) {
+    const int i = blockIdx.x * 16 + (threadIdx.x & 15);
+    const int j = blockIdx.y * 16 + (threadIdx.x >> 4);
+    if (i >= W || j >= H) return;
+    const float s = it[(size_t)j * W + i];
+    bool e = false;
+    for (int dj = -1; dj <= 1 && !e; ++dj) {
+        const int nj = j + dj;
+        if (nj < 0 || nj >= H) continue;
+        for (int di = -1; di <= 1; ++di) {
+            const int ni = i + di;
+            if (ni < 0 || ni >= W || (di == 0 && dj == 0)) continue;
+            const float sn = it[(size_t)nj * W + ni];
+            if ((s < 0.0f) != (sn < 0.0f) || (s >= 0.0f && fabsf(__fsub_rn(s, sn)) > thr)) {
+                e = true;
+                break;
+            }
+        }
+    }
+    edge[(size_t)j * W + i] = e ? 1 : 0;
+}
+
+// -------------------------------------------------------------- histogram
+// math_core/cuda_kernels.py:1999-2013: bin = int(s / max(1, max_iter) * (bins - 1)).
+__global__ void __launch_bounds__(256) histogram_kernel(const float* __restrict__ it, size_t n,
+                                                        double inv_max, int num_bins,
+                                                        int* __restrict__ hist) {
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
+         q += (size_t)gridDim.x * blockDim.x) {
+        const float s = it[q];
+        if (s >= 0.0f) {
+            const double pos = ((double)s * inv_max) * (double)(num_bins - 1);
+            int bin = (int)pos;
+            if (bin >= num_bins) bin = num_bins - 1;
+            else if (bin < 0) bin = 0;
+            atomicAdd(hist + bin, 1);
+        }
+    }
+}
+
+// One block of 1024 threads: inclusive prefix sum of the histogram in exact
+// integer arithmetic, then cdf[b] = float32(prefix[b] / total) as the
+// float64 scan of math_core/cuda_kernels.py:1929-1996 produces it.
+constexpr int kScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads) cdf_kernel(const int* __restrict__ hist,
+                                                           int num_bins, float* __restrict__ cdf) {
+    __shared__ long long warp_sums[kScanThreads / 32];
+    __shared__ long long total_s;
+    const int t = threadIdx.x;
+    const int chunk = (num_bins + kScanThreads - 1) / kScanThreads;
+    const int b0 = t * chunk;
+    const int b1 = min(b0 + chunk, num_bins);
+    long long local = 0;
+    for (int q = b0; q < b1; ++q) local += hist[q];
+
+    // Block-wide exclusive scan of the per-thread sums.
+    const int lane = t & 31, warp = t >> 5;
+    long long v = local;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) warp_sums[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        long long w = warp_sums[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long u = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += u;
+        }
+        warp_sums[lane] = w;
+        if (lane == 31) total_s = w;
+    }
+    __syncthreads();
+    long long run = (v - local) + (warp > 0 ? warp_sums[warp - 1] : 0LL);
+    const double total = (double)total_s;
+    for (int q = b0; q < b1; ++q) {
+        run += hist[q];
+        cdf[q] = total > 0.0 ? (float)((double)run / total)
+                             : (float)((double)q / (double)(num_bins - 1));
+    }
+}
+
+// ----------------------------------------------------------------- colour
+// apply_histogram_equalization_kernel (math_core/cuda_kernels.py:2016) and
+// recolor_iter_map_cuda_kernel (math_core/cuda_kernels.py:3201).
+__global__ void __launch_bounds__(256) colour_kernel(const ApFrameParams p, const ApFrameBuffers b,
+                                                     int hist) {
+    const int i = blockIdx.x * 16 + (threadIdx.x & 15);
+    const int j = blockIdx.y * 16 + (threadIdx.x >> 4);
+    if (i >= p.width || j >= p.height) return;
+    const size_t idx = (size_t)j * p.width + i;
+    const double s = (double)b.iter_map[idx];
+    double r = 0.0, g = 0.0, bb = 0.0;
+    if (s >= 0.0) colour_of(p, b.lut, b.cdf, hist != 0, s, r, g, bb);
+    store_rgb(b.rgb, p.is_hdr, idx, r, g, bb);
+}
+
+}  // namespace ap
+
+extern "C" int ap_edge_detect(const float* iter_map, uint8_t* edge_mask, int32_t width,
+                              int32_t height, float threshold, void* stream) {
+    if (!iter_map || !edge_mask || width <= 0 || height <= 0) {
+        ap::set_error("ap_edge_detect: bad arguments");
+        return AP_E_INVALID;
+    }
+    dim3 grid((width + 15) / 16, (height + 15) / 16);
+    ap::edge_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(iter_map, edge_mask, width,
+                                                                        height, threshold);
+    return ap::check_launch("edge_kernel");
+}
+
+extern "C" int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height,
+                                int32_t max_iter, int32_t num_bins, int32_t* hist, float* cdf,
+                                void* stream) {
+    if (!iter_map || !hist || !cdf || width <= 0 || height <= 0 || num_bins < 2 ||
+        num_bins > (1 << 24)) {
+        ap::set_error("ap_histogram_cdf: bad arguments");
+        return AP_E_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)num_bins, st);
+    if (e != cudaSuccess) {
+        ap::set_error("ap_histogram_cdf: memset: %s", cudaGetErrorString(e));
+        return AP_E_CUDA;
+    }
+    const size_t n = (size_t)width * height;
+    const double inv_max = 1.0 / fmax(1.0, (double)max_iter);
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    ap::histogram_kernel<<<blocks, 256, 0, st>>>(iter_map, n, inv_max, num_bins, hist);
+    int rc = ap::check_launch("histogram_kernel");
+    if (rc != AP_OK) return rc;
+    ap::cdf_kernel<<<1, ap::kScanThreads, 0, st>>>(hist, num_bins, cdf);
+    return ap::check_launch("cdf_kernel");
+}
+
+extern "C" int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stream) {
+    if (!p || !b || !b->iter_map || !b->rgb || !b->lut || p->width <= 0 || p->height <= 0) {
+        ap::set_error("ap_colour: bad arguments");
+        return AP_E_INVALID;
+    }
+    const int hist = (p->scheme_id == 11 && b->cdf != nullptr) ? 1 : 0;
+    if (hist && p->num_bins < 2) {
+        ap::set_error("ap_colour: num_bins must be >= 2");
+        return AP_E_INVALID;
+    }
+    dim3 grid((p->width + 15) / 16, (p->height + 15) / 16);
+    ap::colour_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(*p, *b, hist);
+    return ap::check_launch("colour_kernel");
+}

@@ -1,0 +1,161 @@
+/*
+ * apeiron_b200.h -- C ABI of the B200 escape-time engine.
+ *
+ * Plain structs, device pointers and sizes; every call returns 0 on success
+ * or a negative AP_E_* code, with a message retrievable through
+ * ap_last_error().  All launches go to the caller's cudaStream_t (passed as
+ * void*; NULL means the legacy default stream) and never synchronise it.
+ *
+ * The entry points replace the Numba CUDA kernel launches that
+ * math_core/engine.py issues from render_frame_ssaa (math_core/engine.py:1339)
+ * and recolor_frame (math_core/engine.py:2138).  Each declaration cites the
+ * reference kernel(s) it stands in for.
+ */
+#ifndef APEIRON_B200_H
+#define APEIRON_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define AP_API __attribute__((visibility("default")))
+#else
+#define AP_API
+#endif
+
+#define AP_ABI_VERSION 1
+
+/* Return codes. */
+#define AP_OK 0
+#define AP_E_INVALID (-1)   /* bad argument (null pointer, size, enum) */
+#define AP_E_CUDA (-2)      /* a CUDA runtime call failed */
+#define AP_E_UNSUPPORTED (-3)
+
+/* Precision tiers, chosen by the host exactly as math_core/engine.py:1402-1408. */
+#define AP_TIER_FP64 0      /* direct FP64 iteration            (cuda_kernels.py:264) */
+#define AP_TIER_DD 1        /* direct double-double iteration   (cuda_kernels.py:321) */
+#define AP_TIER_PERTURB 2   /* FP64-delta perturbation (+BLA)   (cuda_kernels.py:422, :594) */
+#define AP_TIER_FLOATEXP 3  /* FP64-mantissa FloatExp deltas    (cuda_kernels.py:819, :1102) */
+#define AP_TIER_FLOATEXP32 4 /* FP32-mantissa FloatExp deltas (this engine's fast form) */
+
+/* Arithmetic profiles.  The escape step of a boundary pixel depends on which
+ * multiply-adds are fused, so the engine can reproduce either reference. */
+#define AP_ARITH_REF_CPU 0   /* the reference's Numba CPU kernels as compiled (x86-64, FMA where LLVM fused) */
+#define AP_ARITH_REF_CUDA 1  /* the reference's CUDA sources: explicit cuda.fma fused, nothing else */
+
+/* Launch modes of the unified render pass (cuda_kernels.py:1615-1917). */
+#define AP_MODE_COARSE 0     /* one centred sample per pixel -> iter map + RGB */
+#define AP_MODE_FULL 1       /* f x f samples for every selected pixel (rebase passes) */
+#define AP_MODE_EDGE 2       /* f x f samples only where edge_mask != 0 */
+
+/* ApFrameParams.flags */
+#define AP_FLAG_NO_RGB 1u          /* skip the RGB write (histogram first pass) */
+#define AP_FLAG_ESCAPE_GLITCH 2u   /* flag escapes with |Z|^2 < 4 (non-BLA sample, cuda_kernels.py:467) */
+#define AP_FLAG_NAN_GUARD 4u       /* stage-2 NaN/Inf -> (k, glitch) (cuda_kernels.py:771) */
+#define AP_FLAG_ITER_LAST_SUB 8u   /* supersample passes write the last sub-sample to the iter map */
+#define AP_FLAG_MAP_FUSED 16u      /* pixel -> c mapping as fma(i, dx, x_min) */
+#define AP_FLAG_HIST_COLOUR 32u    /* colour through the CDF table (scheme 11 resolve passes) */
+
+typedef struct ApFrameParams {
+    int32_t width, height;     /* output pixels */
+    int32_t factor;            /* SSAA factor f >= 1 */
+    int32_t max_iter;
+    int32_t fractal_type;      /* 0 Mandelbrot, 1 Burning Ship, 2 Julia, 3 BS-Julia, 4 Multibrot */
+    int32_t tier;              /* AP_TIER_* */
+    int32_t arith;             /* AP_ARITH_* */
+    int32_t mode;              /* AP_MODE_* */
+    uint32_t flags;            /* AP_FLAG_* */
+    int32_t gen_n;             /* Multibrot power */
+    /* Direct tiers: top-left sample and sub-sample steps (double-double; FP64 uses _hi). */
+    double x_min_hi, x_min_lo, y_max_hi, y_max_lo;
+    double dx_hi, dx_lo, dy_hi, dy_lo;
+    /* Formula parameters. */
+    double julia_cx_hi, julia_cx_lo, julia_cy_hi, julia_cy_lo;
+    double gen_kr, gen_ki;
+    /* Perturbation tiers: reference position (sub-sample units) and its c. */
+    double ref_px, ref_py;
+    double ref_cx, ref_cy;
+    int32_t ref_len;           /* reference escape step; orbit arrays hold ref_len + 1 entries */
+    int32_t e_scale;           /* FloatExp exponent scale (config.py:51) */
+    int32_t bla_levels;        /* rows of the BLA table, 0 = no leaps */
+    int32_t strict_glitch;     /* Pauldelbrot test on/off */
+    int32_t rebase_pass;       /* > 0: only pixels with glitch_in != 0 are evaluated */
+    int32_t bbsa_skip;         /* series-approximation skip (0 = off) */
+    double bbsa_inv_r;
+    double bbsa[16];           /* A..H coefficients, re/im interleaved (ar, ai, br, bi, ...) */
+    /* Colouring. */
+    int32_t scheme_id;         /* 0..11 (cuda_kernels.py:171) */
+    int32_t num_bins;          /* CDF bins for scheme 11 (65536) */
+    double palette_offset, color_density, color_contrast;
+    float edge_threshold;
+    int32_t is_hdr;            /* rgb is uint16 when nonzero */
+} ApFrameParams;
+
+typedef struct ApFrameBuffers {
+    const double* ref_re;      /* [ref_len + 1] */
+    const double* ref_im;      /* [ref_len + 1] */
+    const double* bla;         /* [bla_levels, ref_len, 5]: A_re, A_im, B_re, B_im, r^2 */
+    const float* lut;          /* [2048, 3] */
+    const float* cdf;          /* [num_bins] normalised CDF (scheme 11) */
+    const uint8_t* glitch_in;  /* [H, W] */
+    const uint8_t* edge_mask;  /* [H, W] */
+    float* iter_map;           /* [H, W] smooth value, float32, -1 = interior */
+    void* rgb;                 /* [H, W, 3] uint8 or uint16 */
+    uint8_t* glitch_out;       /* [H, W] */
+    int32_t* kmap;             /* optional [H, W]: escape step; -1 never escaped, -2 cardioid/bulb skip */
+    double* s64;               /* optional [H, W]: smooth value in float64, -1 = interior */
+} ApFrameBuffers;
+
+/* Library identity. */
+AP_API int ap_abi_version(void);
+AP_API const char* ap_last_error(void);
+
+/* One unified render pass over the frame.
+ * Replaces mandelbrot_unified_{fp64,dd,perturbation,floatexp}_kernel
+ * (math_core/cuda_kernels.py:1615, :1666, :1736, :1827) launched from
+ * math_core/engine.py:1652-1888 and the rebase relaunches at :2060, :2103. */
+AP_API int ap_render_pass(const ApFrameParams* p, const ApFrameBuffers* b, void* stream);
+
+/* Supersample/rebase resolve under histogram colouring.
+ * Replaces ssaa_resolve_hist_{fp64,dd,perturbation,floatexp}_kernel
+ * (math_core/cuda_kernels.py:2038-2234, launched at math_core/engine.py:1596-1635, :2048, :2092). */
+AP_API int ap_resolve_hist_pass(const ApFrameParams* p, const ApFrameBuffers* b, void* stream);
+
+/* 8-neighbour edge mask.  Replaces edge_detect_kernel (math_core/cuda_kernels.py:1587). */
+AP_API int ap_edge_detect(const float* iter_map, uint8_t* edge_mask, int32_t width, int32_t height,
+                   float threshold, void* stream);
+
+/* Histogram of the iteration map followed by the normalised CDF.
+ * Replaces zero_histogram_cuda_kernel, build_histogram_kernel, scan_blocks_cuda_kernel,
+ * scan_single_block_cuda_kernel and finalize_normalized_cdf_cuda_kernel
+ * (math_core/cuda_kernels.py:1922-2013, launched at math_core/engine.py:1435, :1576-1585).
+ * hist: caller scratch of num_bins int32; cdf: num_bins float32 output. */
+AP_API int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height, int32_t max_iter,
+                     int32_t num_bins, int32_t* hist, float* cdf, void* stream);
+
+/* Colour every pixel from its smooth value.  With scheme 11 the CDF table is used
+ * (apply_histogram_equalization_kernel, math_core/cuda_kernels.py:2016); otherwise
+ * the closed-form transfer function (recolor_iter_map_cuda_kernel, :3201). */
+AP_API int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stream);
+
+/* Chained-BLA table from a reference orbit, built on the device.
+ * Replaces _jit_build_bla_table (math_core/high_precision.py:1101) and its upload
+ * (math_core/engine.py:416).  out: [levels, ref_len, 5] float64. */
+AP_API int ap_build_bla(const double* ref_re, const double* ref_im, int32_t ref_len, int32_t fractal_type,
+                 double tol, int32_t levels, int32_t gen_n, double gen_kr, double gen_ki,
+                 double* out, void* stream);
+
+/* Measurement helper (no counterpart in the reference): dependent-FMA throughput
+ * probe, precision 64 or 32, blocks x 256 threads x 8 chains x iters FMAs.
+ * scratch: >= blocks elements of the precision's type; *flops = FLOPs launched. */
+AP_API int ap_fma_peak_launch(int32_t precision, int32_t blocks, int32_t iters, void* scratch,
+                              double* flops, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* APEIRON_B200_H */

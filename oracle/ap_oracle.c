@@ -1,0 +1,719 @@
+/*
+ * ap_oracle.c -- CPU restatement of the reference escape-time path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine:
+ * the parity tests, __graft_entry__.smoke() and the CPU-baseline leg of
+ * bench.py call it; the product path never does.  It is written from the
+ * reference's Python/Numba sources line by line, in plain C, and shares no
+ * code with the CUDA kernels.
+ *
+ * Build: see oracle/Makefile (gcc -O2 -ffp-contract=off -pthread).  Implicit
+ * contraction is disabled, so every fused multiply-add below is written out
+ * with fma() exactly where the reference computes one:
+ *
+ *   AP_ARITH_REF_CPU   the reference's Numba CPU kernels as compiled here by
+ *                      LLVM for x86-64 (fastmath functions contract some
+ *                      multiply-adds and reassociate a few sums; the fused
+ *                      forms below were read off that compiled code).
+ *   AP_ARITH_REF_CUDA  the reference's CUDA sources as written: cuda.fma is
+ *                      fused, every other operation is rounded separately.
+ *
+ * Parity is pinned by the .npz fixtures in tests/golden, generated by running the reference
+ * (tests/golden/make_golden.py).
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+
+#include "apeiron_b200.h"
+
+#define APO_EXPORT __attribute__((visibility("default")))
+
+/* ---- row-parallel helper (pthreads; rows are handed out one at a time) ---- */
+typedef void (*row_fn)(void* ctx, int row);
+typedef struct {
+    row_fn fn;
+    void* ctx;
+    int rows;
+    int next;
+    pthread_mutex_t lock;
+} RowPool;
+
+static void* row_worker(void* arg) {
+    RowPool* rp = (RowPool*)arg;
+    for (;;) {
+        pthread_mutex_lock(&rp->lock);
+        int r = rp->next++;
+        pthread_mutex_unlock(&rp->lock);
+        if (r >= rp->rows) break;
+        rp->fn(rp->ctx, r);
+    }
+    return NULL;
+}
+
+static int g_threads = 0; /* 0: all online cores */
+
+static void parallel_rows(int rows, row_fn fn, void* ctx) {
+    int n = g_threads > 0 ? g_threads : (int)sysconf(_SC_NPROCESSORS_ONLN);
+    if (n < 1) n = 1;
+    if (n > 256) n = 256;
+    if (n > rows) n = rows;
+    RowPool rp = {fn, ctx, rows, 0, PTHREAD_MUTEX_INITIALIZER};
+    if (n <= 1) {
+        row_worker(&rp);
+        return;
+    }
+    pthread_t th[256];
+    int started = 0;
+    for (int t = 1; t < n; t++)
+        if (pthread_create(&th[started], NULL, row_worker, &rp) == 0) started++;
+    row_worker(&rp);
+    for (int t = 0; t < started; t++) pthread_join(th[t], NULL);
+}
+
+/* config.py:25-26 (passed by the engine to every kernel as doubles). */
+static const double INV_LN2 = 1.4426950408889634;
+static const double LN_BAILOUT_LOG = 1.7129177284488854;
+static const double BAILOUT = 65536.0;
+
+typedef struct {
+    float s;      /* float32 smooth value as the reference stores it; -1 interior */
+    double s64;   /* the same quantity in float64 */
+    int k;        /* escape step, -1 never escaped */
+    int glitch;
+} Sample;
+
+/* Python's float modulo for a positive divisor (x % m). */
+static double py_mod(double x, double m) {
+    double r = fmod(x, m);
+    if (r != 0.0) {
+        if ((r < 0.0) != (m < 0.0)) r += m;
+    } else {
+        r = copysign(0.0, m);
+    }
+    return r;
+}
+
+/* 1/ln(n) rounded to float32 for Multibrot, else 1/ln 2 (cpu_kernels.py:241). */
+static double inv_ln_for(int fractal_type, int gen_n) {
+    if (fractal_type == 4 && gen_n > 1) return (double)(float)(1.0 / log((double)gen_n));
+    return INV_LN2;
+}
+
+/* Smooth escape value: f32(k+1) - f32(nu) (cpu_kernels.py:249, cuda_kernels.py:280). */
+static Sample escaped(int k, double mag2, double inv_ln) {
+    Sample o;
+    double log_mag = log(mag2);
+    o.k = k;
+    o.glitch = 0;
+    if (log_mag > 1.0) {
+        double nu = (log(0.5 * log_mag) - LN_BAILOUT_LOG) * inv_ln;
+        o.s = (float)((double)k + 1.0) - (float)nu;
+        o.s64 = ((double)k + 1.0) - nu;
+    } else {
+        o.s = (float)k;
+        o.s64 = (double)k;
+    }
+    return o;
+}
+
+static Sample interior(void) {
+    Sample o;
+    o.s = -1.0f;
+    o.s64 = -1.0;
+    o.k = -1;
+    o.glitch = 0;
+    return o;
+}
+
+/* Removed by the Mandelbrot cardioid/bulb test: interior with zero iterations. */
+static Sample skipped(void) {
+    Sample o = interior();
+    o.k = -2;
+    return o;
+}
+
+/* ------------------------------------------------------------------------- */
+/* FP64 direct iteration: cpu_kernels.py:228-266 / cuda_kernels.py:264-317    */
+/* ------------------------------------------------------------------------- */
+static Sample fp64_sample(double x, double y, const ApFrameParams* p) {
+    const int ft = p->fractal_type;
+    const int cpu = (p->arith == AP_ARITH_REF_CPU);
+    const int max_iter = p->max_iter;
+    double zx, zy, cx, cy;
+
+    if (ft == 0) {
+        /* Main cardioid and period-2 bulb. */
+        double xm = x - 0.25;
+        double y2 = y * y;
+        double q = cpu ? fma(xm, xm, y2) : xm * xm + y2;
+        double xp = x + 1.0;
+        double b = cpu ? fma(xp, xp, y2) : xp * xp + y2;
+        if ((q * (q + xm) <= 0.25 * y2) || (b <= 0.0625)) return skipped();
+    }
+    if (ft == 2 || ft == 3) {
+        zx = x; zy = y; cx = p->julia_cx_hi; cy = p->julia_cy_hi;
+    } else {
+        zx = 0.0; zy = 0.0; cx = x; cy = y;
+    }
+    const double inv_ln = inv_ln_for(ft, p->gen_n);
+
+    if (ft == 0 || ft == 2) {
+        for (int k = 0; k < max_iter; k++) {
+            double zx2 = zx * zx, zy2 = zy * zy;
+            double mag2 = zx2 + zy2;
+            if (mag2 > BAILOUT) return escaped(k, mag2, inv_ln);
+            if (cpu) {
+                /* zy' = fma(2zy, zx, cy); zx' = (cx - zy^2) + zx^2 */
+                double nzy = fma(zy + zy, zx, cy);
+                zx = (cx - zy2) + zx2;
+                zy = nzy;
+            } else {
+                zy = 2.0 * zx * zy + cy;
+                zx = zx2 - zy2 + cx;
+            }
+        }
+        return interior();
+    } else if (ft == 1 || ft == 3) {
+        for (int k = 0; k < max_iter; k++) {
+            double zx2 = zx * zx, zy2 = zy * zy;
+            double mag2 = zx2 + zy2;
+            if (mag2 > BAILOUT) return escaped(k, mag2, inv_ln);
+            double ax = fabs(zx), ay = fabs(zy);
+            if (cpu) {
+                /* zy' = fma(|zx|, 2|zy|, -cy); zx' = (cx + zx^2) - zy^2 */
+                double nzy = fma(ax, ay + ay, -cy);
+                zx = (cx + zx2) - zy2;
+                zy = nzy;
+            } else {
+                zy = 2.0 * ax * ay - cy;
+                zx = zx2 - zy2 + cx;
+            }
+        }
+        return interior();
+    } else if (ft == 4) {
+        const int n = p->gen_n;
+        const double kr = p->gen_kr, ki = p->gen_ki;
+        for (int k = 0; k < max_iter; k++) {
+            double mag2;
+            if (cpu) {
+                mag2 = fma(zx, zx, zy * zy);
+            } else {
+                double zx2 = zx * zx, zy2 = zy * zy;
+                mag2 = zx2 + zy2;
+            }
+            if (mag2 > BAILOUT) return escaped(k, mag2, inv_ln);
+            double zr = zx, zi = zy;
+            for (int t = 0; t < n - 1; t++) {
+                double nr, ni;
+                if (cpu) {
+                    nr = fma(zr, zx, -(zi * zy));
+                    ni = fma(zi, zx, zr * zy);
+                } else {
+                    nr = zr * zx - zi * zy;
+                    ni = zr * zy + zi * zx;
+                }
+                zr = nr; zi = ni;
+            }
+            if (cpu) {
+                /* zx' = fma(zx, kr, -fma(ki, zy, -cx)) + zn_r ; zy' = fma(ki, zx, fma(zy, kr, cy)) + zn_i */
+                double a = fma(zx, kr, -fma(ki, zy, -cx));
+                double b = fma(ki, zx, fma(zy, kr, cy));
+                zx = a + zr;
+                zy = b + zi;
+            } else {
+                double kz_r = kr * zx - ki * zy;
+                double kz_i = kr * zy + ki * zx;
+                zx = zr + kz_r + cx;
+                zy = zi + kz_i + cy;
+            }
+        }
+        return interior();
+    }
+    return interior();
+}
+
+/* ------------------------------------------------------------------------- */
+/* Colouring: cuda_kernels.py:157-259                                         */
+/* ------------------------------------------------------------------------- */
+static double tri_wave(double phase) {
+    return 1.0 - fabs((phase < 0.0 ? phase + 2.0 : phase) - 1.0);
+}
+
+static double palette_norm(double s, int scheme, double off, double density, double contrast) {
+    const double dens = density <= 0.0 ? 1.0 : density;
+    const double cont = contrast <= 0.0 ? 1.0 : contrast;
+    const double TWO_PI = 6.28318530718;
+    if (scheme == 0 || scheme > 10) {
+        double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        return cont != 1.0 ? pow(tri, cont) : tri;
+    } else if (scheme == 1) {
+        return tri_wave(py_mod(log(s * cont + 1.0) * (0.45 * dens) + off * 2.0, 2.0));
+    } else if (scheme == 2) {
+        double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        double k = 4.0 * cont;
+        double td = tanh(0.5 * k);
+        double scale = fabs(td) > 1e-7 ? 0.5 / td : 0.5186574;
+        return 0.5 + tanh((tri - 0.5) * k) * scale;
+    } else if (scheme == 3) {
+        double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        double k = 3.0 * cont;
+        double ed = exp(k) - 1.0;
+        double scale = fabs(ed) > 1e-7 ? 1.0 / ed : 0.0523957;
+        return (exp(k * tri) - 1.0) * scale;
+    } else if (scheme == 4) {
+        double tri = tri_wave(py_mod(sqrt(s) * (0.5 * dens) + off * 2.0, 2.0));
+        return cont != 1.0 ? pow(tri, cont) : tri;
+    } else if (scheme == 5) {
+        double ang = s * (0.05 * dens) + off * TWO_PI;
+        double ratio = 1.61803398875 * cont;
+        return 0.5 + 0.25 * (sin(ang) + sin(ang * ratio));
+    } else if (scheme == 6) {
+        double ang = s * (0.08 * dens) + off * TWO_PI;
+        double val = 0.5 * (1.0 - cos(ang));
+        return cont != 1.0 ? pow(val, cont) : val;
+    } else if (scheme == 7) {
+        double ph = s * (0.05 * dens) + off * TWO_PI;
+        double b = 0.5 * cont;
+        double wave = sin(ph) + b * sin(ph * 2.0 + 1.2) + (b * b) * sin(ph * 4.0 + 2.4) +
+                      (b * b * b) * sin(ph * 8.0 + 3.6);
+        double ns = 1.0 + b + b * b + b * b * b;
+        double scale = ns > 1e-7 ? 0.5 / ns : 0.26666666666666666;
+        return 0.5 + scale * wave;
+    } else if (scheme == 8) {
+        double tri = tri_wave(py_mod(sqrt(s) * (0.1 * dens) + off * 2.0, 2.0));
+        if (cont != 1.0) tri = pow(tri, cont);
+        double t2 = tri * tri;
+        return t2 * tri * (tri * (tri * 6.0 - 15.0) + 10.0);
+    } else if (scheme == 9) {
+        double ang = s * (0.04 * dens) + (s * s) * (0.00008 * dens * cont) + off * TWO_PI;
+        return 0.5 + 0.5 * sin(ang);
+    } else if (scheme == 10) {
+        double raw = py_mod(1.0 - exp(-0.06 * cont * sqrt(s * dens)) + off, 1.0);
+        return raw >= 0.0 ? raw : raw + 1.0;
+    }
+    return 0.0;
+}
+
+/* cuda_kernels.py:237-259 */
+static double cdf_norm(double s, int max_iter, const float* cdf, int num_bins,
+                       double off, double density, double contrast) {
+    if (s < 0.0) return -1.0;
+    double inv_max = 1.0 / fmax(1.0, (double)max_iter);
+    double pos = (s * inv_max) * (double)(num_bins - 1);
+    int k = (int)pos;
+    double c;
+    if (k >= num_bins - 1) {
+        c = cdf[num_bins - 1];
+    } else if (k < 0) {
+        c = cdf[0];
+    } else {
+        double frac = pos - (double)k;
+        float c0 = cdf[k], c1 = cdf[k + 1];
+        float d = c1 - c0;                 /* float32 difference */
+        c = (double)c0 + frac * (double)d;
+    }
+    if (contrast != 1.0 && contrast > 0.0) c = pow(c, contrast);
+    double dens = density <= 0.0 ? 1.0 : density;
+    return tri_wave(py_mod(c * (2.0 * dens) + off * 2.0, 2.0));
+}
+
+/* cuda_kernels.py:157-168 */
+static void lut_lerp(const float* lut, double norm, double* r, double* g, double* b) {
+    double n = norm < 0.0 ? 0.0 : (norm > 1.0 ? 1.0 : norm);
+    double pos = n * 2047.0;
+    int i0 = (int)pos;
+    int i1 = i0 >= 2047 ? 2047 : i0 + 1;
+    double frac = pos - (double)i0;
+    double inv = 1.0 - frac;
+    *r = (double)lut[i0 * 3 + 0] * inv + (double)lut[i1 * 3 + 0] * frac;
+    *g = (double)lut[i0 * 3 + 1] * inv + (double)lut[i1 * 3 + 1] * frac;
+    *b = (double)lut[i0 * 3 + 2] * inv + (double)lut[i1 * 3 + 2] * frac;
+}
+
+static double colour_norm(const ApFrameParams* p, const ApFrameBuffers* bf, double s, int hist) {
+    if (hist)
+        return cdf_norm(s, p->max_iter, bf->cdf, p->num_bins, p->palette_offset, p->color_density,
+                        p->color_contrast);
+    return palette_norm(s, p->scheme_id, p->palette_offset, p->color_density, p->color_contrast);
+}
+
+static void put_rgb(const ApFrameParams* p, void* rgb, size_t idx, double r, double g, double b) {
+    if (p->is_hdr) {
+        uint16_t* o = (uint16_t*)rgb + idx * 3;
+        o[0] = (uint16_t)(int64_t)(r + 0.5);
+        o[1] = (uint16_t)(int64_t)(g + 0.5);
+        o[2] = (uint16_t)(int64_t)(b + 0.5);
+    } else {
+        uint8_t* o = (uint8_t*)rgb + idx * 3;
+        o[0] = (uint8_t)(int64_t)(r + 0.5);
+        o[1] = (uint8_t)(int64_t)(g + 0.5);
+        o[2] = (uint8_t)(int64_t)(b + 0.5);
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Sample dispatch over the tiers                                             */
+/* ------------------------------------------------------------------------- */
+/* Defined further down (perturbation tiers). */
+static Sample dd_sample_at(const ApFrameParams* p, double sub_i, double sub_j);
+static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
+                             double sub_j);
+
+/* Sub-sample coordinates (sub_i, sub_j) -> sample, as each unified kernel maps them. */
+static Sample sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i, double sub_j) {
+    switch (p->tier) {
+    case AP_TIER_FP64: {
+        double x, y;
+        if (p->flags & AP_FLAG_MAP_FUSED) {
+            x = fma(sub_i, p->dx_hi, p->x_min_hi);
+            y = fma(-sub_j, p->dy_hi, p->y_max_hi);
+        } else {
+            x = p->x_min_hi + sub_i * p->dx_hi;
+            y = p->y_max_hi - sub_j * p->dy_hi;
+        }
+        return fp64_sample(x, y, p);
+    }
+    case AP_TIER_DD:
+        return dd_sample_at(p, sub_i, sub_j);
+    default:
+        return pert_sample_at(p, b, sub_i, sub_j);
+    }
+}
+
+static int is_perturbative(const ApFrameParams* p) {
+    return p->tier == AP_TIER_PERTURB || p->tier == AP_TIER_FLOATEXP || p->tier == AP_TIER_FLOATEXP32;
+}
+
+/* One unified pass (cuda_kernels.py:1615-1917).  hist_resolve selects the
+ * ssaa_resolve_hist_* semantics (cuda_kernels.py:2038-2234). */
+typedef struct {
+    const ApFrameParams* p;
+    const ApFrameBuffers* b;
+    int hist_resolve;
+} PassCtx;
+
+static void render_row(void* vctx, int j) {
+    const PassCtx* c = (const PassCtx*)vctx;
+    const ApFrameParams* p = c->p;
+    const ApFrameBuffers* b = c->b;
+    const int hist_resolve = c->hist_resolve;
+    const int W = p->width, f = p->factor;
+    const double sub_offset = ((double)f - 1.0) * 0.5;
+    const int pert = is_perturbative(p);
+    const int hist_colour = hist_resolve || (p->flags & AP_FLAG_HIST_COLOUR);
+    {
+        for (int i = 0; i < W; i++) {
+            const size_t idx = (size_t)j * W + i;
+            if (p->rebase_pass > 0 && b->glitch_in[idx] == 0) continue;
+            int mode = p->mode;
+            if (hist_resolve) {
+                /* Resolve pass: edge pixels on pass 0, glitched pixels on rebase passes. */
+                if (p->rebase_pass == 0 && b->edge_mask[idx] == 0) continue;
+                mode = AP_MODE_FULL;
+            } else if (mode == AP_MODE_EDGE && b->edge_mask[idx] == 0) {
+                continue;
+            }
+            if (mode == AP_MODE_COARSE) {
+                Sample o = sample_at(p, b, (double)(i * f) + sub_offset, (double)(j * f) + sub_offset);
+                b->iter_map[idx] = o.s;
+                if (b->kmap) b->kmap[idx] = o.k;
+                if (b->s64) b->s64[idx] = o.s64;
+                if (pert && b->glitch_out) b->glitch_out[idx] = o.glitch > 0 ? 1 : 0;
+                if (!(p->flags & AP_FLAG_NO_RGB)) {
+                    double r = 0, g = 0, bb = 0;
+                    if ((double)o.s >= 0.0) {
+                        lut_lerp(b->lut, colour_norm(p, b, (double)o.s, hist_colour), &r, &g, &bb);
+                    }
+                    put_rgb(p, b->rgb, idx, r, g, bb);
+                }
+            } else {
+                double ra = 0.0, ga = 0.0, ba = 0.0;
+                int glitches = 0;
+                Sample last = interior();
+                for (int sy = 0; sy < f; sy++) {
+                    for (int sx = 0; sx < f; sx++) {
+                        Sample o = sample_at(p, b, (double)(i * f + sx), (double)(j * f + sy));
+                        last = o;
+                        if (o.glitch > 0) glitches++;
+                        if ((double)o.s >= 0.0) {
+                            double r, g, bb;
+                            lut_lerp(b->lut, colour_norm(p, b, (double)o.s, hist_colour), &r, &g, &bb);
+                            ra += r; ga += g; ba += bb;
+                        }
+                    }
+                }
+                const double inv = 1.0 / (double)(f * f);
+                put_rgb(p, b->rgb, idx, ra * inv, ga * inv, ba * inv);
+                if (pert && b->glitch_out) b->glitch_out[idx] = glitches > 0 ? 1 : 0;
+                const int write_iter = hist_resolve ? (p->rebase_pass > 0)
+                                                    : ((p->flags & AP_FLAG_ITER_LAST_SUB) != 0);
+                if (write_iter) {
+                    b->iter_map[idx] = last.s;
+                    if (b->kmap) b->kmap[idx] = last.k;
+                    if (b->s64) b->s64[idx] = last.s64;
+                }
+            }
+        }
+    }
+}
+
+static void render_pass(const ApFrameParams* p, const ApFrameBuffers* b, int hist_resolve) {
+    PassCtx c = {p, b, hist_resolve};
+    parallel_rows(p->height, render_row, &c);
+}
+
+/* ------------------------------------------------------------------------- */
+/* DD and perturbation tiers (filled in by the following sections)            */
+/* ------------------------------------------------------------------------- */
+/* Double-double arithmetic: cpu_kernels.py:96-153 (CPU: Dekker split) and
+ * cuda_kernels.py:45-90 (CUDA: error-free product by fma). */
+typedef struct { double hi, lo; } DD;
+
+static DD dd_two_sum(double a, double b) {
+    double s = a + b, v = s - a;
+    DD r = {s, (a - (s - v)) + (b - v)};
+    return r;
+}
+
+static DD dd_two_prod(double a, double b, int cpu) {
+    DD r;
+    if (cpu) {
+        double c = 134217729.0 * a;
+        double ah = c - (c - a), al = a - ah;
+        c = 134217729.0 * b;
+        double bh = c - (c - b), bl = b - bh;
+        r.hi = a * b;
+        r.lo = ((ah * bh - r.hi) + ah * bl + al * bh) + al * bl;
+    } else {
+        r.hi = a * b;
+        r.lo = fma(a, b, -r.hi);
+    }
+    return r;
+}
+
+static DD dd_add(DD a, DD b) {
+    DD s = dd_two_sum(a.hi, b.hi);
+    return dd_two_sum(s.hi, s.lo + a.lo + b.lo);
+}
+
+static DD dd_sub(DD a, DD b) {
+    DD s = dd_two_sum(a.hi, -b.hi);
+    return dd_two_sum(s.hi, s.lo + a.lo - b.lo);
+}
+
+static DD dd_mul(DD a, DD b, int cpu) {
+    DD pr = dd_two_prod(a.hi, b.hi, cpu);
+    return dd_two_sum(pr.hi, pr.lo + a.hi * b.lo + a.lo * b.hi);
+}
+
+static DD dd_mul_f64(DD a, double b, int cpu) {
+    DD pr = dd_two_prod(a.hi, b, cpu);
+    return dd_two_sum(pr.hi, pr.lo + a.lo * b);
+}
+
+static DD dd_sqr(DD a, int cpu) {
+    DD pr = dd_two_prod(a.hi, a.hi, cpu);
+    return dd_two_sum(pr.hi, pr.lo + 2.0 * a.hi * a.lo);
+}
+
+static DD dd_abs(DD a) {
+    if (a.hi < 0.0 || (a.hi == 0.0 && a.lo < 0.0)) {
+        DD r = {-a.hi, -a.lo};
+        return r;
+    }
+    return a;
+}
+
+/* cpu_kernels.py:271-369 / cuda_kernels.py:321-418 */
+static Sample dd_sample(DD cx0, DD cy0, const ApFrameParams* p) {
+    const int ft = p->fractal_type, cpu = p->arith == AP_ARITH_REF_CPU;
+    if (ft == 0) {
+        double xm = cx0.hi - 0.25, y2 = cy0.hi * cy0.hi;
+        double q = xm * xm + y2;
+        if ((q * (q + xm) <= 0.25 * y2) || ((cx0.hi + 1.0) * (cx0.hi + 1.0) + y2 <= 0.0625))
+            return skipped();
+    }
+    DD jx = {p->julia_cx_hi, p->julia_cx_lo}, jy = {p->julia_cy_hi, p->julia_cy_lo};
+    DD zero = {0.0, 0.0};
+    DD zx, zy, cx, cy;
+    if (ft == 2 || ft == 3) { zx = cx0; zy = cy0; cx = jx; cy = jy; }
+    else { zx = zero; zy = zero; cx = cx0; cy = cy0; }
+    const double inv_ln = inv_ln_for(ft, p->gen_n);
+    for (int k = 0; k < p->max_iter; k++) {
+        DD zx2 = dd_sqr(zx, cpu), zy2 = dd_sqr(zy, cpu);
+        double mag2 = zx2.hi + zy2.hi;
+        if (mag2 > BAILOUT) return escaped(k, mag2, inv_ln);
+        if (ft == 0 || ft == 2) {
+            DD sub = dd_sub(zx2, zy2);
+            DD zxy = dd_mul(zx, zy, cpu);
+            DD two = {zxy.hi * 2.0, zxy.lo * 2.0};
+            zx = dd_add(sub, cx);
+            zy = dd_add(two, cy);
+        } else if (ft == 1 || ft == 3) {
+            DD sub = dd_sub(zx2, zy2);
+            DD zxy = dd_mul(dd_abs(zx), dd_abs(zy), cpu);
+            DD two = {zxy.hi * 2.0, zxy.lo * 2.0};
+            zx = dd_add(sub, cx);
+            zy = dd_sub(two, cy);
+        } else if (ft == 4) {
+            DD cr = zx, ci = zy;
+            for (int t = 0; t < p->gen_n - 1; t++) {
+                DD r1 = dd_mul(cr, zx, cpu), r2 = dd_mul(ci, zy, cpu);
+                DD re = dd_sub(r1, r2);
+                DD i1 = dd_mul(cr, zy, cpu), i2 = dd_mul(ci, zx, cpu);
+                DD im = dd_add(i1, i2);
+                cr = re; ci = im;
+            }
+            DD kz_r = dd_sub(dd_mul_f64(zx, p->gen_kr, cpu), dd_mul_f64(zy, p->gen_ki, cpu));
+            DD kz_i = dd_add(dd_mul_f64(zy, p->gen_kr, cpu), dd_mul_f64(zx, p->gen_ki, cpu));
+            DD tr = dd_add(cr, kz_r), ti = dd_add(ci, kz_i);
+            zx = dd_add(tr, cx);
+            zy = dd_add(ti, cy);
+        } else {
+            return interior();
+        }
+    }
+    return interior();
+}
+
+/* Pixel mapping of the DD kernels (cuda_kernels.py:1685-1691). */
+static Sample dd_sample_at(const ApFrameParams* p, double sub_i, double sub_j) {
+    const int cpu = p->arith == AP_ARITH_REF_CPU;
+    DD dy = {p->dy_hi, p->dy_lo}, ymax = {p->y_max_hi, p->y_max_lo};
+    DD dx = {p->dx_hi, p->dx_lo}, xmin = {p->x_min_hi, p->x_min_lo};
+    DD cy = dd_sub(ymax, dd_mul_f64(dy, sub_j, cpu));
+    DD cx = dd_add(xmin, dd_mul_f64(dx, sub_i, cpu));
+    return dd_sample(cx, cy, p);
+}
+
+static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
+                             double sub_j) {
+    (void)p; (void)b; (void)sub_i; (void)sub_j;
+    return interior();
+}
+
+/* ------------------------------------------------------------------------- */
+/* Exported oracle entry points (apo_*: host pointers, same structs as ap_*)  */
+/* ------------------------------------------------------------------------- */
+APO_EXPORT int apo_abi_version(void) { return AP_ABI_VERSION; }
+
+APO_EXPORT int apo_render_pass(const ApFrameParams* p, const ApFrameBuffers* b) {
+    if (!p || !b || p->width <= 0 || p->height <= 0 || p->factor < 1) return AP_E_INVALID;
+    render_pass(p, b, 0);
+    return AP_OK;
+}
+
+APO_EXPORT int apo_resolve_hist_pass(const ApFrameParams* p, const ApFrameBuffers* b) {
+    if (!p || !b || p->width <= 0 || p->height <= 0 || p->factor < 1) return AP_E_INVALID;
+    render_pass(p, b, 1);
+    return AP_OK;
+}
+
+/* cuda_kernels.py:1587-1611 (float32 difference against the float32 threshold). */
+APO_EXPORT int apo_edge_detect(const float* it, uint8_t* edge, int W, int H, float thr) {
+    for (int j = 0; j < H; j++) {
+        for (int i = 0; i < W; i++) {
+            float s = it[(size_t)j * W + i];
+            int e = 0;
+            for (int dj = -1; dj <= 1 && !e; dj++) {
+                int nj = j + dj;
+                if (nj < 0 || nj >= H) continue;
+                for (int di = -1; di <= 1; di++) {
+                    int ni = i + di;
+                    if (ni < 0 || ni >= W || (di == 0 && dj == 0)) continue;
+                    float sn = it[(size_t)nj * W + ni];
+                    float d = s - sn;
+                    if ((s < 0.0f) != (sn < 0.0f) || (s >= 0.0f && fabsf(d) > thr)) {
+                        e = 1;
+                        break;
+                    }
+                }
+            }
+            edge[(size_t)j * W + i] = (uint8_t)e;
+        }
+    }
+    return AP_OK;
+}
+
+/* cuda_kernels.py:1922-2013: histogram, float64 prefix sum, normalised float32 CDF. */
+APO_EXPORT int apo_histogram_cdf(const float* it, int W, int H, int max_iter, int num_bins,
+                                 int32_t* hist, float* cdf) {
+    memset(hist, 0, sizeof(int32_t) * (size_t)num_bins);
+    const double inv_max = 1.0 / fmax(1.0, (double)max_iter);
+    for (size_t q = 0; q < (size_t)W * H; q++) {
+        float s = it[q];
+        if (s >= 0.0f) {
+            double pos = ((double)s * inv_max) * (double)(num_bins - 1);
+            int bin = (int)pos;
+            if (bin >= num_bins) bin = num_bins - 1;
+            else if (bin < 0) bin = 0;
+            hist[bin] += 1;
+        }
+    }
+    double total = 0.0;
+    for (int q = 0; q < num_bins; q++) total += (double)hist[q];
+    double run = 0.0;
+    for (int q = 0; q < num_bins; q++) {
+        run += (double)hist[q];
+        cdf[q] = total > 0.0 ? (float)(run / total) : (float)((double)q / (double)(num_bins - 1));
+    }
+    return AP_OK;
+}
+
+/* apply_histogram_equalization_kernel (cuda_kernels.py:2016) and
+ * recolor_iter_map_cuda_kernel (cuda_kernels.py:3201). */
+static void colour_row(void* vctx, int j) {
+    const PassCtx* c = (const PassCtx*)vctx;
+    const ApFrameParams* p = c->p;
+    const ApFrameBuffers* b = c->b;
+    const int hist = p->scheme_id == 11 && b->cdf != NULL;
+    for (int i = 0; i < p->width; i++) {
+        size_t idx = (size_t)j * p->width + i;
+        double s = b->iter_map[idx];
+        double r = 0, g = 0, bb = 0;
+        if (s >= 0.0) lut_lerp(b->lut, colour_norm(p, b, s, hist), &r, &g, &bb);
+        put_rgb(p, b->rgb, idx, r, g, bb);
+    }
+}
+
+APO_EXPORT int apo_colour(const ApFrameParams* p, const ApFrameBuffers* b) {
+    PassCtx c = {p, b, 0};
+    parallel_rows(p->height, colour_row, &c);
+    return AP_OK;
+}
+
+/* Per-sample FP64 values on an explicit coordinate grid (x per column, y per row). */
+typedef struct {
+    const ApFrameParams* p;
+    const double* xs;
+    const double* ys;
+    int W;
+    float* s32;
+    double* s64;
+    int32_t* kmap;
+} GridCtx;
+
+static void grid_row(void* vctx, int j) {
+    const GridCtx* c = (const GridCtx*)vctx;
+    for (int i = 0; i < c->W; i++) {
+        Sample o = fp64_sample(c->xs[i], c->ys[j], c->p);
+        size_t idx = (size_t)j * c->W + i;
+        if (c->s32) c->s32[idx] = o.s;
+        if (c->s64) c->s64[idx] = o.s64;
+        if (c->kmap) c->kmap[idx] = o.k;
+    }
+}
+
+APO_EXPORT int apo_fp64_grid(const ApFrameParams* p, const double* xs, const double* ys, int W, int H,
+                             float* s32, double* s64, int32_t* kmap) {
+    GridCtx c = {p, xs, ys, W, s32, s64, kmap};
+    parallel_rows(H, grid_row, &c);
+    return AP_OK;
+}
+
+/* Number of worker threads (0 = all online cores). */
+APO_EXPORT void apo_set_threads(int n) { g_threads = n < 0 ? 0 : n; }

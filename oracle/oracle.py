@@ -1,0 +1,118 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Loads oracle/_build/libap_oracle.so (built by ``make -C oracle``) and exposes
+numpy-level helpers.  Only the tests, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py use this module.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from fractura_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libap_oracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER(abi.ApFrameParams)
+        B = C.POINTER(abi.ApFrameBuffers)
+        L.apo_render_pass.argtypes = [P, B]
+        L.apo_resolve_hist_pass.argtypes = [P, B]
+        L.apo_colour.argtypes = [P, B]
+        L.apo_edge_detect.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float]
+        L.apo_histogram_cdf.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_void_p, C.c_void_p]
+        L.apo_fp64_grid.argtypes = [P, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                    C.c_void_p, C.c_void_p, C.c_void_p]
+        L.apo_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"oracle {what} failed with code {rc}")
+
+
+def set_threads(n):
+    lib().apo_set_threads(int(n))
+
+
+def fp64_grid(params, xs, ys):
+    xs = np.ascontiguousarray(xs, np.float64)
+    ys = np.ascontiguousarray(ys, np.float64)
+    H, W = len(ys), len(xs)
+    s32 = np.empty((H, W), np.float32)
+    s64 = np.empty((H, W), np.float64)
+    k = np.empty((H, W), np.int32)
+    _check(lib().apo_fp64_grid(C.byref(params), ptr(xs), ptr(ys), W, H, ptr(s32), ptr(s64), ptr(k)),
+           "fp64_grid")
+    return s32, s64, k
+
+
+class Frame:
+    """Host buffers of one frame, laid out as ApFrameBuffers expects."""
+
+    def __init__(self, W, H, is_hdr=False, lut=None):
+        self.W, self.H = W, H
+        self.iter_map = np.zeros((H, W), np.float32)
+        self.rgb = np.zeros((H, W, 3), np.uint16 if is_hdr else np.uint8)
+        self.glitch_out = np.zeros((H, W), np.uint8)
+        self.glitch_in = np.zeros((H, W), np.uint8)
+        self.edge = np.zeros((H, W), np.uint8)
+        self.kmap = np.zeros((H, W), np.int32)
+        self.s64 = np.zeros((H, W), np.float64)
+        self.cdf = None
+        self.hist = None
+        self.lut = lut
+        self.ref_re = self.ref_im = self.bla = None
+
+    def buffers(self):
+        b = abi.ApFrameBuffers()
+        b.ref_re, b.ref_im, b.bla = ptr(self.ref_re), ptr(self.ref_im), ptr(self.bla)
+        b.lut, b.cdf = ptr(self.lut), ptr(self.cdf)
+        b.glitch_in, b.edge_mask = ptr(self.glitch_in), ptr(self.edge)
+        b.iter_map, b.rgb, b.glitch_out = ptr(self.iter_map), ptr(self.rgb), ptr(self.glitch_out)
+        b.kmap, b.s64 = ptr(self.kmap), ptr(self.s64)
+        return b
+
+
+def render_pass(params, fr):
+    _check(lib().apo_render_pass(C.byref(params), C.byref(fr.buffers())), "render_pass")
+
+
+def resolve_hist_pass(params, fr):
+    _check(lib().apo_resolve_hist_pass(C.byref(params), C.byref(fr.buffers())), "resolve_hist_pass")
+
+
+def colour(params, fr):
+    _check(lib().apo_colour(C.byref(params), C.byref(fr.buffers())), "colour")
+
+
+def edge_detect(fr, threshold):
+    _check(lib().apo_edge_detect(ptr(fr.iter_map), ptr(fr.edge), fr.W, fr.H, float(threshold)),
+           "edge_detect")
+
+
+def histogram_cdf(fr, max_iter, num_bins=65536):
+    fr.hist = np.zeros(num_bins, np.int32)
+    fr.cdf = np.zeros(num_bins, np.float32)
+    _check(lib().apo_histogram_cdf(ptr(fr.iter_map), fr.W, fr.H, int(max_iter), int(num_bins),
+                                   ptr(fr.hist), ptr(fr.cdf)), "histogram_cdf")

@@ -1,0 +1,205 @@
+"""Generate the golden fixtures under tests/golden/ by running the reference.
+
+Run in a container that holds the reference tree (default /root/reference,
+override with APEIRON_REFERENCE_ROOT):
+
+    python tests/golden/make_golden.py [section ...]
+
+Every fixture records the inputs it was made from, so the tests rebuild the
+same inputs without the reference.  Sections:
+
+  fp64     per-sample FP64 escape values for all five formulas
+           (math_core/cpu_kernels.py:228 cpu_compute_fp64_sample)
+  render1  full-frame renders of the 640x360 Mandelbrot overview through
+           math_core/engine.py:471 render_frame_cpu (schemes 0..11, SSAA)
+  dd       per-sample double-double escape values
+           (math_core/cpu_kernels.py:271 cpu_compute_dd_sample)
+  render2  Burning Ship DD frames at 1e-20 with 2x adaptive SSAA
+  orbits   Decimal reference orbits (math_core/high_precision.py:706)
+  pert     per-sample FP64-delta perturbation values with and without
+           chained BLA (math_core/cpu_kernels.py:374)
+  bla      chained-BLA tables (math_core/high_precision.py:1101)
+  fexp     FloatExp perturbation samples at 1e-1000
+           (math_core/cpu_kernels.py:606)
+  render3  deep-zoom perturbation frames with Pauldelbrot rebasing
+"""
+import hashlib
+import json
+import os
+import sys
+import time
+from decimal import Decimal
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+import ref_shim  # noqa: E402
+
+R = ref_shim.install()
+INV_LN2 = R.config.INV_LN2_F32
+LN_BAIL = R.config.LN_BAILOUT_LOG
+
+SEED = 20261203
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name)
+    np.savez_compressed(path, **arrays)
+    print(f"  wrote {name}: {os.path.getsize(path) / 1024:.1f} KiB")
+
+
+# ---------------------------------------------------------------------------
+# Per-sample FP64 escape values
+# ---------------------------------------------------------------------------
+FP64_CASES = [
+    # name, fractal_type, cx, cy, width, max_iter, jx, jy, n, kr, ki
+    ("mandel_seahorse", 0, -0.7436439, 0.1318259, 1e-6, 2000, 0.0, 0.0, 3, 0.25, 1.0),
+    ("mandel_overview", 0, -0.65, 0.0, 4.0, 500, 0.0, 0.0, 3, 0.25, 1.0),
+    ("ship", 1, -1.75, 0.03, 0.18, 1000, 0.0, 0.0, 3, 0.25, 1.0),
+    ("julia", 2, 0.0, 0.0, 3.0, 2000, -0.8, 0.156, 3, 0.25, 1.0),
+    ("ship_julia", 3, 0.0, 0.0, 4.0, 1000, -1.755, 0.03, 3, 0.25, 1.0),
+    ("multibrot3", 4, 0.0, 0.0, 3.0, 1000, 0.0, 0.0, 3, 0.1, 0.2),
+    ("multibrot4", 4, 0.0, 0.0, 3.0, 1000, 0.0, 0.0, 4, 0.1, 0.2),
+    ("multibrot5", 4, 0.0, 0.0, 3.0, 600, 0.0, 0.0, 5, 0.1, 0.2),
+    ("multibrot2k", 4, -0.5, 0.0, 3.0, 800, 0.0, 0.0, 2, 0.25, 1.0),
+]
+FP64_W, FP64_H = 128, 72
+
+
+def fp64_grid(cx, cy, w):
+    """Plain IEEE grid: x = x_min + i*dx, y = y_max - j*dy (no contraction)."""
+    h = w * FP64_H / FP64_W
+    dx = w / (FP64_W - 1)
+    dy = h / (FP64_H - 1)
+    x_min = cx - w * 0.5
+    y_max = cy + h * 0.5
+    i = np.arange(FP64_W, dtype=np.float64)
+    j = np.arange(FP64_H, dtype=np.float64)
+    xs = x_min + i * dx
+    ys = y_max - j * dy
+    return xs, ys
+
+
+def gen_fp64():
+    out = {}
+    meta = []
+    f = R.ck.cpu_compute_fp64_sample
+    for (name, ft, cx, cy, w, mi, jx, jy, n, kr, ki) in FP64_CASES:
+        xs, ys = fp64_grid(cx, cy, w)
+        s = np.empty((FP64_H, FP64_W), np.float32)
+        for jj in range(FP64_H):
+            for ii in range(FP64_W):
+                s[jj, ii] = f(float(xs[ii]), float(ys[jj]), mi, ft, jx, jy, n, kr, ki, INV_LN2, LN_BAIL)
+        out[name + "__s"] = s
+        out[name + "__x"] = xs
+        out[name + "__y"] = ys
+        meta.append(dict(name=name, fractal_type=ft, max_iter=mi, julia_cx=jx, julia_cy=jy,
+                         gen_n=n, gen_kr=kr, gen_ki=ki))
+    save("fp64_samples.npz", meta=json.dumps(meta), **out)
+
+
+# ---------------------------------------------------------------------------
+# Full-frame FP64 renders through render_frame_cpu
+# ---------------------------------------------------------------------------
+RENDER1_CASES = [
+    # name, W, H, max_iter, cx, cy, width, scheme, factor, offset, density, contrast, type, jx, jy, n, kr, ki
+    ("cfg1_hist", 640, 360, 1000, "-0.65", "0.0", "4.0", 11, 1, 0.0, 1.0, 1.0, 0, 0.0, 0.0, 3, 0.25, 1.0),
+    ("cfg1_s0", 640, 360, 1000, "-0.65", "0.0", "4.0", 0, 1, 0.0, 1.0, 1.0, 0, 0.0, 0.0, 3, 0.25, 1.0),
+    ("ssaa2_s0", 160, 90, 500, "-0.7436", "0.1318", "0.02", 0, 2, 0.0, 1.0, 1.0, 0, 0.0, 0.0, 3, 0.25, 1.0),
+    ("ssaa2_hist", 160, 90, 500, "-0.7436", "0.1318", "0.02", 11, 2, 0.1, 1.3, 0.8, 0, 0.0, 0.0, 3, 0.25, 1.0),
+    ("ssaa3_julia", 96, 54, 400, "0.0", "0.0", "3.0", 6, 3, 0.2, 1.0, 1.0, 2, -0.8, 0.156, 3, 0.25, 1.0),
+] + [
+    (f"scheme{sid}", 96, 54, 600, "-0.7436", "0.1318", "0.05", sid, 1, 0.15 * (sid % 3), 1.0 + 0.1 * sid,
+     1.0 if sid % 2 == 0 else 1.4, 0, 0.0, 0.0, 3, 0.25, 1.0)
+    for sid in range(1, 11)
+] + [
+    ("ship_s2", 96, 54, 300, "-1.75", "0.03", "0.18", 2, 1, 0.0, 1.0, 1.0, 1, 0.0, 0.0, 3, 0.25, 1.0),
+    ("multibrot_s5", 96, 54, 300, "0.0", "0.0", "3.0", 5, 2, 0.3, 0.7, 1.2, 4, 0.0, 0.0, 3, 0.1, 0.2),
+    ("shipjulia_hist", 96, 54, 300, "0.0", "0.0", "4.0", 11, 1, 0.0, 1.0, 1.0, 3, -1.755, 0.03, 3, 0.25, 1.0),
+]
+
+
+def gen_render1():
+    out = {}
+    meta = []
+    for c in RENDER1_CASES:
+        (name, W, H, mi, cx, cy, w, sid, fac, off, den, con, ft, jx, jy, n, kr, ki) = c
+        it = np.zeros((H, W), np.float32)
+        t0 = time.time()
+        rgb = R.engine.render_frame_cpu(
+            W, H, mi, Decimal(cx), Decimal(cy), Decimal(w), "synthetic",
+            ssaa_factor=fac, edge_threshold=0.35, color_scheme_id=sid,
+            precision_mode="1e-12 (FP64)", fractal_type=ft, julia_cx=jx, julia_cy=jy,
+            bbsa_tol=1e-4, bbsa_order=4, glitch_mode="Off (Single-Ref)",
+            gen_n=n, gen_kr=kr, gen_ki=ki, cpu_threads=8, palette_offset=off,
+            color_density=den, color_contrast=con, h_iter_buf=it)
+        print(f"  {name}: {time.time() - t0:.2f}s")
+        out[name + "__rgb"] = rgb
+        out[name + "__iter"] = it
+        meta.append(dict(name=name, W=W, H=H, max_iter=mi, cx=cx, cy=cy, width=w, scheme=sid,
+                         factor=fac, offset=off, density=den, contrast=con, fractal_type=ft,
+                         julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki))
+    save("render_fp64.npz", meta=json.dumps(meta), **out)
+
+
+def config2_centre(seed=SEED):
+    """Config-2 centre: (-1.75 + 1e-17*u1, 0.03 + 1e-17*u2), u ~ U(-1, 1) from the seed."""
+    rng = np.random.default_rng(seed)
+    u1, u2 = rng.uniform(-1.0, 1.0, size=2)
+    cx = Decimal("-1.75") + Decimal(repr(float(u1))) * Decimal("1e-17")
+    cy = Decimal("0.03") + Decimal(repr(float(u2))) * Decimal("1e-17")
+    return str(cx), str(cy)
+
+
+def render2_cases():
+    cx2, cy2 = config2_centre()
+    return [
+        # Burning Ship DD at 1e-20, 2x adaptive SSAA (config 2 at quarter size).
+        ("cfg2_quarter", 320, 180, 20000, cx2, cy2, "1e-20", 0, 2, 0.0, 1.0, 1.0, 1, 0.0, 0.0, 3, 0.25, 1.0),
+        ("cfg2_hist", 160, 90, 20000, cx2, cy2, "1e-20", 11, 2, 0.0, 1.0, 1.0, 1, 0.0, 0.0, 3, 0.25, 1.0),
+        ("dd_mandel", 64, 36, 3000, "-0.10109636384562", "0.95628651080914", "4e-18", 0, 1,
+         0.0, 1.0, 1.0, 0, 0.0, 0.0, 3, 0.25, 1.0),
+        ("dd_mandel_ssaa", 48, 27, 3000, "-0.10109636384562", "0.95628651080914", "3e-17", 6, 2,
+         0.1, 1.0, 1.0, 0, 0.0, 0.0, 3, 0.25, 1.0),
+        ("dd_julia", 64, 36, 2000, "0.123456789012345678", "0.0987654321098765", "1e-16", 0, 1,
+         0.0, 1.0, 1.0, 2, -0.8, 0.156, 3, 0.25, 1.0),
+        ("dd_shipjulia", 64, 36, 2000, "0.1", "0.2", "1e-15", 0, 1, 0.0, 1.0, 1.0, 3, -1.755, 0.03,
+         3, 0.25, 1.0),
+        ("dd_multibrot3", 64, 36, 2000, "-0.5641", "0.6612", "1e-14", 0, 1, 0.0, 1.0, 1.0, 4, 0.0, 0.0,
+         3, 0.1, 0.2),
+        ("dd_multibrot5", 48, 27, 1000, "0.7", "0.2", "1e-13", 11, 1, 0.0, 1.0, 1.0, 4, 0.0, 0.0,
+         5, 0.1, 0.2),
+    ]
+
+
+def gen_render2():
+    out = {}
+    meta = []
+    for c in render2_cases():
+        (name, W, H, mi, cx, cy, w, sid, fac, off, den, con, ft, jx, jy, n, kr, ki) = c
+        it = np.zeros((H, W), np.float32)
+        t0 = time.time()
+        rgb = R.engine.render_frame_cpu(
+            W, H, mi, Decimal(cx), Decimal(cy), Decimal(w), "synthetic",
+            ssaa_factor=fac, edge_threshold=0.35, color_scheme_id=sid,
+            precision_mode="1e-24 (DD)", fractal_type=ft, julia_cx=jx, julia_cy=jy,
+            bbsa_tol=1e-4, bbsa_order=4, glitch_mode="Off (Single-Ref)",
+            gen_n=n, gen_kr=kr, gen_ki=ki, cpu_threads=8, palette_offset=off,
+            color_density=den, color_contrast=con, h_iter_buf=it)
+        print(f"  {name}: {time.time() - t0:.2f}s  escaped {np.mean(it >= 0):.3f}")
+        out[name + "__rgb"] = rgb
+        out[name + "__iter"] = it
+        meta.append(dict(name=name, W=W, H=H, max_iter=mi, cx=cx, cy=cy, width=w, scheme=sid,
+                         factor=fac, offset=off, density=den, contrast=con, fractal_type=ft,
+                         julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki))
+    save("render_dd.npz", meta=json.dumps(meta), **out)
+
+
+SECTIONS = {"fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2}
+
+if __name__ == "__main__":
+    wanted = sys.argv[1:] or list(SECTIONS)
+    for s in wanted:
+        print(f"[{s}]")
+        SECTIONS[s]()
