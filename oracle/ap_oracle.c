@@ -590,10 +590,288 @@ static Sample dd_sample_at(const ApFrameParams* p, double sub_i, double sub_j) {
     return dd_sample(cx, cy, p);
 }
 
+/* ------------------------------------------------------------------------- */
+/* FP64-delta perturbation: cpu_kernels.py:374-602 (CPU) and                  */
+/* cuda_kernels.py:422-590 / :594-815 (CUDA, plain and BLA variants).         */
+/* ------------------------------------------------------------------------- */
+static void c_mul(double ar, double ai, double br, double bi, double* r, double* i) {
+    *r = ar * br - ai * bi;
+    *i = ar * bi + ai * br;
+}
+
+/* Horner series of cpu_kernels.py:206-223 (u = dc / r). */
+static void eval_bbsa(const double* c, double ux, double uy, double* zx, double* zy) {
+    int eight = 0;
+    for (int q = 8; q < 16; q++) eight |= (c[q] != 0.0);
+    double tr, ti;
+    if (eight) {
+        c_mul(ux, uy, c[14], c[15], &tr, &ti);
+        for (int t = 6; t >= 0; t--) c_mul(ux, uy, c[2 * t] + tr, c[2 * t + 1] + ti, &tr, &ti);
+    } else {
+        c_mul(ux, uy, c[6], c[7], &tr, &ti);
+        for (int t = 2; t >= 0; t--) c_mul(ux, uy, c[2 * t] + tr, c[2 * t + 1] + ti, &tr, &ti);
+    }
+    *zx = tr;
+    *zy = ti;
+}
+
+static Sample glitch_at(int k) {
+    Sample o;
+    o.s = (float)k;
+    o.s64 = (double)k;
+    o.k = k;
+    o.glitch = 1;
+    return o;
+}
+
 static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
                              double sub_j) {
-    (void)p; (void)b; (void)sub_i; (void)sub_j;
-    return interior();
+    const int ft = p->fractal_type, cpu = p->arith == AP_ARITH_REF_CPU;
+    const int julia = (ft == 2 || ft == 3);
+    const int ref_len = p->ref_len, max_iter = p->max_iter;
+    const double* re = b->ref_re;
+    const double* im = b->ref_im;
+    const int esc_glitch = (p->flags & AP_FLAG_ESCAPE_GLITCH) != 0;
+    const int nan_guard = (p->flags & AP_FLAG_NAN_GUARD) != 0;
+    const int strict = p->strict_glitch > 0;
+    const double dcy = (p->ref_py - sub_j) * p->dy_hi;
+    const double dcx = (sub_i - p->ref_px) * p->dx_hi;
+    double dzx, dzy;
+    int k;
+    if (p->bbsa_skip > 0 && (ft == 0 || ft == 2 || ft == 4) &&
+        (dcx * p->bbsa_inv_r) * (dcx * p->bbsa_inv_r) + (dcy * p->bbsa_inv_r) * (dcy * p->bbsa_inv_r) <= 1.0) {
+        eval_bbsa(p->bbsa, dcx * p->bbsa_inv_r, dcy * p->bbsa_inv_r, &dzx, &dzy);
+        k = p->bbsa_skip;
+    } else {
+        dzx = julia ? dcx : 0.0;
+        dzy = julia ? dcy : 0.0;
+        k = 0;
+    }
+    const double dcpx = julia ? 0.0 : dcx, dcpy = julia ? 0.0 : dcy;
+    int glitch = 0;
+    const int levels = p->bla_levels;
+    const int has_bla = levels > 1 && b->bla != NULL && (ft == 0 || ft == 2 || ft == 4);
+    const double inv_ln = inv_ln_for(ft, p->gen_n);
+    const size_t L = (size_t)ref_len;
+
+    while (k < ref_len) {
+        const double rx = re[k], ry = im[k];
+        const double zx = rx + dzx, zy = ry + dzy;
+        const double mag2 = zx * zx + zy * zy;
+        if (mag2 > BAILOUT) {
+            if (esc_glitch && strict && k > 15 && (rx * rx + ry * ry) < 4.0) glitch = 1;
+            Sample o = escaped(k, mag2, inv_ln);
+            o.glitch = glitch;
+            return o;
+        }
+        if (strict && k > 15) {
+            const double r_mag2 = rx * rx + ry * ry;
+            if (mag2 < 1e-6 * r_mag2 && r_mag2 > 1e-8) glitch = 1;
+        }
+        if (has_bla && k < ref_len - 1) {
+            const double dz_mag2 = dzx * dzx + dzy * dzy;
+            if (dz_mag2 < b->bla[((size_t)0 * L + k) * 5 + 4]) {
+                int best = 0, max_d = levels - 1;
+                if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) max_d = max_d > 8 ? 8 : max_d;
+                for (int d = max_d; d > 0; d--) {
+                    if (k + (1 << d) < ref_len && dz_mag2 < b->bla[((size_t)d * L + k) * 5 + 4]) {
+                        best = d;
+                        break;
+                    }
+                }
+                const double* e = b->bla + ((size_t)best * L + k) * 5;
+                const double ar = e[0], ai = e[1], br = e[2], bi = e[3];
+                double nx, ny;
+                if (cpu) {
+                    nx = (ar * dzx - ai * dzy) + (br * dcpx - bi * dcpy);
+                    ny = (ar * dzy + ai * dzx) + (br * dcpy + bi * dcpx);
+                } else {
+                    nx = fma(ar, dzx, fma(-ai, dzy, fma(br, dcpx, -bi * dcpy)));
+                    ny = fma(ar, dzy, fma(ai, dzx, fma(br, dcpy, bi * dcpx)));
+                }
+                dzx = nx;
+                dzy = ny;
+                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) return glitch_at(k);
+                k += 1 << best;
+                continue;
+            }
+        }
+        if (ft == 0 || ft == 2) {
+            double nx, ny;
+            if (cpu) {
+                nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+                ny = 2.0 * ((rx + dzx) * dzy + ry * dzx) + dcpy;
+            } else {
+                nx = fma(2.0 * rx + dzx, dzx, fma(-(2.0 * ry + dzy), dzy, dcpx));
+                ny = fma(2.0, fma(rx + dzx, dzy, ry * dzx), dcpy);
+            }
+            dzx = nx;
+            dzy = ny;
+        } else if (ft == 1 || ft == 3) {
+            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+            const double ddx = (rx + dzx) * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+            const double ddy = (ry + dzy) * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcpy;
+            dzx = nx;
+        } else {
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p->gen_n - 1; t++) {
+                double t1r, t1i, t2r, t2i;
+                c_mul(pr, pi, rx, ry, &t1r, &t1i);
+                c_mul(pr + qr, pi + qi, dzx, dzy, &t2r, &t2i);
+                pr = t1r + t2r;
+                pi = t1i + t2i;
+                c_mul(qr, qi, rx, ry, &qr, &qi);
+            }
+            double kr, ki;
+            c_mul(p->gen_kr, p->gen_ki, dzx, dzy, &kr, &ki);
+            dzx = pr + kr + dcpx;
+            dzy = pi + ki + dcpy;
+        }
+        k++;
+    }
+
+    /* Stage 2: the reference escaped (or the orbit ended); iterate z directly. */
+    double zx = re[ref_len] + dzx, zy = im[ref_len] + dzy;
+    const double cx = julia ? p->julia_cx_hi : p->ref_cx + dcx;
+    const double cy = julia ? p->julia_cy_hi : p->ref_cy + dcy;
+    if (ref_len < max_iter) glitch = 1;
+    while (k < max_iter) {
+        const double zx2 = zx * zx, zy2 = zy * zy;
+        const double mag2 = zx2 + zy2;
+        if (nan_guard && (isnan(mag2) || isinf(mag2))) return glitch_at(k);
+        if (mag2 > BAILOUT) {
+            Sample o = escaped(k, mag2, inv_ln);
+            o.glitch = glitch;
+            return o;
+        }
+        if (ft == 0 || ft == 2) {
+            zy = 2.0 * zx * zy + cy;
+            zx = zx2 - zy2 + cx;
+        } else if (ft == 1 || ft == 3) {
+            zy = 2.0 * fabs(zx) * fabs(zy) - cy;
+            zx = zx2 - zy2 + cx;
+        } else {
+            double zr = zx, zi = zy;
+            for (int t = 0; t < p->gen_n - 1; t++) {
+                const double nr = zr * zx - zi * zy, ni = zr * zy + zi * zx;
+                zr = nr;
+                zi = ni;
+            }
+            const double kzr = p->gen_kr * zx - p->gen_ki * zy;
+            const double kzi = p->gen_kr * zy + p->gen_ki * zx;
+            zx = zr + kzr + cx;
+            zy = zi + kzi + cy;
+        }
+        k++;
+    }
+    Sample o = interior();
+    o.glitch = glitch;
+    return o;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Chained BLA table: _jit_build_bla_table (high_precision.py:1101-1238).     */
+/* The reference builds it with a fastmath Numba kernel; the fused forms      */
+/* below are the ones its compiled x86-64 code evaluates.                     */
+/* ------------------------------------------------------------------------- */
+APO_EXPORT int apo_build_bla(const double* re, const double* im, int ref_len, int ft, double tol,
+                             int levels, int gen_n, double kr, double ki, double* T) {
+    const size_t L = (size_t)ref_len;
+    memset(T, 0, sizeof(double) * (size_t)levels * L * 5);
+    if (!(ft == 0 || ft == 2 || ft == 4) || ref_len < 4 || tol <= 0.0) return AP_OK;
+    const double tol_sq_4 = (tol * tol) * 4.0;
+    for (int k = 0; k < ref_len - 1; k++) {
+        const double rx = re[k], ry = im[k];
+        double* e = T + (size_t)k * 5;
+        const double r_mag2 = fma(ry, ry, rx * rx);
+        if (ft == 0 || ft == 2) {
+            e[0] = 2.0 * rx;
+            e[1] = 2.0 * ry;
+            e[2] = 1.0;
+            e[3] = 0.0;
+            double r_sq = tol_sq_4 * r_mag2;
+            r_sq = 0.25 < r_sq ? 0.25 : r_sq;
+            if (k == 0 && r_mag2 < 1e-14) r_sq = 0.0;
+            e[4] = r_sq;
+        } else {
+            /* Multibrot: A = n R^(n-1) + K, radius from the quadratic bound (high_precision.py:1126-1175). */
+            double zr = 1.0, zi = 0.0;
+            for (int t = 0; t < gen_n - 1; t++) {
+                const double nr = fma(zr, rx, -(zi * ry)), ni = fma(zr, ry, zi * rx);
+                zr = nr;
+                zi = ni;
+            }
+            const double ar = fma((double)gen_n, zr, kr), ai = fma((double)gen_n, zi, ki);
+            e[0] = ar;
+            e[1] = ai;
+            e[2] = 1.0;
+            e[3] = 0.0;
+            const double tol_a = sqrt(fma(ai, ai, ar * ar)) * tol;
+            if (!(tol_a > 0.0)) {
+                e[4] = 0.0;
+            } else {
+                const double r_mag = sqrt(r_mag2);
+                double r_pow;
+                if (gen_n == 2) r_pow = 1.0;
+                else if (gen_n == 3) r_pow = r_mag;
+                else if (gen_n == 4) r_pow = r_mag2;
+                else r_pow = pow(r_mag, (double)(gen_n - 2));
+                const double bq = r_pow * (0.25 * (double)(gen_n * (gen_n - 1)));
+                const double denom = sqrt(fma(bq, bq, tol_a)) + bq;
+                double x = denom > 1e-300 ? tol_a / denom : 0.0;
+                if (gen_n > 3) {
+                    const double x_max = pow(tol_a, 1.0 / (double)(gen_n - 1));
+                    if (x > x_max) x = x_max;
+                }
+                x = 0.5 < x ? 0.5 : x;
+                double r_sq = x * x;
+                if (k == 0 && r_mag2 < 1e-14) r_sq = 0.0;
+                e[4] = r_sq;
+            }
+        }
+    }
+    int step = 1;
+    for (int d = 1; d < levels; d++) {
+        const int step_next = step * 2;
+        for (int k = 0; k < ref_len - step_next; k++) {
+            const double* e1 = T + ((size_t)(d - 1) * L + k) * 5;
+            const double* e2 = T + ((size_t)(d - 1) * L + k + step) * 5;
+            double* o = T + ((size_t)d * L + k) * 5;
+            const double r1 = e1[4], r2 = e2[4];
+            if (!(r1 > 0.0 && r2 > 0.0)) continue;
+            const double a1r = e1[0], a1i = e1[1], b1r = e1[2], b1i = e1[3];
+            const double a2r = e2[0], a2i = e2[1], b2r = e2[2], b2i = e2[3];
+            const double ar = fma(a2r, a1r, -(a2i * a1i));
+            const double ai = fma(a2i, a1r, a2r * a1i);
+            const double a_mag2 = fma(ar, ar, ai * ai);
+            if (a_mag2 > 1e150) {
+                o[0] = o[1] = o[2] = o[3] = o[4] = 0.0;
+                continue;
+            }
+            const double br = fma(a2r, b1r, -(a2i * b1i)) + b2r;
+            const double bi = fma(a2i, b1r, fma(a2r, b1i, b2i));
+            const double b_mag2 = fma(br, br, bi * bi);
+            if (b_mag2 > 1e150) {
+                o[0] = o[1] = o[2] = o[3] = o[4] = 0.0;
+                continue;
+            }
+            o[0] = ar;
+            o[1] = ai;
+            o[2] = br;
+            o[3] = bi;
+            const double a1_mag2 = fma(a1i, a1i, a1r * a1r);
+            double rc = r1;
+            if (a1_mag2 > 1e-300) {
+                const double r2s = (0.25 * r2) / a1_mag2;
+                rc = r1 < r2s ? r1 : r2s;
+            }
+            o[4] = rc <= 0.0 ? 0.0 : (rc > 0.25 ? 0.25 : rc);
+        }
+        step = step_next;
+    }
+    return AP_OK;
 }
 
 /* ------------------------------------------------------------------------- */
@@ -717,3 +995,33 @@ APO_EXPORT int apo_fp64_grid(const ApFrameParams* p, const double* xs, const dou
 
 /* Number of worker threads (0 = all online cores). */
 APO_EXPORT void apo_set_threads(int n) { g_threads = n < 0 ? 0 : n; }
+
+/* Per-sample perturbation values at explicit sub-sample coordinates. */
+typedef struct {
+    const ApFrameParams* p;
+    const ApFrameBuffers* b;
+    const double* xs;
+    const double* ys;
+    int W;
+    float* s32;
+    uint8_t* glitch;
+    int32_t* kmap;
+} PertGridCtx;
+
+static void pert_grid_row(void* vctx, int j) {
+    const PertGridCtx* c = (const PertGridCtx*)vctx;
+    for (int i = 0; i < c->W; i++) {
+        Sample o = pert_sample_at(c->p, c->b, c->xs[i], c->ys[j]);
+        size_t idx = (size_t)j * c->W + i;
+        c->s32[idx] = o.s;
+        c->glitch[idx] = (uint8_t)(o.glitch > 0);
+        if (c->kmap) c->kmap[idx] = o.k;
+    }
+}
+
+APO_EXPORT int apo_pert_grid(const ApFrameParams* p, const ApFrameBuffers* b, const double* xs,
+                             const double* ys, int W, int H, float* s32, uint8_t* glitch, int32_t* kmap) {
+    PertGridCtx c = {p, b, xs, ys, W, s32, glitch, kmap};
+    parallel_rows(H, pert_grid_row, &c);
+    return AP_OK;
+}

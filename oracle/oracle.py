@@ -38,6 +38,10 @@ def lib():
         L.apo_fp64_grid.argtypes = [P, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                     C.c_void_p, C.c_void_p, C.c_void_p]
         L.apo_set_threads.argtypes = [C.c_int]
+        L.apo_pert_grid.argtypes = [P, B, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                    C.c_void_p, C.c_void_p]
+        L.apo_build_bla.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
+                                    C.c_int, C.c_double, C.c_double, C.c_void_p]
         _lib = L
     return _lib
 
@@ -65,6 +69,35 @@ def fp64_grid(params, xs, ys):
     _check(lib().apo_fp64_grid(C.byref(params), ptr(xs), ptr(ys), W, H, ptr(s32), ptr(s64), ptr(k)),
            "fp64_grid")
     return s32, s64, k
+
+
+def pert_grid(params, ref_re, ref_im, bla, xs, ys):
+    """Perturbation samples at sub-sample coordinates xs (columns) x ys (rows)."""
+    re = np.ascontiguousarray(ref_re, np.float64)
+    im = np.ascontiguousarray(ref_im, np.float64)
+    xs = np.ascontiguousarray(xs, np.float64)
+    ys = np.ascontiguousarray(ys, np.float64)
+    b = abi.ApFrameBuffers()
+    b.ref_re, b.ref_im = ptr(re), ptr(im)
+    if bla is not None:
+        bla = np.ascontiguousarray(bla, np.float64)
+        b.bla = ptr(bla)
+    H, W = len(ys), len(xs)
+    s = np.empty((H, W), np.float32)
+    g = np.empty((H, W), np.uint8)
+    k = np.empty((H, W), np.int32)
+    _check(lib().apo_pert_grid(C.byref(params), C.byref(b), ptr(xs), ptr(ys), W, H, ptr(s), ptr(g),
+                               ptr(k)), "pert_grid")
+    return s, g
+
+
+def build_bla(ref_re, ref_im, ref_len, fractal_type, tol, levels, gen_n, gen_kr, gen_ki):
+    T = np.zeros((levels, ref_len, 5), np.float64)
+    _check(lib().apo_build_bla(ptr(np.ascontiguousarray(ref_re, np.float64)),
+                               ptr(np.ascontiguousarray(ref_im, np.float64)), int(ref_len),
+                               int(fractal_type), float(tol), int(levels), int(gen_n), float(gen_kr),
+                               float(gen_ki), ptr(T)), "build_bla")
+    return T
 
 
 class Frame:

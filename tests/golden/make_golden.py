@@ -196,7 +196,126 @@ def gen_render2():
     save("render_dd.npz", meta=json.dumps(meta), **out)
 
 
-SECTIONS = {"fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2}
+# ---------------------------------------------------------------------------
+# Deep-zoom workloads (config 3): preset centre extended with seeded digits
+# ---------------------------------------------------------------------------
+def config3_centre(seed=SEED, digits=600):
+    """The 1e-160 preset centre (presets.json:154-157) extended to `digits` decimals."""
+    with open(os.path.join(ref_shim.REF_ROOT, "presets.json")) as f:
+        data = json.load(f)
+    marks = data.get("bookmarks", data) if isinstance(data, dict) else data
+    e = next(b for b in marks if "1e-160" in b.get("name", "") and b.get("fractal_type") == 0)
+    rng = np.random.default_rng(seed)
+    out = []
+    for key in ("center_x", "center_y"):
+        v = e[key]
+        frac = v.split(".")[1]
+        extra = "".join(str(d) for d in rng.integers(0, 10, size=max(0, digits - len(frac))))
+        out.append(v + extra)
+    return out[0], out[1]
+
+
+def write_workloads():
+    cx3, cy3 = config3_centre()
+    cx2, cy2 = config2_centre()
+    wl = {"seed": SEED, "config2_centre": [cx2, cy2], "config3_centre": [cx3, cy3]}
+    with open(os.path.join(HERE, "workloads.json"), "w") as f:
+        json.dump(wl, f, indent=1)
+    print("  wrote workloads.json")
+    return wl
+
+
+def deep_point(ft, cx, cy, w, jx=0.0, jy=0.0, n=3, kr=0.25, ki=1.0, levels=6, grid=96, mi=3000):
+    """Deterministic boundary search: zoom x40 per level toward the escaped grid point
+    with the largest escape value (reference FP64 evaluator)."""
+    f = R.ck.cpu_compute_fp64_sample
+    for _ in range(levels):
+        best = (-1.0, cx, cy)
+        for jj in range(grid):
+            y = cy + w * (0.5 - jj / (grid - 1))
+            for ii in range(grid):
+                x = cx + w * (ii / (grid - 1) - 0.5)
+                v = f(x, y, mi, ft, jx, jy, n, kr, ki, INV_LN2, LN_BAIL)
+                if v > best[0]:
+                    best = (float(v), x, y)
+        _, cx, cy = best
+        w /= 40.0
+    return repr(cx), repr(cy)
+
+
+PERT_SPECS = [
+    # name, fractal_type, start cx, cy, width, W, H, max_iter, stride, jx, jy, n, kr, ki
+    ("ship", 1, -1.75, -0.03, 0.2, 640, 360, 6000, 10, 0.0, 0.0, 3, 0.25, 1.0),
+    ("julia", 2, 0.0, 0.0, 3.0, 640, 360, 6000, 10, -0.8, 0.156, 3, 0.25, 1.0),
+    ("ship_julia", 3, 0.0, 0.0, 4.0, 640, 360, 6000, 10, -1.755, 0.03, 3, 0.25, 1.0),
+    ("multibrot3", 4, 0.0, 0.0, 3.0, 640, 360, 6000, 10, 0.0, 0.0, 3, 0.1, 0.2),
+    ("multibrot4", 4, 0.0, 0.0, 3.0, 320, 180, 6000, 8, 0.0, 0.0, 4, 0.1, 0.2),
+]
+
+
+def pert_cases():
+    cases = [("cfg3", 0, None, None, "1e-160", 1920, 1080, 200000, 40, 0.0, 0.0, 3, 0.25, 1.0)]
+    for (name, ft, cx, cy, w, W, H, mi, stride, jx, jy, n, kr, ki) in PERT_SPECS:
+        px, py = deep_point(ft, cx, cy, w, jx, jy, n, kr, ki)
+        cases.append((name, ft, px, py, "2e-14", W, H, mi, stride, jx, jy, n, kr, ki))
+    return cases
+
+
+def gen_pert():
+    wl = write_workloads()
+    hp, ck, cfg = R.hp, R.ck, R.config
+    out = {}
+    meta = []
+    for (name, ft, cx, cy, w, W, H, mi, stride, jx, jy, n, kr, ki) in pert_cases():
+        if cx is None:
+            cx, cy = wl["config3_centre"]
+        cfg.ensure_decimal_precision(Decimal(w))
+        pw = Decimal(w)
+        ph = pw * (Decimal(H) / Decimal(W))
+        hp.clear_reference_orbit_cache()
+        t0 = time.time()
+        bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
+            Decimal(cx), Decimal(cy), pw, ph, mi, W, H, fractal_type=ft, julia_cx=jx, julia_cy=jy,
+            gen_n=n, gen_kr=kr, gen_ki=ki, is_floatexp=False)
+        t_orbit = time.time() - t0
+        dx = float(pw / Decimal(max(1, W - 1)))
+        dy = float(ph / Decimal(max(1, H - 1)))
+        ref_px = float(W - 1) * float(bu)
+        ref_py = float(H - 1) * float(bv)
+        tab = hp.build_bla_table(re, im, rl, fractal_type=ft, tol=1e-6, gen_n=n, gen_kr=kr, gen_ki=ki)
+        zero16 = (0.0,) * 16
+        si = np.arange(0, W, stride, dtype=np.float64)
+        sj = np.arange(0, H, stride, dtype=np.float64)
+        res = {}
+        for variant, table, strict in (("plain", np.zeros((1, 1, 1)), 0), ("bla", tab, 1)):
+            s = np.empty((len(sj), len(si)), np.float32)
+            g = np.empty((len(sj), len(si)), np.uint8)
+            for a, jj in enumerate(sj):
+                for b, ii in enumerate(si):
+                    sv, gl = ck.cpu_compute_perturbation_sample(
+                        re, im, rl, mi, ref_px, ref_py, float(ii), float(jj), dx, dy,
+                        float(bcx), float(bcy), ft, float(jx), float(jy), 0, 1.0, *zero16,
+                        n, kr, ki, strict, INV_LN2, LN_BAIL, bla_table=table)
+                    s[a, b] = sv
+                    g[a, b] = gl
+            res[variant] = (s, g)
+        print(f"  {name}: ref_len {rl} at u,v=({bu},{bv}) orbit {t_orbit:.1f}s total {time.time()-t0:.1f}s "
+              f"glitched(bla) {res['bla'][1].mean():.3f}")
+        out[name + "__re"] = re[:rl + 1]
+        out[name + "__im"] = im[:rl + 1]
+        for variant in res:
+            out[f"{name}__{variant}_s"] = res[variant][0]
+            out[f"{name}__{variant}_g"] = res[variant][1]
+        out[name + "__bla_sha256"] = np.frombuffer(
+            hashlib.sha256(np.ascontiguousarray(tab).tobytes()).digest(), np.uint8)
+        meta.append(dict(name=name, fractal_type=ft, cx=cx, cy=cy, width=w, W=W, H=H, max_iter=mi,
+                         stride=stride, julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki,
+                         ref_cx=str(bcx), ref_cy=str(bcy), u=bu, v=bv, ref_len=int(rl),
+                         bla_shape=list(tab.shape), dx=dx, dy=dy, ref_px=ref_px, ref_py=ref_py))
+    save("pert_samples.npz", meta=json.dumps(meta), **out)
+
+
+SECTIONS = {"fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert}
 
 if __name__ == "__main__":
     wanted = sys.argv[1:] or list(SECTIONS)
