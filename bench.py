@@ -125,12 +125,13 @@ def fma_peak_tflops(precision, stream_h, torch):
     flops = C.c_double()
     iters = 4096 if precision == 64 else 16384
     best = 0.0
+    st = torch.cuda.current_stream()
     for rep in range(6):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
+        a.record(st)
         _lib.check(L.ap_fma_peak_launch(precision, blocks, iters, C.c_void_p(scratch.data_ptr()),
-                                        C.byref(flops), stream_h), "ap_fma_peak_launch")
-        b.record()
+                                        C.byref(flops), C.c_void_p(st.cuda_stream)), "ap_fma_peak_launch")
+        b.record(st)
         b.synchronize()
         if rep > 0:
             best = max(best, flops.value / (a.elapsed_time(b) * 1e-3) / 1e12)

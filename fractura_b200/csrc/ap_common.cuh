@@ -86,8 +86,14 @@ __device__ __forceinline__ double tri_wave(double phase) {
     return 1.0 - fabs((phase < 0.0 ? phase + 2.0 : phase) - 1.0);
 }
 
+// sqrt of the smooth value: the CPU reference holds it as float32 and Numba
+// evaluates math.sqrt(float32) in float32; the CUDA reference holds float64.
+__device__ __forceinline__ double sqrt_s(double s, bool f32) {
+    return f32 ? (double)__fsqrt_rn((float)s) : sqrt(s);
+}
+
 static __device__ __noinline__ double palette_norm(double s, int scheme, double off, double density,
-                                            double contrast) {
+                                                   double contrast, bool f32) {
     const double dens = density <= 0.0 ? 1.0 : density;
     const double cont = contrast <= 0.0 ? 1.0 : contrast;
     const double kTwoPi = 6.28318530718;
@@ -95,21 +101,21 @@ static __device__ __noinline__ double palette_norm(double s, int scheme, double 
     case 1:
         return tri_wave(py_mod(log(s * cont + 1.0) * (0.45 * dens) + off * 2.0, 2.0));
     case 2: {
-        const double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        const double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.125 * dens) + off * 2.0, 2.0));
         const double k = 4.0 * cont;
         const double td = tanh(0.5 * k);
         const double scale = fabs(td) > 1e-7 ? 0.5 / td : 0.5186574;
         return 0.5 + tanh((tri - 0.5) * k) * scale;
     }
     case 3: {
-        const double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        const double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.125 * dens) + off * 2.0, 2.0));
         const double k = 3.0 * cont;
         const double ed = exp(k) - 1.0;
         const double scale = fabs(ed) > 1e-7 ? 1.0 / ed : 0.0523957;
         return (exp(k * tri) - 1.0) * scale;
     }
     case 4: {
-        const double tri = tri_wave(py_mod(sqrt(s) * (0.5 * dens) + off * 2.0, 2.0));
+        const double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.5 * dens) + off * 2.0, 2.0));
         return cont != 1.0 ? pow(tri, cont) : tri;
     }
     case 5: {
@@ -132,7 +138,7 @@ static __device__ __noinline__ double palette_norm(double s, int scheme, double 
         return 0.5 + scale * wave;
     }
     case 8: {
-        double tri = tri_wave(py_mod(sqrt(s) * (0.1 * dens) + off * 2.0, 2.0));
+        double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.1 * dens) + off * 2.0, 2.0));
         if (cont != 1.0) tri = pow(tri, cont);
         const double t2 = tri * tri;
         return t2 * tri * (tri * (tri * 6.0 - 15.0) + 10.0);
@@ -146,7 +152,7 @@ static __device__ __noinline__ double palette_norm(double s, int scheme, double 
         return raw >= 0.0 ? raw : raw + 1.0;
     }
     default: {  // scheme 0 and every id above 10
-        const double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        const double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.125 * dens) + off * 2.0, 2.0));
         return cont != 1.0 ? pow(tri, cont) : tri;
     }
     }
@@ -211,7 +217,7 @@ __device__ __forceinline__ void colour_of(const ApFrameParams& p, const float* _
     const double norm = hist ? cdf_norm(s, p.max_iter, cdf, p.num_bins, p.palette_offset,
                                         p.color_density, p.color_contrast)
                              : palette_norm(s, p.scheme_id, p.palette_offset, p.color_density,
-                                            p.color_contrast);
+                                            p.color_contrast, p.arith == AP_ARITH_REF_CPU);
     lut_lerp(lut, norm, r, g, b);
 }
 

@@ -1,0 +1,306 @@
+"""Perturbation tiers of render_frame: orbit, BLA table, passes and rebasing.
+
+Host orchestration of math_core/engine.py:1807-2113 (FP64 deltas) and
+:1718-1806 (FloatExp deltas): the reference orbit comes from
+high_precision.find_optimal_reference_orbit (host, Decimal), is copied to
+the device once per orbit, the chained-BLA table is built on the device
+from it (ap_build_bla), and every pixel pass is one C-ABI launch.  The
+Pauldelbrot rebase loop (math_core/engine.py:1890-2113) reads the glitch
+and iteration maps back, picks a new reference pixel on the host
+(select_rebase_pixel) and re-renders only the glitched pixels.
+"""
+import ctypes as C
+from decimal import Decimal, localcontext
+
+import numpy as np
+
+from . import abi, _lib
+from .config import compute_floatexp_scale, compute_required_prec_bits, decimal_context
+from . import high_precision as hp
+
+BLA_LEVELS = 16
+MAX_REBASE_PASSES = 4
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+def select_rebase_pixel(glitch_map, iter_map, max_iter, visited, W, H):
+    """Next reference pixel (row, col) for a rebase pass, or None.
+
+    Bins glitched pixels on a 16x16 grid; in the most populated bin first an
+    unvisited interior pixel closest to the bin's median, then the unvisited
+    escaped pixel with the highest smooth value, then the unvisited pixel
+    closest to the median; failing every bin, the first unvisited glitched
+    pixel (math_core/engine.py:1923-1992).
+    """
+    gi = np.argwhere(glitch_map > 0)
+    if len(gi) == 0:
+        return None
+    bin_r = np.clip((gi[:, 0] * 16) // H, 0, 15)
+    bin_c = np.clip((gi[:, 1] * 16) // W, 0, 15)
+    bin_idx = bin_r * 16 + bin_c
+    counts = np.bincount(bin_idx, minlength=256)
+    for b in np.argsort(-counts):
+        if counts[b] == 0:
+            break
+        cluster = gi[bin_idx == b]
+        its = iter_map[cluster[:, 0], cluster[:, 1]]
+        cr = np.median(cluster[:, 0])
+        cc = np.median(cluster[:, 1])
+        interior = (its < 0) | (its >= max_iter)
+        if np.any(interior):
+            pts = cluster[interior]
+            dists = (pts[:, 0] - cr) ** 2 + (pts[:, 1] - cc) ** 2
+            for d in np.argsort(dists):
+                cand = (int(pts[d, 0]), int(pts[d, 1]))
+                if cand not in visited:
+                    return cand
+        escaped = (its > 0) & (its < max_iter)
+        cands = cluster[escaped]
+        if len(cands) > 0:
+            for c in np.argsort(-its[escaped]):
+                cand = (int(cands[c, 0]), int(cands[c, 1]))
+                if cand not in visited:
+                    return cand
+        dists = (cluster[:, 0] - cr) ** 2 + (cluster[:, 1] - cc) ** 2
+        for d in np.argsort(dists):
+            cand = (int(cluster[d, 0]), int(cluster[d, 1]))
+            if cand not in visited:
+                return cand
+    for g in range(len(gi)):
+        cand = (int(gi[g, 0]), int(gi[g, 1]))
+        if cand not in visited:
+            return cand
+    return None
+
+
+class RebaseState:
+    """Progress bookkeeping of the rebase loop (math_core/engine.py:1893-1919)."""
+
+    def __init__(self, init_rc, exhaustive, strict_limit=512):
+        self.visited = {init_rc}
+        self.prev = None
+        self.no_progress = 0
+        self.passes = 0
+        self.exhaustive = exhaustive
+        self.strict_limit = strict_limit
+
+    def should_continue(self, n_glitched):
+        if n_glitched == 0:
+            return False
+        if self.exhaustive and n_glitched <= self.strict_limit:
+            return False
+        if self.prev is not None and n_glitched >= self.prev:
+            self.no_progress += 1
+            if self.no_progress >= 2:
+                return False
+        else:
+            self.no_progress = 0
+        self.prev = n_glitched
+        return True
+
+
+def _upload_orbit(torch, re, im, ref_len, slot, tag):
+    from .engine import get_scratch_device_array_1d
+    n = ref_len + 1
+    d_re = get_scratch_device_array_1d(n, np.float64, f"{tag}_re_{slot}")[:n]
+    d_im = get_scratch_device_array_1d(n, np.float64, f"{tag}_im_{slot}")[:n]
+    d_re.copy_(torch.from_numpy(np.ascontiguousarray(re[:n])), non_blocking=False)
+    d_im.copy_(torch.from_numpy(np.ascontiguousarray(im[:n])), non_blocking=False)
+    return d_re, d_im
+
+
+def _build_bla(L, d_re, d_im, ref_len, fractal_type, tol, gen_n, gen_kr, gen_ki, slot, stream_h):
+    from .engine import get_scratch_device_array_1d
+    n = BLA_LEVELS * max(ref_len, 1) * 5
+    table = get_scratch_device_array_1d(n, np.float64, f"bla_table_{slot}")[:n]
+    _lib.check(L.ap_build_bla(_ptr(d_re), _ptr(d_im), int(ref_len), int(fractal_type),
+                              float(tol), BLA_LEVELS, int(gen_n), float(gen_kr), float(gen_ki),
+                              _ptr(table), stream_h), "ap_build_bla")
+    return table
+
+
+def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_iter, center_x_dec,
+                              center_y_dec, plot_width_dec, tier, scheme, num_bins, fractal_type,
+                              julia_cx, julia_cy, bbsa_tol, bbsa_order, glitch_mode, gen_n, gen_kr,
+                              gen_ki, edge_threshold, slot, arith_code, extra_out=None):
+    """All device passes of one perturbation-tier frame (math_core/engine.py:1718-2113)."""
+    import torch
+    from .engine import _buffers, get_scratch_device_array
+    L = _lib.load()
+    cpu_sem = arith_code == abi.AP_ARITH_REF_CPU
+    kmap = s64 = None
+    if extra_out is not None:
+        kmap, s64 = extra_out
+    ctx = decimal_context(plot_width_dec)
+    with localcontext(ctx):
+        plot_height_dec = plot_width_dec * (Decimal(H) / Decimal(W))
+        dx_f = float(plot_width_dec / Decimal(max(1, W - 1)))
+        dy_f = float(plot_height_dec / Decimal(max(1, H - 1)))
+        floatexp = tier == abi.AP_TIER_FLOATEXP
+        if floatexp:
+            e_scale = compute_floatexp_scale(plot_width_dec)
+            norm_w = plot_width_dec * (Decimal(2) ** e_scale)
+            norm_h = plot_height_dec * (Decimal(2) ** e_scale)
+            dx_f = float(norm_w / Decimal(max(1, W - 1)))
+            dy_f = float(norm_h / Decimal(max(1, H - 1)))
+            if bbsa_order in (4, 8):
+                bbsa_order = 32
+                if bbsa_tol > 1e-6:
+                    bbsa_tol = 1e-6
+        else:
+            e_scale = 0
+    strict = 1 if ("Auto Rebasing" in glitch_mode or "Strict" in glitch_mode
+                   or "Pauldelbrot" in glitch_mode) else 0
+
+    bcx, bcy, bu, bv, re, im, ref_len = hp.find_optimal_reference_orbit(
+        center_x_dec, center_y_dec, plot_width_dec, plot_height_dec, max_iter, W, H,
+        fractal_type=fractal_type, julia_cx=julia_cx, julia_cy=julia_cy, gen_n=gen_n,
+        gen_kr=gen_kr, gen_ki=gen_ki, is_floatexp=floatexp)
+    if bbsa_order not in (0, 32) and fractal_type in (0, 2, 4) and bbsa_tol > 0:
+        raise NotImplementedError(
+            "series-approximation starts (bbsa_order 4/8) are not served yet; use 0 or 32")
+    d_re, d_im = _upload_orbit(torch, re, im, ref_len, slot, "ref")
+    # The CPU reference's histogram path evaluates samples without BLA leaps
+    # (math_core/engine.py:624-637, cpu_kernels.py:1887); every other path leaps.
+    use_bla = bbsa_order == 32 and fractal_type in (0, 2, 4) and not (cpu_sem and scheme == 11)
+    bla = _build_bla(L, d_re, d_im, ref_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
+                     slot, stream_h) if use_bla else None
+
+    p.dx_hi, p.dy_hi = dx_f / float(factor), dy_f / float(factor)
+    p.ref_px = float(W - 1) * float(bu) * float(factor)
+    p.ref_py = float(H - 1) * float(bv) * float(factor)
+    p.ref_cx, p.ref_cy = float(bcx), float(bcy)
+    p.julia_cx_hi, p.julia_cy_hi = float(julia_cx), float(julia_cy)
+    p.ref_len = int(ref_len)
+    p.e_scale = int(e_scale)
+    p.strict_glitch = strict
+    p.bla_levels = BLA_LEVELS if use_bla else 0
+    p.rebase_pass = 0
+    # Sample variant: the CPU reference flags both; the CUDA unified kernels use the
+    # BLA variant (NaN guard), their histogram resolve passes the plain one (escape glitch).
+    unified_flags = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_NAN_GUARD
+    resolve_flags = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_ESCAPE_GLITCH
+    fr.glitch_in.zero_()
+    orbit = (d_re, d_im)
+    cdf = None
+
+    if scheme == 11:
+        hist = get_scratch_device_array((num_bins,), np.int32, f"hist_bins_{slot}")
+        cdf = get_scratch_device_array((num_bins,), np.float32, f"cdf_lut_{slot}")
+        p.mode = abi.AP_MODE_COARSE
+        p.flags = unified_flags | abi.AP_FLAG_NO_RGB
+        b = _buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
+        _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
+        _lib.check(L.ap_histogram_cdf(_ptr(fr.iter), W, H, max_iter, num_bins, _ptr(hist), _ptr(cdf),
+                                      stream_h), "ap_histogram_cdf")
+        _lib.check(L.ap_colour(C.byref(p), C.byref(b), stream_h), "ap_colour")
+        if factor > 1:
+            fr.edge_mask()
+            _lib.check(L.ap_edge_detect(_ptr(fr.iter), _ptr(fr.edge), W, H,
+                                        float(np.float32(edge_threshold)), stream_h), "ap_edge_detect")
+            q = _resolve_params(p, resolve_flags, cpu_sem)
+            b = _buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla if cpu_sem else None)
+            _lib.check(L.ap_resolve_hist_pass(C.byref(q), C.byref(b), stream_h), "ap_resolve_hist_pass")
+    else:
+        p.mode = abi.AP_MODE_COARSE
+        p.flags = unified_flags
+        b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
+        _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
+        if factor > 1:
+            fr.edge_mask()
+            _lib.check(L.ap_edge_detect(_ptr(fr.iter), _ptr(fr.edge), W, H,
+                                        float(np.float32(edge_threshold)), stream_h), "ap_edge_detect")
+            p.mode = abi.AP_MODE_EDGE
+            p.flags = unified_flags | (0 if cpu_sem else abi.AP_FLAG_ITER_LAST_SUB)
+            b = _buffers(fr, lut, orbit=orbit, bla=bla)
+            _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
+
+    allow = strict == 1
+    if not (allow and plot_width_dec < Decimal("1e-12")):
+        return dict(ref_len=ref_len, passes=0)
+
+    exhaustive = "Strict" in glitch_mode
+    state = RebaseState((int(np.clip(p.ref_py / factor, 0, H - 1)), int(np.clip(p.ref_px / factor, 0, W - 1))),
+                        exhaustive, strict_limit=128 if cpu_sem else 512)
+    bits = compute_required_prec_bits(plot_width_dec)
+    while state.passes < MAX_REBASE_PASSES:
+        st.synchronize()
+        h_glitch = fr.glitch_out.cpu().numpy()
+        n_gl = int(np.count_nonzero(h_glitch))
+        if not state.should_continue(n_gl):
+            break
+        state.passes += 1
+        h_iter = fr.iter.cpu().numpy()
+        chosen = select_rebase_pixel(h_glitch, h_iter, max_iter, state.visited, W, H)
+        if chosen is None:
+            break
+        g_row, g_col = chosen
+        state.visited.add(chosen)
+        with localcontext(ctx):
+            x_min_dec = center_x_dec - (plot_width_dec / Decimal(2))
+            y_max_dec = center_y_dec + (plot_height_dec / Decimal(2))
+            r_cx = x_min_dec + (Decimal(int(g_col)) / Decimal(max(1, W - 1))) * plot_width_dec
+            r_cy = y_max_dec - (Decimal(int(g_row)) / Decimal(max(1, H - 1))) * plot_height_dec
+        r_re, r_im, r_len = hp.compute_single_highprec_orbit(
+            r_cx, r_cy, max_iter, fractal_type, julia_cx, julia_cy, bits,
+            gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki)
+        if r_len > 100:
+            hp.cache_reference_orbit(r_cx, r_cy, plot_width_dec, max_iter, r_re, r_im, r_len,
+                                     fractal_type=fractal_type, julia_cx=julia_cx,
+                                     julia_cy=julia_cy, gen_n=gen_n, gen_kr=gen_kr,
+                                     gen_ki=gen_ki, is_floatexp=floatexp)
+        d_re, d_im = _upload_orbit(torch, r_re, r_im, r_len, slot, "rebase")
+        fr.glitch_in.copy_(torch.from_numpy(h_glitch))
+        bla = _build_bla(L, d_re, d_im, r_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
+                         slot, stream_h) if use_bla else None
+        q = _copy_params(p)
+        q.ref_px, q.ref_py = float(g_col) * float(factor), float(g_row) * float(factor)
+        q.ref_cx, q.ref_cy = float(r_cx), float(r_cy)
+        q.ref_len = int(r_len)
+        q.bla_levels = BLA_LEVELS if bla is not None else 0
+        q.rebase_pass = state.passes
+        orbit = (d_re, d_im)
+        if scheme == 11 and cdf is not None:
+            q = _resolve_params(q, resolve_flags, cpu_sem)
+            b = _buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla if cpu_sem else None, kmap=kmap, s64=s64)
+            _lib.check(L.ap_resolve_hist_pass(C.byref(q), C.byref(b), stream_h), "ap_resolve_hist_pass")
+        elif factor == 1:
+            q.mode = abi.AP_MODE_COARSE
+            q.flags = unified_flags
+            b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
+            _lib.check(L.ap_render_pass(C.byref(q), C.byref(b), stream_h), "ap_render_pass")
+        else:
+            b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
+            if cpu_sem:
+                # CPU reference: coarse re-render of glitched pixels, then their supersample.
+                q.mode = abi.AP_MODE_COARSE
+                q.flags = unified_flags
+                _lib.check(L.ap_render_pass(C.byref(q), C.byref(b), stream_h), "ap_render_pass")
+                q.mode = abi.AP_MODE_FULL
+                b = _buffers(fr, lut, orbit=orbit, bla=bla)
+            else:
+                q.mode = abi.AP_MODE_FULL
+                q.flags = unified_flags | abi.AP_FLAG_ITER_LAST_SUB
+            _lib.check(L.ap_render_pass(C.byref(q), C.byref(b), stream_h), "ap_render_pass")
+    if exhaustive:
+        st.synchronize()
+        if int(torch.count_nonzero(fr.glitch_out)) > 0:
+            raise NotImplementedError("Strict Metric exhaustive re-evaluation is not served yet")
+    return dict(ref_len=ref_len, passes=state.passes)
+
+
+def _copy_params(p):
+    q = abi.ApFrameParams()
+    C.pointer(q)[0] = p
+    return q
+
+
+def _resolve_params(p, flags, cpu_sem):
+    q = _copy_params(p)
+    q.flags = flags
+    if not cpu_sem:
+        q.bla_levels = 0  # the CUDA resolve kernels use the non-BLA sample
+    return q

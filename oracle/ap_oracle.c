@@ -243,29 +243,33 @@ static double tri_wave(double phase) {
     return 1.0 - fabs((phase < 0.0 ? phase + 2.0 : phase) - 1.0);
 }
 
-static double palette_norm(double s, int scheme, double off, double density, double contrast) {
+/* sqrt of the smooth value: the CPU reference holds it as float32 and Numba
+ * evaluates math.sqrt(float32) in float32; the CUDA reference holds float64. */
+static double sqrt_s(double s, int f32) { return f32 ? (double)sqrtf((float)s) : sqrt(s); }
+
+static double palette_norm(double s, int scheme, double off, double density, double contrast, int f32) {
     const double dens = density <= 0.0 ? 1.0 : density;
     const double cont = contrast <= 0.0 ? 1.0 : contrast;
     const double TWO_PI = 6.28318530718;
     if (scheme == 0 || scheme > 10) {
-        double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.125 * dens) + off * 2.0, 2.0));
         return cont != 1.0 ? pow(tri, cont) : tri;
     } else if (scheme == 1) {
         return tri_wave(py_mod(log(s * cont + 1.0) * (0.45 * dens) + off * 2.0, 2.0));
     } else if (scheme == 2) {
-        double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.125 * dens) + off * 2.0, 2.0));
         double k = 4.0 * cont;
         double td = tanh(0.5 * k);
         double scale = fabs(td) > 1e-7 ? 0.5 / td : 0.5186574;
         return 0.5 + tanh((tri - 0.5) * k) * scale;
     } else if (scheme == 3) {
-        double tri = tri_wave(py_mod(sqrt(s) * (0.125 * dens) + off * 2.0, 2.0));
+        double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.125 * dens) + off * 2.0, 2.0));
         double k = 3.0 * cont;
         double ed = exp(k) - 1.0;
         double scale = fabs(ed) > 1e-7 ? 1.0 / ed : 0.0523957;
         return (exp(k * tri) - 1.0) * scale;
     } else if (scheme == 4) {
-        double tri = tri_wave(py_mod(sqrt(s) * (0.5 * dens) + off * 2.0, 2.0));
+        double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.5 * dens) + off * 2.0, 2.0));
         return cont != 1.0 ? pow(tri, cont) : tri;
     } else if (scheme == 5) {
         double ang = s * (0.05 * dens) + off * TWO_PI;
@@ -284,7 +288,7 @@ static double palette_norm(double s, int scheme, double off, double density, dou
         double scale = ns > 1e-7 ? 0.5 / ns : 0.26666666666666666;
         return 0.5 + scale * wave;
     } else if (scheme == 8) {
-        double tri = tri_wave(py_mod(sqrt(s) * (0.1 * dens) + off * 2.0, 2.0));
+        double tri = tri_wave(py_mod(sqrt_s(s, f32) * (0.1 * dens) + off * 2.0, 2.0));
         if (cont != 1.0) tri = pow(tri, cont);
         double t2 = tri * tri;
         return t2 * tri * (tri * (tri * 6.0 - 15.0) + 10.0);
@@ -338,7 +342,8 @@ static double colour_norm(const ApFrameParams* p, const ApFrameBuffers* bf, doub
     if (hist)
         return cdf_norm(s, p->max_iter, bf->cdf, p->num_bins, p->palette_offset, p->color_density,
                         p->color_contrast);
-    return palette_norm(s, p->scheme_id, p->palette_offset, p->color_density, p->color_contrast);
+    return palette_norm(s, p->scheme_id, p->palette_offset, p->color_density, p->color_contrast,
+                        p->arith == AP_ARITH_REF_CPU);
 }
 
 static void put_rgb(const ApFrameParams* p, void* rgb, size_t idx, double r, double g, double b) {

@@ -315,7 +315,52 @@ def gen_pert():
     save("pert_samples.npz", meta=json.dumps(meta), **out)
 
 
-SECTIONS = {"fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert}
+def render3_cases():
+    wl = json.load(open(os.path.join(HERE, "workloads.json")))
+    cx3, cy3 = wl["config3_centre"]
+    pc = {c[0]: c for c in pert_cases()}
+    cases = [
+        # name, W, H, max_iter, cx, cy, width, scheme, factor, bbsa_order, glitch_mode, type, jx, jy, n, kr, ki
+        ("cfg3_bla_pauldelbrot", 192, 108, 20000, cx3, cy3, "1e-160", 0, 1, 32, "Pauldelbrot", 0, 0.0, 0.0, 3, 0.25, 1.0),
+        ("cfg3_plain", 192, 108, 20000, cx3, cy3, "1e-160", 5, 1, 0, "Off (Single-Ref)", 0, 0.0, 0.0, 3, 0.25, 1.0),
+        ("cfg3_hist", 128, 72, 20000, cx3, cy3, "1e-160", 11, 1, 32, "Pauldelbrot", 0, 0.0, 0.0, 3, 0.25, 1.0),
+        ("cfg3_ssaa2", 64, 36, 20000, cx3, cy3, "1e-160", 0, 2, 32, "Pauldelbrot", 0, 0.0, 0.0, 3, 0.25, 1.0),
+        ("cfg3_hist_ssaa2", 64, 36, 20000, cx3, cy3, "1e-160", 11, 2, 32, "Pauldelbrot", 0, 0.0, 0.0, 3, 0.25, 1.0),
+    ]
+    for name in ("ship", "julia", "ship_julia", "multibrot3"):
+        c = pc[name]
+        cases.append((f"{name}_frame", 160, 90, c[7], c[2], c[3], c[4], 0, 1, 32, "Pauldelbrot",
+                      c[1], c[9], c[10], c[11], c[12], c[13]))
+    return cases
+
+
+def gen_render3():
+    out = {}
+    meta = []
+    for c in render3_cases():
+        (name, W, H, mi, cx, cy, w, sid, fac, order, gm, ft, jx, jy, n, kr, ki) = c
+        R.hp.clear_reference_orbit_cache()
+        it = np.zeros((H, W), np.float32)
+        t0 = time.time()
+        rgb = R.engine.render_frame_cpu(
+            W, H, mi, Decimal(cx), Decimal(cy), Decimal(w), "synthetic",
+            ssaa_factor=fac, edge_threshold=0.35, color_scheme_id=sid,
+            precision_mode="1e-300 (Perturbation)", fractal_type=ft, julia_cx=jx, julia_cy=jy,
+            bbsa_tol=1e-6 if order == 32 else 0.0, bbsa_order=order, glitch_mode=gm,
+            gen_n=n, gen_kr=kr, gen_ki=ki, cpu_threads=8, palette_offset=0.0,
+            color_density=1.0, color_contrast=1.0, h_iter_buf=it)
+        print(f"  {name}: {time.time() - t0:.2f}s escaped {np.mean(it >= 0):.3f}")
+        out[name + "__rgb"] = rgb
+        out[name + "__iter"] = it
+        meta.append(dict(name=name, W=W, H=H, max_iter=mi, cx=cx, cy=cy, width=w, scheme=sid,
+                         factor=fac, bbsa_order=order, glitch_mode=gm, fractal_type=ft,
+                         julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki,
+                         offset=0.0, density=1.0, contrast=1.0))
+    save("render_pert.npz", meta=json.dumps(meta), **out)
+
+
+SECTIONS = {"fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
+            "render3": gen_render3}
 
 if __name__ == "__main__":
     wanted = sys.argv[1:] or list(SECTIONS)

@@ -64,3 +64,118 @@ def oracle_direct_frame(m, tier=abi.AP_TIER_FP64, arith=abi.AP_ARITH_REF_CPU, lu
 def rgb_mismatch(a, b):
     diff = np.abs(a.astype(np.int64) - b.astype(np.int64))
     return int(diff.any(axis=-1).sum()), int(diff.max()) if diff.size else 0
+
+
+def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max_passes=4):
+    """A perturbation-tier frame through the oracle, pass for pass as the engine issues it
+    (fractura_b200.perturbation.render_perturbation_frame), including the rebase loop."""
+    from fractura_b200 import high_precision as hp
+    from fractura_b200.config import compute_required_prec_bits
+    from fractura_b200.perturbation import RebaseState, select_rebase_pixel
+    W, H, f, mi = m["W"], m["H"], m["factor"], m["max_iter"]
+    ft, scheme = m["fractal_type"], m["scheme"]
+    cpu_sem = arith == abi.AP_ARITH_REF_CPU
+    pw = Decimal(m["width"])
+    cxd, cyd = Decimal(m["cx"]), Decimal(m["cy"])
+    ctx = decimal_context(pw)
+    with localcontext(ctx):
+        ph = pw * (Decimal(H) / Decimal(W))
+        dx_f = float(pw / Decimal(max(1, W - 1)))
+        dy_f = float(ph / Decimal(max(1, H - 1)))
+    hp.clear_reference_orbit_cache()
+    bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
+        cxd, cyd, pw, ph, mi, W, H, fractal_type=ft, julia_cx=m["julia_cx"], julia_cy=m["julia_cy"],
+        gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"])
+    order = m["bbsa_order"]
+    use_bla = order == 32 and ft in (0, 2, 4) and not (cpu_sem and scheme == 11)
+    tol = 1e-6
+
+    def table(r_re, r_im, r_len):
+        return oracle.build_bla(r_re, r_im, r_len, ft, tol, 16, m["gen_n"], m["gen_kr"], m["gen_ki"])
+
+    fr = oracle.Frame(W, H, lut=synthetic_lut() if lut is None else lut)
+    fr.ref_re, fr.ref_im = np.ascontiguousarray(re[:rl + 1]), np.ascontiguousarray(im[:rl + 1])
+    fr.bla = table(re, im, rl) if use_bla else None
+    strict = 1 if "Pauldelbrot" in m["glitch_mode"] or "Strict" in m["glitch_mode"] else 0
+    p = abi.new_params(width=W, height=H, factor=f, max_iter=mi, fractal_type=ft,
+                       tier=abi.AP_TIER_PERTURB, arith=arith, gen_n=m["gen_n"], gen_kr=m["gen_kr"],
+                       gen_ki=m["gen_ki"], scheme_id=scheme, num_bins=65536 if scheme == 11 else 2048,
+                       dx_hi=dx_f / f, dy_hi=dy_f / f, ref_px=float(W - 1) * float(bu) * float(f),
+                       ref_py=float(H - 1) * float(bv) * float(f), ref_cx=float(bcx), ref_cy=float(bcy),
+                       julia_cx_hi=float(m["julia_cx"]), julia_cy_hi=float(m["julia_cy"]),
+                       ref_len=int(rl), bla_levels=16 if use_bla else 0, strict_glitch=strict,
+                       palette_offset=m.get("offset", 0.0), color_density=m.get("density", 1.0),
+                       color_contrast=m.get("contrast", 1.0))
+    uf = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_NAN_GUARD
+    rf = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_ESCAPE_GLITCH
+
+    def resolve(q):
+        bla_keep = fr.bla
+        if not cpu_sem:
+            fr.bla = None
+            q.bla_levels = 0
+        q.flags = rf
+        oracle.resolve_hist_pass(q, fr)
+        fr.bla = bla_keep
+
+    if scheme == 11:
+        p.flags = uf | abi.AP_FLAG_NO_RGB
+        oracle.render_pass(p, fr)
+        oracle.histogram_cdf(fr, mi)
+        oracle.colour(p, fr)
+        if f > 1:
+            oracle.edge_detect(fr, np.float32(edge_threshold))
+            q = abi.ApFrameParams.from_buffer_copy(p)
+            resolve(q)
+    else:
+        p.flags = uf
+        oracle.render_pass(p, fr)
+        if f > 1:
+            oracle.edge_detect(fr, np.float32(edge_threshold))
+            p.mode = abi.AP_MODE_EDGE
+            p.flags = uf | (0 if cpu_sem else abi.AP_FLAG_ITER_LAST_SUB)
+            oracle.render_pass(p, fr)
+    if not (strict and pw < Decimal("1e-12")):
+        return fr, 0
+    state = RebaseState((int(np.clip(p.ref_py / f, 0, H - 1)), int(np.clip(p.ref_px / f, 0, W - 1))),
+                        "Strict" in m["glitch_mode"], 128 if cpu_sem else 512)
+    bits = compute_required_prec_bits(pw)
+    while state.passes < max_passes:
+        g = fr.glitch_out.copy()
+        if not state.should_continue(int(np.count_nonzero(g))):
+            break
+        state.passes += 1
+        chosen = select_rebase_pixel(g, fr.iter_map, mi, state.visited, W, H)
+        if chosen is None:
+            break
+        state.visited.add(chosen)
+        gr, gc = chosen
+        with localcontext(ctx):
+            r_cx = (cxd - pw / Decimal(2)) + (Decimal(gc) / Decimal(max(1, W - 1))) * pw
+            r_cy = (cyd + ph / Decimal(2)) - (Decimal(gr) / Decimal(max(1, H - 1))) * ph
+        r_re, r_im, r_len = hp.compute_single_highprec_orbit(
+            r_cx, r_cy, mi, ft, m["julia_cx"], m["julia_cy"], bits,
+            gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"])
+        fr.ref_re, fr.ref_im = np.ascontiguousarray(r_re[:r_len + 1]), np.ascontiguousarray(r_im[:r_len + 1])
+        fr.bla = table(r_re, r_im, r_len) if use_bla else None
+        fr.glitch_in[...] = g
+        q = abi.ApFrameParams.from_buffer_copy(p)
+        q.ref_px, q.ref_py = float(gc) * f, float(gr) * f
+        q.ref_cx, q.ref_cy = float(r_cx), float(r_cy)
+        q.ref_len = int(r_len)
+        q.bla_levels = 16 if use_bla else 0
+        q.rebase_pass = state.passes
+        if scheme == 11:
+            resolve(q)
+        elif f == 1:
+            q.mode, q.flags = abi.AP_MODE_COARSE, uf
+            oracle.render_pass(q, fr)
+        elif cpu_sem:
+            q.mode, q.flags = abi.AP_MODE_COARSE, uf
+            oracle.render_pass(q, fr)
+            q.mode = abi.AP_MODE_FULL
+            oracle.render_pass(q, fr)
+        else:
+            q.mode, q.flags = abi.AP_MODE_FULL, uf | abi.AP_FLAG_ITER_LAST_SUB
+            oracle.render_pass(q, fr)
+    return fr, state.passes

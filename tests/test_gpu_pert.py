@@ -1,0 +1,83 @@
+"""GPU parity of the perturbation tier (FP64 deltas, chained BLA, Pauldelbrot rebasing)."""
+import ctypes as C
+from decimal import Decimal
+
+import numpy as np
+import pytest
+
+import oracle
+from fractura_b200 import _lib, engine
+from fractura_b200 import high_precision as hp
+from helpers import load_golden, oracle_pert_frame, rgb_mismatch
+
+pytestmark = pytest.mark.gpu
+
+PS, PMETA = load_golden("pert_samples.npz")
+RS, RMETA = load_golden("render_pert.npz")
+
+
+@pytest.mark.parametrize("name", [m["name"] for m in PMETA if m["bla_shape"][0] > 1])
+def test_device_bla_table_matches_oracle(name):
+    import torch
+    m = next(x for x in PMETA if x["name"] == name)
+    re, im = PS[name + "__re"], PS[name + "__im"]
+    rl = m["ref_len"]
+    d_re = torch.from_numpy(re).cuda()
+    d_im = torch.from_numpy(im).cuda()
+    out = torch.empty((16, rl, 5), dtype=torch.float64, device="cuda")
+    L = _lib.load()
+    _lib.check(L.ap_build_bla(C.c_void_p(d_re.data_ptr()), C.c_void_p(d_im.data_ptr()), rl,
+                              m["fractal_type"], 1e-6, 16, m["gen_n"], m["gen_kr"], m["gen_ki"],
+                              C.c_void_p(out.data_ptr()), None), "ap_build_bla")
+    T = oracle.build_bla(re, im, rl, m["fractal_type"], 1e-6, 16, m["gen_n"], m["gen_kr"], m["gen_ki"])
+    got = out.cpu().numpy()
+    if m["fractal_type"] == 4 and m["gen_n"] > 3:
+        # x_max = tol_a^(1/(n-1)) goes through pow(); CUDA's and glibc's pow may differ by an ulp
+        assert np.array_equal(got[..., :4], T[..., :4])
+        assert np.allclose(got[..., 4], T[..., 4], rtol=1e-15, atol=0)
+    else:
+        assert got.tobytes() == T.tobytes()
+
+
+@pytest.mark.parametrize("variant", ["plain", "bla"])
+def test_config3_full_frame_matches_reference_samples(variant):
+    """1920x1080 frame at the 1e-160 view (one pass, no rebase) against the reference's
+    per-sample values (cpu_compute_perturbation_sample) on every 40th pixel."""
+    m = next(x for x in PMETA if x["name"] == "cfg3")
+    hp.clear_reference_orbit_cache()
+    it = np.zeros((m["H"], m["W"]), np.float32)
+    engine.render_frame_ssaa(m["W"], m["H"], m["max_iter"], Decimal(m["cx"]), Decimal(m["cy"]),
+                             Decimal(m["width"]), None, color_scheme_id=0,
+                             precision_mode="1e-300 (Perturbation)", fractal_type=0,
+                             bbsa_tol=1e-6, bbsa_order=32 if variant == "bla" else 0,
+                             glitch_mode="Off (Single-Ref)", h_iter_buf=it)
+    st = m["stride"]
+    ref = PS[f"cfg3__{variant}_s"]
+    assert np.array_equal(it[::st, ::st].view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("name", [m["name"] for m in RMETA])
+@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda"])
+def test_pert_frame_with_rebasing(name, arith):
+    import torch
+    m = next(x for x in RMETA if x["name"] == name)
+    W, H = m["W"], m["H"]
+    hp.clear_reference_orbit_cache()
+    it = np.zeros((H, W), np.float32)
+    kmap = torch.empty((H, W), dtype=torch.int32, device="cuda")
+    s64 = torch.empty((H, W), dtype=torch.float64, device="cuda")
+    rgb = engine.render_frame_ssaa(
+        W, H, m["max_iter"], Decimal(m["cx"]), Decimal(m["cy"]), Decimal(m["width"]), None,
+        ssaa_factor=m["factor"], color_scheme_id=m["scheme"], precision_mode="1e-300 (Perturbation)",
+        fractal_type=m["fractal_type"], julia_cx=m["julia_cx"], julia_cy=m["julia_cy"],
+        bbsa_tol=1e-6 if m["bbsa_order"] == 32 else 0.0, bbsa_order=m["bbsa_order"],
+        glitch_mode=m["glitch_mode"], gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"],
+        h_iter_buf=it, arith=arith, _extra_out=(kmap, s64))
+    code = 0 if arith == "ref_cpu" else 1
+    fr, _ = oracle_pert_frame(m, arith=code)
+    assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32)), \
+        int((it.view(np.uint32) != fr.iter_map.view(np.uint32)).sum())
+    n_bad, max_diff = rgb_mismatch(rgb, fr.rgb)
+    assert n_bad == 0, (n_bad, max_diff)
+    if arith == "ref_cpu" and name != "cfg3_hist_ssaa2":
+        assert np.array_equal(it.view(np.uint32), RS[name + "__iter"].view(np.uint32))
