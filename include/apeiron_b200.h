@@ -136,6 +136,19 @@ AP_API int ap_edge_detect(const float* iter_map, uint8_t* edge_mask, int32_t wid
 AP_API int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height, int32_t max_iter,
                      int32_t num_bins, int32_t* hist, float* cdf, void* stream);
 
+/* Largest num_bins ap_histogram_cdf_noalloc accepts (its built-in scratch, 256 KiB per GPU). */
+#define AP_NOALLOC_MAX_BINS 65536
+
+/* ap_histogram_cdf without the caller scratch: for callers that cannot allocate
+ * device memory (no cudaMalloc where they run).  No counterpart in the reference.
+ * The histogram goes to an array compiled into the library (AP_NOALLOC_MAX_BINS
+ * int32 per GPU, held from module load until process exit); num_bins above that
+ * is rejected with AP_E_INVALID.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress), so make it before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the GPU race. */
+AP_API int ap_histogram_cdf_noalloc(const float* iter_map, int32_t width, int32_t height,
+                                    int32_t max_iter, int32_t num_bins, float* cdf, void* stream);
+
 /* Colour every pixel from its smooth value.  With scheme 11 the CDF table is used
  * (apply_histogram_equalization_kernel, math_core/cuda_kernels.py:2016); otherwise
  * the closed-form transfer function (recolor_iter_map_cuda_kernel, :3201). */
