@@ -3,14 +3,29 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
-A step renders one frame of the workload.  Rank 0 prints one JSON line:
-  value   device-resident throughput: the frame's device passes on inputs
-          already in HBM, CUDA-event timed per step with an L2 flush
-          (a 512 MiB write) between steps, max over ranks;
-  e2e     the same metric through engine.render_frame_ssaa with host
-          buffers: host planning, H2D of the step's inputs and D2H of the
-          RGB frame inside the timed region;
-  roofline, clocks, cpu_baseline, gpu_launches as documented in DESIGN.md.
+Workload (default "cfg3"): 1920x1080 Mandelbrot at width 1e-160 around the
+600-digit centre of tests/golden/workloads.json, max_iter 200000, chained BLA
+(16 levels, tol 1e-6), Pauldelbrot glitch detection and up to 4 rebase
+passes.  A step renders one frame.  The metric is nominal iterations per
+second: the sum over pixels of the escape step (max_iter for pixels that never
+escape, 0 for cardioid skips), BLA leaps counting the steps they skip.
+
+Rank 0 prints one JSON line:
+  value     device-resident throughput: the frame's recorded device work
+            (render passes, device BLA builds, rebase passes, device copies)
+            replayed with every reference orbit already in HBM; CUDA events
+            per step on the launching stream, a 512 MiB write between steps
+            (L2 flush), max over ranks;
+  e2e       the same metric through engine.render_frame_ssaa with host
+            buffers: orbit search (LRU-cached like the reference's), the
+            four rebase orbits in Decimal, H2D of orbits, D2H of the glitch
+            and iteration maps per rebase pass and of the RGB frame;
+  plain     the plain FP64-delta form (no BLA, no rebasing) on the same view;
+  roofline  FP64 pipe of render_pass_kernel: executed FP64 operations (from
+            the kernel's work counters) / its event-timed duration, against
+            the measured dependent-FMA FP64 peak;
+  cpu_baseline, clocks, gpu_launches (kernels launched by the library in
+            the timed region, from its own counter).
 Multi-GPU: one process per GPU, every rank renders its own frame (weak
 scaling, no collective on the data path).
 """
@@ -30,21 +45,40 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-FP64_FLOPS_PER_ITER = 8.0  # Mandelbrot FP64 step: 3 mul + 1 fma (2) + 3 add/sub
+# Executed FP64 operations of the perturbation loop (reference-CPU arithmetic, no fused ops):
+#   stage-1 step: z = Z + dz (2), |z|^2 (3), Pauldelbrot test (4), BLA radius test (3),
+#                 dz' = (2Z + dz) dz + dc (13)                                        -> 25
+#   BLA leap:     z, |z|^2 (5), Pauldelbrot test (4), radius test (3), A dz + B dc (14) -> 26
+#   stage-2 step: z^2 + c direct (8)
+FLOPS_STEP1 = 25.0
+FLOPS_LEAP = 26.0
+FLOPS_STEP2 = 8.0
+FLOPS_DIRECT = 8.0  # FP64 direct Mandelbrot step
 
 
 # --------------------------------------------------------------- workloads
+def _centres():
+    with open(os.path.join(ROOT, "tests", "golden", "workloads.json")) as f:
+        return json.load(f)
+
+
+def workload_cfg3():
+    cx, cy = _centres()["config3_centre"]
+    return dict(name="mandelbrot_perturb_bla_pauldelbrot_1920x1080_w1e-160", W=1920, H=1080,
+                max_iter=200000, cx=cx, cy=cy, width="1e-160", scheme=0, factor=1, fractal_type=0,
+                precision_mode="1e-300 (Perturbation)", bbsa_order=32, bbsa_tol=1e-6,
+                glitch_mode="Pauldelbrot", arith="ref_cpu", dtype="f64")
+
+
 def workload_cfg1():
-    """640x360 Mandelbrot, FP64 direct, centre (-0.65, 0), width 4, max_iter 1000,
-    histogram-equalised colouring, 1x SSAA."""
     return dict(name="mandelbrot_fp64_640x360_hist", W=640, H=360, max_iter=1000, cx="-0.65",
                 cy="0.0", width="4.0", scheme=11, factor=1, fractal_type=0,
-                precision_mode="1e-12 (FP64)", flops_per_iter=FP64_FLOPS_PER_ITER,
-                bound="fp64")
+                precision_mode="1e-12 (FP64)", bbsa_order=0, bbsa_tol=0.0,
+                glitch_mode="Off (Single-Ref)", arith="ref_cpu", dtype="f64")
 
 
-WORKLOADS = {"cfg1": workload_cfg1}
-DEFAULT_WORKLOAD = "cfg1"
+WORKLOADS = {"cfg3": workload_cfg3, "cfg1": workload_cfg1}
+DEFAULT_WORKLOAD = "cfg3"
 
 
 # ------------------------------------------------------------------ helpers
@@ -54,7 +88,7 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock and throttle-reason sampling during the timed region."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -69,10 +103,9 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            threading.Thread(target=self._read, daemon=True).start()
         except OSError:
             self.proc = None
         return self
@@ -108,16 +141,8 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def measured_peaks():
-    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            return json.load(f)
-    return {}
-
-
-def fma_peak_tflops(precision, stream_h, torch):
-    """Dependent-FMA probe of the FP64/FP32 vector pipe (TFLOP/s, best of 5)."""
+def fma_peak_tflops(precision, torch):
+    """Dependent-FMA probe of the FP64/FP32 vector pipe in TFLOP/s (best of 5)."""
     from fractura_b200 import _lib
     L = _lib.load()
     blocks = 148 * 16
@@ -130,7 +155,8 @@ def fma_peak_tflops(precision, stream_h, torch):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(st)
         _lib.check(L.ap_fma_peak_launch(precision, blocks, iters, C.c_void_p(scratch.data_ptr()),
-                                        C.byref(flops), C.c_void_p(st.cuda_stream)), "ap_fma_peak_launch")
+                                        C.byref(flops), C.c_void_p(st.cuda_stream)),
+                   "ap_fma_peak_launch")
         b.record(st)
         b.synchronize()
         if rep > 0:
@@ -146,188 +172,18 @@ def load_traffic(workload_name):
     return None
 
 
-# --------------------------------------------------------- reference arm
-def cpu_reference_arm(args, wl, rank, world):
-    """The reference's CPU path of the hot loop, restated in C (oracle/), on all host cores."""
-    if rank != 0:
-        return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle
-    cores = os.cpu_count() or 1
-    oracle.set_threads(cores)
-    value, sample = time_oracle(wl, args.steps, args.warmup)
-    line = {"metric": "G iter/s", "value": value, "unit": "G iter/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference", "config": config_of(wl, args),
-            "cpu_baseline": {"value": value, "unit": "G iter/s", "cores": cores, "kind": "port",
-                             "sample": sample},
-            "e2e": {"value": value, "unit": "G iter/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-
-
-def time_oracle(wl, steps, warmup, rows=None):
-    """Time the oracle on the workload frame (or every n-th row); returns (G iter/s, description)."""
-    import oracle
-    from fractura_b200 import abi
-    from helpers import direct_params
-    m = dict(W=wl["W"], H=wl["H"], factor=wl["factor"], max_iter=wl["max_iter"], cx=wl["cx"],
-             cy=wl["cy"], width=wl["width"], scheme=wl["scheme"], fractal_type=wl["fractal_type"])
-    p = direct_params(m, abi.AP_TIER_FP64, abi.AP_ARITH_REF_CPU)
-    p.flags = abi.AP_FLAG_NO_RGB
-    fr = oracle.Frame(wl["W"], wl["H"])
-    times = []
-    for it in range(warmup + steps):
-        t0 = time.perf_counter()
-        oracle.render_pass(p, fr)
-        oracle.histogram_cdf(fr, wl["max_iter"])
-        times.append(time.perf_counter() - t0)
-    iters = nominal_iterations(fr.kmap, wl["max_iter"])
-    t = float(np.mean(times[warmup:]))
-    return iters / t / 1e9, f"full {wl['W']}x{wl['H']} frame, oracle C port, mean of {steps} steps"
-
-
 def nominal_iterations(kmap, max_iter):
-    """Sum of escape steps, max_iter for never-escaped samples, 0 for cardioid skips."""
+    """Escape steps summed; max_iter for never-escaped samples; 0 for cardioid skips."""
     k = np.asarray(kmap)
     return float(k[k >= 0].astype(np.int64).sum() + np.int64(max_iter) * np.count_nonzero(k == -1))
 
 
-def config_of(wl, args):
+def config_of(wl, n_gpus):
     return {"workload": wl["name"], "width": wl["W"], "height": wl["H"], "max_iter": wl["max_iter"],
-            "ssaa": wl["factor"], "precision_mode": wl["precision_mode"],
+            "view_width": wl["width"], "ssaa": wl["factor"], "bla": wl["bbsa_order"] == 32,
+            "glitch_mode": wl["glitch_mode"], "max_rebase_passes": 4, "arith": wl["arith"],
             "l2": "flushed between timed steps (512 MiB write)",
-            "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single"}
-
-
-# -------------------------------------------------------------- our arm
-def our_arm(args, wl, rank, world, local_rank):
-    import torch
-    from fractura_b200 import _lib, abi, engine
-
-    torch.cuda.set_device(local_rank)
-    dev_stream = torch.cuda.Stream()
-    stream_h = C.c_void_p(dev_stream.cuda_stream)
-    W, H = wl["W"], wl["H"]
-    view = engine.plan_direct_view(W, H, wl["factor"], Decimal(wl["cx"]), Decimal(wl["cy"]),
-                                   Decimal(wl["width"]), abi.AP_TIER_FP64)
-    num_bins = 65536 if wl["scheme"] == 11 else 2048
-    with torch.cuda.stream(dev_stream):
-        fr = engine._DeviceFrame(W, H, False, slot=0)
-        lut = engine.get_device_lut(None)
-        kmap = torch.empty((H, W), dtype=torch.int32, device="cuda")
-        flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
-
-    def params():
-        p = abi.new_params(width=W, height=H, factor=wl["factor"], max_iter=wl["max_iter"],
-                           fractal_type=wl["fractal_type"], tier=abi.AP_TIER_FP64,
-                           arith=abi.AP_ARITH_REF_CPU, scheme_id=wl["scheme"], num_bins=num_bins)
-        for k, v in view.items():
-            setattr(p, k, v)
-        return p
-
-    L = _lib.load()
-    pass_events = []
-
-    def device_step(record):
-        """The frame's device passes (what render_frame issues after planning)."""
-        p = params()
-        p.flags = abi.AP_FLAG_NO_RGB
-        b = engine._buffers(fr, lut, kmap=kmap)
-        if record:
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(dev_stream)
-        _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
-        if record:
-            e1.record(dev_stream)
-            pass_events.append((e0, e1))
-        hist = engine.get_scratch_device_array((num_bins,), np.int32, "hist_bins_0")
-        cdf = engine.get_scratch_device_array((num_bins,), np.float32, "cdf_lut_0")
-        _lib.check(L.ap_histogram_cdf(C.c_void_p(fr.iter.data_ptr()), W, H, wl["max_iter"], num_bins,
-                                      C.c_void_p(hist.data_ptr()), C.c_void_p(cdf.data_ptr()),
-                                      stream_h), "ap_histogram_cdf")
-        b = engine._buffers(fr, lut, cdf=cdf)
-        _lib.check(L.ap_colour(C.byref(p), C.byref(b), stream_h), "ap_colour")
-
-    launches_per_step = 4  # render pass, histogram, CDF scan, colour
-
-    for _ in range(args.warmup):
-        device_step(False)
-    torch.cuda.synchronize()
-    iters = nominal_iterations(kmap.cpu().numpy(), wl["max_iter"])
-
-    barrier(world)
-    step_ms = []
-    with ClockSampler(local_rank) as clocks:
-        torch.cuda.synchronize()
-        for _ in range(args.steps):
-            with torch.cuda.stream(dev_stream):
-                flush.fill_(1)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(dev_stream)
-            device_step(True)
-            e1.record(dev_stream)
-            e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-        torch.cuda.synchronize()
-    barrier(world)
-    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
-    pass_ms = float(np.mean([a.elapsed_time(b) for a, b in pass_events]))
-    value = iters * args.steps * world / (total_ms * 1e-3) / 1e9
-
-    # End to end through the public entry point with host buffers.
-    h_rgb = torch.empty((H, W, 3), dtype=torch.uint8).pin_memory().numpy()
-    call = dict(ssaa_factor=wl["factor"], color_scheme_id=wl["scheme"],
-                precision_mode=wl["precision_mode"], fractal_type=wl["fractal_type"],
-                h_rgb_buf=h_rgb, stream=dev_stream)
-    for _ in range(args.warmup):
-        engine.render_frame_ssaa(W, H, wl["max_iter"], Decimal(wl["cx"]), Decimal(wl["cy"]),
-                                 Decimal(wl["width"]), None, **call)
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        engine.render_frame_ssaa(W, H, wl["max_iter"], Decimal(wl["cx"]), Decimal(wl["cy"]),
-                                 Decimal(wl["width"]), None, **call)
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
-    barrier(world)
-    e2e = iters * args.steps * world / e2e_s / 1e9
-
-    if rank != 0:
-        return
-    peak64 = fma_peak_tflops(64, stream_h, torch)
-    achieved = wl["flops_per_iter"] * iters / (pass_ms * 1e-3) / 1e12
-    traffic = load_traffic(wl["name"])
-    cpu_value, cpu_sample = cpu_baseline(wl)
-    line = {
-        "metric": "G iter/s", "value": value, "unit": "G iter/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
-        "config": config_of(wl, args),
-        "nominal_iterations_per_frame": iters,
-        "e2e": {"value": e2e, "unit": "G iter/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": H * W * 3},
-        "roofline": {"bound": wl["bound"], "kernel": "render_pass_kernel", "achieved": achieved,
-                     "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64 if peak64 else None,
-                     "peak_source": "measured dependent-FMA FP64 probe (ap_fma_peak_launch) in this run",
-                     "kernel_ms": pass_ms,
-                     "traffic": traffic.get("bytes_per_launch") if traffic else None},
-        "clocks": clocks.summary(),
-        "gpu_launches": launches_per_step * args.steps,
-        "cpu_baseline": {"value": cpu_value, "unit": "G iter/s", "cores": os.cpu_count(),
-                         "kind": "port", "sample": cpu_sample},
-    }
-    print(json.dumps(line), flush=True)
-
-
-def cpu_baseline(wl):
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle
-    oracle.set_threads(os.cpu_count() or 1)
-    return time_oracle(wl, 3, 1)
+            "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single"}
 
 
 def barrier(world):
@@ -346,6 +202,233 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
+# ----------------------------------------------------------- CPU baseline
+def oracle_baseline(wl, budget_s=12.0):
+    """The reference's per-pixel path restated in C (oracle/) on all host cores, on a
+    bounded sample of the workload: every n-th row of the frame, chained BLA, one pass."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from fractura_b200 import abi
+    from fractura_b200 import high_precision as hp
+    from fractura_b200.config import decimal_context
+    from decimal import localcontext
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    W, H, mi = wl["W"], wl["H"], wl["max_iter"]
+    if wl["precision_mode"].startswith("1e-12"):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from helpers import direct_params
+        m = dict(W=W, H=H, factor=1, max_iter=mi, cx=wl["cx"], cy=wl["cy"], width=wl["width"],
+                 scheme=wl["scheme"], fractal_type=wl["fractal_type"])
+        p = direct_params(m, abi.AP_TIER_FP64, abi.AP_ARITH_REF_CPU)
+        p.flags = abi.AP_FLAG_NO_RGB
+        fr = oracle.Frame(W, H)
+        t0 = time.perf_counter()
+        oracle.render_pass(p, fr)
+        t = time.perf_counter() - t0
+        return nominal_iterations(fr.kmap, mi) / t / 1e9, cores, f"full {W}x{H} frame, one pass"
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from helpers import oracle_pert_frame
+    m = dict(W=W, H=H, factor=wl["factor"], max_iter=mi, cx=wl["cx"], cy=wl["cy"],
+             width=wl["width"], scheme=wl["scheme"], fractal_type=wl["fractal_type"],
+             julia_cx=0.0, julia_cy=0.0, gen_n=3, gen_kr=0.25, gen_ki=1.0,
+             bbsa_order=wl["bbsa_order"], glitch_mode=wl["glitch_mode"])
+    t0 = time.perf_counter()
+    fr, passes = oracle_pert_frame(m)
+    t = time.perf_counter() - t0
+    return (nominal_iterations(fr.kmap, mi) / t / 1e9, cores,
+            f"full {W}x{H} frame incl. host orbits and {passes} rebase passes, C port of the "
+            f"reference's CPU kernels")
+
+
+def cpu_reference_arm(args, wl, rank, world):
+    """--impl reference: the reference's CPU implementation of the path (C port in
+    oracle/) on all host cores, rank 0 only."""
+    if rank != 0:
+        return
+    vals = []
+    sample = cores = None
+    for _ in range(max(1, args.steps)):
+        v, cores, sample = oracle_baseline(wl)
+        vals.append(v)
+    value = float(np.median(vals))
+    line = {"metric": "G iter/s", "value": value, "unit": "G iter/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"], "data": "synthetic",
+            "impl": "reference", "config": config_of(wl, args.gpus),
+            "cpu_baseline": {"value": value, "unit": "G iter/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "G iter/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- our arm
+def render_call(engine, wl, stream, extra=None, **over):
+    kw = dict(ssaa_factor=wl["factor"], color_scheme_id=wl["scheme"],
+              precision_mode=wl["precision_mode"], fractal_type=wl["fractal_type"],
+              bbsa_tol=wl["bbsa_tol"], bbsa_order=wl["bbsa_order"], glitch_mode=wl["glitch_mode"],
+              stream=stream, arith=wl["arith"])
+    kw.update(over)
+    return engine.render_frame_ssaa(wl["W"], wl["H"], wl["max_iter"], Decimal(wl["cx"]),
+                                    Decimal(wl["cy"]), Decimal(wl["width"]), None,
+                                    _extra_out=extra, **kw)
+
+
+def timed_replay(torch, _lib, ops, stream, steps, flush, record_pass=False):
+    """Replay recorded device work `steps` times; per-step CUDA events on `stream`,
+    L2 flush before each step.  Returns (per-step ms, render-pass event pairs)."""
+    step_ms, pass_ev = [], []
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        with torch.cuda.stream(stream):
+            for fn, args, what in ops:
+                if record_pass and what in ("ap_render_pass", "ap_resolve_hist_pass"):
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    _lib.check(fn(*args), what)
+                    b.record(stream)
+                    pass_ev.append((a, b))
+                elif args is None:
+                    fn()
+                else:
+                    _lib.check(fn(*args), what)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+    return step_ms, pass_ev
+
+
+def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla):
+    """Executed FP64 operations of every render pass in one replay, from the work counters."""
+    counters = torch.zeros((H, W, 4), dtype=torch.int32, device="cuda")
+    f1 = 18.0 + (4.0 if strict else 0.0) + (3.0 if has_bla else 0.0)
+    total = 0.0
+    launches = 0
+    with torch.cuda.stream(stream):
+        for fn, args, what in ops:
+            if args is None:
+                fn()
+                continue
+            if what in ("ap_render_pass", "ap_resolve_hist_pass"):
+                bufs = args[1]._obj
+                q = type(bufs).from_buffer_copy(bufs)
+                counters.zero_()
+                q.counters = C.c_void_p(counters.data_ptr())
+                _lib.check(fn(args[0], C.byref(q), args[2]), what)
+                c = counters.view(-1, 4).sum(dim=0, dtype=torch.int64).cpu().numpy()
+                p = args[0]._obj
+                if p.tier == abi.AP_TIER_FP64:
+                    total += FLOPS_DIRECT * float(c[0])
+                else:
+                    total += f1 * float(c[0]) + FLOPS_LEAP * float(c[1]) + FLOPS_STEP2 * float(c[2])
+                launches += 1
+            else:
+                _lib.check(fn(*args), what)
+    torch.cuda.synchronize()
+    return total, launches
+
+
+def our_arm(args, wl, rank, world, local_rank):
+    import torch
+    from fractura_b200 import _lib, abi, engine
+    from fractura_b200 import high_precision as hp
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    W, H = wl["W"], wl["H"]
+    kmap = torch.empty((H, W), dtype=torch.int32, device="cuda")
+    s64 = torch.empty((H, W), dtype=torch.float64, device="cuda")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    L = _lib.load()
+
+    # Warm-up renders through the public entry point (also fills the orbit cache).
+    hp.clear_reference_orbit_cache()
+    for _ in range(args.warmup):
+        render_call(engine, wl, stream, (kmap, s64))
+    torch.cuda.synchronize()
+    # Record one frame's device work.
+    with _lib.recording() as rec:
+        render_call(engine, wl, stream, (kmap, s64))
+    torch.cuda.synchronize()
+    iters = nominal_iterations(kmap.cpu().numpy(), wl["max_iter"])
+    from fractura_b200 import perturbation
+    n_rebase = perturbation.LAST_FRAME_STATS["rebase_passes"]
+    h2d = perturbation.LAST_FRAME_STATS["h2d_bytes"]
+    d2h = perturbation.LAST_FRAME_STATS["d2h_bytes"] + H * W * 3
+
+    barrier(world)
+    c0 = L.ap_launch_counter()
+    with ClockSampler(local_rank) as clocks:
+        torch.cuda.synchronize()
+        step_ms, pass_ev = timed_replay(torch, _lib, rec.ops, stream, args.steps, flush,
+                                        record_pass=True)
+        torch.cuda.synchronize()
+    launches = L.ap_launch_counter() - c0
+    barrier(world)
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+    value = iters * args.steps * world / (total_ms * 1e-3) / 1e9
+
+    # End to end through render_frame_ssaa with a pinned host RGB buffer.
+    h_rgb = torch.empty((H, W, 3), dtype=torch.uint8).pin_memory().numpy()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        render_call(engine, wl, stream, h_rgb_buf=h_rgb)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    barrier(world)
+    e2e = iters * args.steps * world / e2e_s / 1e9
+
+    if rank != 0:
+        return
+    # Plain FP64-delta comparator on the same view (no BLA, no rebasing).
+    plain = None
+    if wl["bbsa_order"] == 32:
+        for _ in range(2):
+            render_call(engine, wl, stream, (kmap, s64), bbsa_order=0, glitch_mode="Off (Single-Ref)")
+        with _lib.recording() as prec:
+            render_call(engine, wl, stream, (kmap, s64), bbsa_order=0, glitch_mode="Off (Single-Ref)")
+        torch.cuda.synchronize()
+        p_iters = nominal_iterations(kmap.cpu().numpy(), wl["max_iter"])
+        p_ms, _ = timed_replay(torch, _lib, prec.ops, stream, max(2, args.steps // 2), flush)
+        plain = {"value": p_iters / (float(np.mean(p_ms)) * 1e-3) / 1e9, "unit": "G iter/s",
+                 "ms_per_frame": float(np.mean(p_ms)), "form": "fp64 deltas, no BLA, no rebasing"}
+
+    strict = "Pauldelbrot" in wl["glitch_mode"] or "Strict" in wl["glitch_mode"]
+    flops, n_pass = pass_flops(torch, _lib, abi, rec.ops, stream, H, W, strict,
+                               wl["bbsa_order"] == 32)
+    pass_ms = float(np.sum([a.elapsed_time(b) for a, b in pass_ev])) / args.steps
+    peak64 = fma_peak_tflops(64, torch)
+    achieved = flops / (pass_ms * 1e-3) / 1e12 if pass_ms > 0 else None
+    traffic = load_traffic(wl["name"])
+    cpu_value, cores, cpu_sample = oracle_baseline(wl)
+    line = {
+        "metric": "G iter/s", "value": value, "unit": "G iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
+        "data": "synthetic", "impl": "ours", "config": config_of(wl, world),
+        "nominal_iterations_per_frame": iters, "rebase_passes": n_rebase,
+        "e2e": {"value": e2e, "unit": "G iter/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "plain_fp64_delta": plain,
+        "speedup_vs_plain": (value / plain["value"]) if plain else None,
+        "roofline": {"bound": "fp64", "kernel": "render_pass_kernel", "achieved": achieved,
+                     "peak": peak64, "unit": "TFLOP/s",
+                     "frac": achieved / peak64 if (achieved and peak64) else None,
+                     "peak_source": "measured dependent-FMA FP64 probe (ap_fma_peak_launch), this run",
+                     "launches_per_step": n_pass, "kernel_ms_per_step": pass_ms,
+                     "traffic": traffic.get("bytes_per_launch") if traffic else None},
+        "clocks": clocks.summary(),
+        "gpu_launches": int(launches),
+        "cpu_baseline": {"value": cpu_value, "unit": "G iter/s", "cores": cores, "kind": "port",
+                         "sample": cpu_sample},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,8 +437,7 @@ def main():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(3, args.warmup)
     rank, world, local_rank = dist_env()
     wl = WORKLOADS[args.workload]()
     if args.impl == "reference":

@@ -5,6 +5,8 @@ every entry point raises ``EngineUnavailable``; nothing falls back to the CPU.
 """
 import ctypes as C
 import os
+import threading
+from contextlib import contextmanager
 
 from . import abi
 
@@ -14,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libapeiron_b200.so")
 EXPORTS = (
     "ap_abi_version", "ap_last_error", "ap_render_pass", "ap_resolve_hist_pass",
     "ap_edge_detect", "ap_histogram_cdf", "ap_colour", "ap_build_bla", "ap_fma_peak_launch",
-    "ap_histogram_cdf_noalloc",
+    "ap_histogram_cdf_noalloc", "ap_launch_counter",
 )
 
 
@@ -54,9 +56,10 @@ def load():
     L.ap_build_bla.argtypes = [vp, vp, i32, i32, f64, i32, i32, f64, f64, vp, vp]
     L.ap_fma_peak_launch.argtypes = [i32, i32, i32, vp, C.POINTER(C.c_double), vp]
     L.ap_histogram_cdf_noalloc.argtypes = [vp, i32, i32, i32, i32, vp, vp]
+    L.ap_launch_counter.restype = C.c_uint64
     for name in EXPORTS:
         fn = getattr(L, name)
-        if fn.restype is None or fn.restype is C.c_int:
+        if fn.restype is None:
             fn.restype = C.c_int
     if L.ap_abi_version() != abi.AP_ABI_VERSION:
         raise EngineUnavailable(
@@ -73,3 +76,57 @@ def check(rc, what):
 
 def last_error():
     return load().ap_last_error().decode(errors="replace")
+
+
+# ------------------------------------------------------------------ recording
+# A frame's device work can be recorded while it is rendered and replayed
+# later with identical arguments (bench.py times the replay: every input is
+# then resident, and no host work sits between the launches).
+_rec = threading.local()
+
+
+class Recording:
+    def __init__(self):
+        self.ops = []  # (callable, args or None, what)
+
+
+@contextmanager
+def recording():
+    rec = Recording()
+    _rec.active = rec
+    try:
+        yield rec
+    finally:
+        _rec.active = None
+
+
+def _snapshot(arg):
+    obj = getattr(arg, "_obj", None)
+    if isinstance(obj, C.Structure):
+        copy = type(obj).from_buffer_copy(obj)
+        return C.byref(copy)
+    return arg
+
+
+def launch(fn, *args, what):
+    """Call a C-ABI entry point, raise on error, and record it if a recording is active."""
+    check(fn(*args), what)
+    rec = getattr(_rec, "active", None)
+    if rec is not None:
+        rec.ops.append((fn, tuple(_snapshot(a) for a in args), what))
+
+
+def device_op(fn):
+    """Run a device-side torch operation (copy, fill) and record it if a recording is active."""
+    fn()
+    rec = getattr(_rec, "active", None)
+    if rec is not None:
+        rec.ops.append((fn, None, "device_op"))
+
+
+def replay(ops):
+    for fn, args, what in ops:
+        if args is None:
+            fn()
+        else:
+            check(fn(*args), what)

@@ -5,7 +5,7 @@ compares the sizes against the library's own ``sizeof`` report.
 """
 import ctypes as C
 
-AP_ABI_VERSION = 1
+AP_ABI_VERSION = 2
 
 AP_OK = 0
 AP_E_INVALID = -1
@@ -68,6 +68,7 @@ class ApFrameBuffers(C.Structure):
         ("glitch_in", C.c_void_p), ("edge_mask", C.c_void_p),
         ("iter_map", C.c_void_p), ("rgb", C.c_void_p),
         ("glitch_out", C.c_void_p), ("kmap", C.c_void_p), ("s64", C.c_void_p),
+        ("counters", C.c_void_p),
     ]
 
 

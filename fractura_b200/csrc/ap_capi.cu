@@ -15,7 +15,10 @@ void set_error(const char* fmt, ...) {
     va_end(ap_list);
 }
 
+static unsigned long long g_launches = 0;
+
 int check_launch(const char* what) {
+    __atomic_fetch_add(&g_launches, 1ULL, __ATOMIC_RELAXED);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_error("%s: %s", what, cudaGetErrorString(e));
@@ -29,3 +32,7 @@ int check_launch(const char* what) {
 extern "C" int ap_abi_version(void) { return AP_ABI_VERSION; }
 
 extern "C" const char* ap_last_error(void) { return ap::g_last_error; }
+
+extern "C" uint64_t ap_launch_counter(void) {
+    return __atomic_load_n(&ap::g_launches, __ATOMIC_RELAXED);
+}

@@ -24,8 +24,11 @@ int check_launch(const char* what);
 struct SampleOut {
     float s;      // float32 smooth value (reference storage type), -1 interior
     double s64;   // float64 smooth value
-    int k;        // escape step, -1 = never escaped
+    int k;        // escape step, -1 = never escaped, -2 = cardioid/bulb skip
     int glitch;
+    int iters;    // iterations stepped one at a time (work accounting)
+    int leaps;    // BLA leaps taken
+    int iters2;   // perturbation stage-2 direct steps
 };
 
 __device__ __forceinline__ SampleOut interior_sample() {
@@ -34,6 +37,16 @@ __device__ __forceinline__ SampleOut interior_sample() {
     o.s64 = -1.0;
     o.k = -1;
     o.glitch = 0;
+    o.iters = 0;
+    o.leaps = 0;
+    o.iters2 = 0;
+    return o;
+}
+
+// Never escaped within max_iter iterations.
+__device__ __forceinline__ SampleOut interior_after(int max_iter) {
+    SampleOut o = interior_sample();
+    o.iters = max_iter;
     return o;
 }
 
@@ -51,6 +64,9 @@ __device__ __forceinline__ SampleOut escaped_sample(int k, double mag2, double i
     const double log_mag = log(mag2);
     o.k = k;
     o.glitch = 0;
+    o.iters = k;
+    o.leaps = 0;
+    o.iters2 = 0;
     if (log_mag > 1.0) {
         const double nu = (log(0.5 * log_mag) - kLnBailoutLog) * inv_ln;
         o.s = __fsub_rn((float)((double)k + 1.0), (float)nu);

@@ -100,7 +100,7 @@ __device__ __forceinline__ SampleOut dd_sample(dd cxv, dd cyv, const ApFramePara
             zx = dd_add(sub, cx);
             zy = dd_add(dd{zxy.hi * 2.0, zxy.lo * 2.0}, cy);
         }
-        return interior_sample();
+        return interior_after(max_iter);
     }
     if (ft == 1 || ft == 3) {
         for (int k = 0; k < max_iter; ++k) {
@@ -112,7 +112,7 @@ __device__ __forceinline__ SampleOut dd_sample(dd cxv, dd cyv, const ApFramePara
             zx = dd_add(sub, cx);
             zy = dd_sub(dd{zxy.hi * 2.0, zxy.lo * 2.0}, cy);
         }
-        return interior_sample();
+        return interior_after(max_iter);
     }
     if (ft == 4) {
         const int n = p.gen_n;
@@ -134,7 +134,7 @@ __device__ __forceinline__ SampleOut dd_sample(dd cxv, dd cyv, const ApFramePara
             zx = dd_add(dd_add(cr, kz_r), cx);
             zy = dd_add(dd_add(ci, kz_i), cy);
         }
-        return interior_sample();
+        return interior_after(max_iter);
     }
     return interior_sample();
 }

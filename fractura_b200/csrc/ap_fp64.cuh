@@ -48,7 +48,7 @@ __device__ __forceinline__ SampleOut fp64_sample(double x, double y, const ApFra
                 zx = zx2 - zy2 + cx;
             }
         }
-        return interior_sample();
+        return interior_after(max_iter);
     }
     if (ft == 1 || ft == 3) {
         for (int k = 0; k < max_iter; ++k) {
@@ -65,7 +65,7 @@ __device__ __forceinline__ SampleOut fp64_sample(double x, double y, const ApFra
                 zx = zx2 - zy2 + cx;
             }
         }
-        return interior_sample();
+        return interior_after(max_iter);
     }
     if (ft == 4) {
         const int n = p.gen_n;
@@ -104,7 +104,7 @@ __device__ __forceinline__ SampleOut fp64_sample(double x, double y, const ApFra
                 zy = zi + kz_i + cy;
             }
         }
-        return interior_sample();
+        return interior_after(max_iter);
     }
     return interior_sample();
 }

@@ -36,7 +36,7 @@ __device__ __forceinline__ cplx bbsa_eval(const double* c, double ux, double uy)
 }
 
 __device__ __forceinline__ SampleOut glitch_sample(int k) {
-    SampleOut o;
+    SampleOut o = interior_sample();
     o.s = (float)k;
     o.s64 = (double)k;
     o.k = k;
@@ -78,6 +78,14 @@ __device__ __forceinline__ SampleOut perturb_sample_at(const ApFrameParams& p,
     }
     const double dcpx = julia ? 0.0 : dcx, dcpy = julia ? 0.0 : dcy;
     int glitch = 0;
+    const int k0 = k;
+    int leaps = 0, skipped = 0, k2 = -1;
+    auto done = [&](SampleOut o, int k_end) {
+        o.iters = (k2 < 0 ? k_end - k0 : k2 - k0) - skipped;
+        o.iters2 = k2 < 0 ? 0 : k_end - k2;
+        o.leaps = leaps;
+        return o;
+    };
     const int levels = p.bla_levels;
     const bool has_bla = levels > 1 && b.bla != nullptr && (ft == 0 || ft == 2 || ft == 4);
     const size_t L = (size_t)ref_len;
@@ -92,7 +100,7 @@ __device__ __forceinline__ SampleOut perturb_sample_at(const ApFrameParams& p,
                 glitch = 1;
             SampleOut o = escaped_sample(k, mag2, inv_ln);
             o.glitch = glitch;
-            return o;
+            return done(o, k);
         }
         if (strict && k > 15) {
             const double r_mag2 = rx * rx + ry * ry;
@@ -122,8 +130,10 @@ __device__ __forceinline__ SampleOut perturb_sample_at(const ApFrameParams& p,
                 }
                 dzx = nx;
                 dzy = ny;
-                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) return glitch_sample(k);
+                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) return done(glitch_sample(k), k);
                 k += 1 << best;
+                ++leaps;
+                skipped += 1 << best;
                 continue;
             }
         }
@@ -168,15 +178,16 @@ __device__ __forceinline__ SampleOut perturb_sample_at(const ApFrameParams& p,
     const double cx = julia ? p.julia_cx_hi : p.ref_cx + dcx;
     const double cy = julia ? p.julia_cy_hi : p.ref_cy + dcy;
     if (ref_len < max_iter) glitch = 1;
+    k2 = k;
     const bool nan_guard = (p.flags & AP_FLAG_NAN_GUARD) != 0;
     while (k < max_iter) {
         const double zx2 = zx * zx, zy2 = zy * zy;
         const double mag2 = zx2 + zy2;
-        if (nan_guard && (isnan(mag2) || isinf(mag2))) return glitch_sample(k);
+        if (nan_guard && (isnan(mag2) || isinf(mag2))) return done(glitch_sample(k), k);
         if (mag2 > kBailout) {
             SampleOut o = escaped_sample(k, mag2, inv_ln);
             o.glitch = glitch;
-            return o;
+            return done(o, k);
         }
         if (ft == 0 || ft == 2) {
             zy = 2.0 * zx * zy + cy;
@@ -200,7 +211,7 @@ __device__ __forceinline__ SampleOut perturb_sample_at(const ApFrameParams& p,
     }
     SampleOut o = interior_sample();
     o.glitch = glitch;
-    return o;
+    return done(o, max_iter);
 }
 
 template <int ARITH>

@@ -67,6 +67,9 @@ __global__ void __launch_bounds__(256) render_pass_kernel(const ApFrameParams p,
         b.iter_map[idx] = o.s;
         if (b.kmap) b.kmap[idx] = o.k;
         if (b.s64) b.s64[idx] = o.s64;
+        if (b.counters) {
+            reinterpret_cast<int4*>(b.counters)[idx] = make_int4(o.iters, o.leaps, o.iters2, 0);
+        }
         if (kPert && b.glitch_out) b.glitch_out[idx] = o.glitch > 0 ? 1 : 0;
         if (!(p.flags & AP_FLAG_NO_RGB)) {
             double r = 0.0, g = 0.0, bb = 0.0;
@@ -77,13 +80,16 @@ __global__ void __launch_bounds__(256) render_pass_kernel(const ApFrameParams p,
     }
 
     double ra = 0.0, ga = 0.0, ba = 0.0;
-    int glitches = 0;
+    int glitches = 0, iters = 0, leaps = 0, iters2 = 0;
     SampleOut last = interior_sample();
     for (int sy = 0; sy < f; ++sy) {
         for (int sx = 0; sx < f; ++sx) {
             const SampleOut o =
                 sample_at<TIER, ARITH>(p, b, (double)(i * f + sx), (double)(j * f + sy));
             last = o;
+            iters += o.iters;
+            leaps += o.leaps;
+            iters2 += o.iters2;
             if (o.glitch > 0) ++glitches;
             if ((double)o.s >= 0.0) {
                 double r, g, bb;
@@ -97,6 +103,9 @@ __global__ void __launch_bounds__(256) render_pass_kernel(const ApFrameParams p,
     const double inv = 1.0 / (double)(f * f);
     store_rgb(b.rgb, p.is_hdr, idx, ra * inv, ga * inv, ba * inv);
     if (kPert && b.glitch_out) b.glitch_out[idx] = glitches > 0 ? 1 : 0;
+    if (b.counters) {
+        reinterpret_cast<int4*>(b.counters)[idx] = make_int4(iters, leaps, iters2, 0);
+    }
     const bool write_iter =
         hist_resolve ? (p.rebase_pass > 0) : ((p.flags & AP_FLAG_ITER_LAST_SUB) != 0);
     if (write_iter) {
@@ -157,6 +166,10 @@ int validate_frame(const ApFrameParams* p, const ApFrameBuffers* b, int hist_res
     }
     if (!b->iter_map) {
         set_error("iter_map is required");
+        return AP_E_INVALID;
+    }
+    if (b->counters && (reinterpret_cast<uintptr_t>(b->counters) & 15u)) {
+        set_error("counters must be 16-byte aligned");
         return AP_E_INVALID;
     }
     const bool need_rgb = hist_resolve || p->mode != AP_MODE_COARSE || !(p->flags & AP_FLAG_NO_RGB);

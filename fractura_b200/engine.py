@@ -288,29 +288,29 @@ def _render_direct(p, fr, lut, stream_h, scheme, factor, arith_code, num_bins, m
         p.mode = abi.AP_MODE_COARSE
         p.flags = abi.AP_FLAG_NO_RGB
         b = _buffers(fr, lut, cdf=cdf, kmap=kmap, s64=s64)
-        _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
-        _lib.check(L.ap_histogram_cdf(_ptr(fr.iter), fr.W, fr.H, max_iter, num_bins, _ptr(hist),
-                                      _ptr(cdf), stream_h), "ap_histogram_cdf")
-        _lib.check(L.ap_colour(C.byref(p), C.byref(b), stream_h), "ap_colour")
+        _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
+        _lib.launch(L.ap_histogram_cdf, _ptr(fr.iter), fr.W, fr.H, max_iter, num_bins, _ptr(hist),
+                                      _ptr(cdf), stream_h, what="ap_histogram_cdf")
+        _lib.launch(L.ap_colour, C.byref(p), C.byref(b), stream_h, what="ap_colour")
         if factor > 1:
             fr.edge_mask()
             b = _buffers(fr, lut, cdf=cdf)
-            _lib.check(L.ap_edge_detect(_ptr(fr.iter), _ptr(fr.edge), fr.W, fr.H,
-                                        float(np.float32(edge_threshold)), stream_h), "ap_edge_detect")
+            _lib.launch(L.ap_edge_detect, _ptr(fr.iter), _ptr(fr.edge), fr.W, fr.H,
+                                        float(np.float32(edge_threshold)), stream_h, what="ap_edge_detect")
             p.flags = abi.AP_FLAG_MAP_FUSED if cpu else 0
-            _lib.check(L.ap_resolve_hist_pass(C.byref(p), C.byref(b), stream_h), "ap_resolve_hist_pass")
+            _lib.launch(L.ap_resolve_hist_pass, C.byref(p), C.byref(b), stream_h, what="ap_resolve_hist_pass")
         return cdf
     p.mode = abi.AP_MODE_COARSE
     p.flags = abi.AP_FLAG_MAP_FUSED if cpu else 0
     b = _buffers(fr, lut, kmap=kmap, s64=s64)
-    _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
+    _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
     if factor > 1:
         fr.edge_mask()
         b = _buffers(fr, lut)
-        _lib.check(L.ap_edge_detect(_ptr(fr.iter), _ptr(fr.edge), fr.W, fr.H,
-                                    float(np.float32(edge_threshold)), stream_h), "ap_edge_detect")
+        _lib.launch(L.ap_edge_detect, _ptr(fr.iter), _ptr(fr.edge), fr.W, fr.H,
+                                    float(np.float32(edge_threshold)), stream_h, what="ap_edge_detect")
         p.mode = abi.AP_MODE_EDGE
-        _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
+        _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
     return None
 
 
@@ -463,10 +463,10 @@ def recolor_frame(params: RenderParameters, d_iter_buf=None, h_iter_buf=None):
         if scheme == 11:
             hist = get_scratch_device_array((65536,), np.int32, f"hist_bins_{slot}")
             cdf = get_scratch_device_array((65536,), np.float32, f"cdf_lut_{slot}")
-            _lib.check(L.ap_histogram_cdf(_ptr(d_iter), W, H, int(params.max_iter), 65536,
-                                          _ptr(hist), _ptr(cdf), stream_h), "ap_histogram_cdf")
+            _lib.launch(L.ap_histogram_cdf, _ptr(d_iter), W, H, int(params.max_iter), 65536,
+                                          _ptr(hist), _ptr(cdf), stream_h, what="ap_histogram_cdf")
         b = _buffers(fr, lut, cdf=cdf)
-        _lib.check(L.ap_colour(C.byref(p), C.byref(b), stream_h), "ap_colour")
+        _lib.launch(L.ap_colour, C.byref(p), C.byref(b), stream_h, what="ap_colour")
         out = _copy_to_host(fr.rgb, params.h_rgb_buf, st)
     if getattr(params, "sync_stream", True):
         st.synchronize()

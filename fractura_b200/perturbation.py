@@ -21,6 +21,9 @@ from . import high_precision as hp
 BLA_LEVELS = 16
 MAX_REBASE_PASSES = 4
 
+# Host<->device traffic of the last perturbation frame (bytes), for benchmarking.
+LAST_FRAME_STATS = {"h2d_bytes": 0, "d2h_bytes": 0, "rebase_passes": 0}
+
 
 def _ptr(t):
     return None if t is None else C.c_void_p(t.data_ptr())
@@ -109,16 +112,18 @@ def _upload_orbit(torch, re, im, ref_len, slot, tag):
     d_im = get_scratch_device_array_1d(n, np.float64, f"{tag}_im_{slot}")[:n]
     d_re.copy_(torch.from_numpy(np.ascontiguousarray(re[:n])), non_blocking=False)
     d_im.copy_(torch.from_numpy(np.ascontiguousarray(im[:n])), non_blocking=False)
+    LAST_FRAME_STATS["h2d_bytes"] += 16 * n
     return d_re, d_im
 
 
-def _build_bla(L, d_re, d_im, ref_len, fractal_type, tol, gen_n, gen_kr, gen_ki, slot, stream_h):
+def _build_bla(L, d_re, d_im, ref_len, fractal_type, tol, gen_n, gen_kr, gen_ki, slot, stream_h,
+               tag="ref"):
     from .engine import get_scratch_device_array_1d
     n = BLA_LEVELS * max(ref_len, 1) * 5
-    table = get_scratch_device_array_1d(n, np.float64, f"bla_table_{slot}")[:n]
-    _lib.check(L.ap_build_bla(_ptr(d_re), _ptr(d_im), int(ref_len), int(fractal_type),
+    table = get_scratch_device_array_1d(n, np.float64, f"bla_table_{tag}_{slot}")[:n]
+    _lib.launch(L.ap_build_bla, _ptr(d_re), _ptr(d_im), int(ref_len), int(fractal_type),
                               float(tol), BLA_LEVELS, int(gen_n), float(gen_kr), float(gen_ki),
-                              _ptr(table), stream_h), "ap_build_bla")
+                              _ptr(table), stream_h, what="ap_build_bla")
     return table
 
 
@@ -154,6 +159,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
             e_scale = 0
     strict = 1 if ("Auto Rebasing" in glitch_mode or "Strict" in glitch_mode
                    or "Pauldelbrot" in glitch_mode) else 0
+    LAST_FRAME_STATS.update(h2d_bytes=0, d2h_bytes=0, rebase_passes=0)
 
     bcx, bcy, bu, bv, re, im, ref_len = hp.find_optimal_reference_orbit(
         center_x_dec, center_y_dec, plot_width_dec, plot_height_dec, max_iter, W, H,
@@ -183,7 +189,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     # BLA variant (NaN guard), their histogram resolve passes the plain one (escape glitch).
     unified_flags = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_NAN_GUARD
     resolve_flags = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_ESCAPE_GLITCH
-    fr.glitch_in.zero_()
+    _lib.device_op(fr.glitch_in.zero_)
     orbit = (d_re, d_im)
     cdf = None
 
@@ -193,30 +199,30 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         p.mode = abi.AP_MODE_COARSE
         p.flags = unified_flags | abi.AP_FLAG_NO_RGB
         b = _buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
-        _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
-        _lib.check(L.ap_histogram_cdf(_ptr(fr.iter), W, H, max_iter, num_bins, _ptr(hist), _ptr(cdf),
-                                      stream_h), "ap_histogram_cdf")
-        _lib.check(L.ap_colour(C.byref(p), C.byref(b), stream_h), "ap_colour")
+        _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
+        _lib.launch(L.ap_histogram_cdf, _ptr(fr.iter), W, H, max_iter, num_bins, _ptr(hist), _ptr(cdf),
+                                      stream_h, what="ap_histogram_cdf")
+        _lib.launch(L.ap_colour, C.byref(p), C.byref(b), stream_h, what="ap_colour")
         if factor > 1:
             fr.edge_mask()
-            _lib.check(L.ap_edge_detect(_ptr(fr.iter), _ptr(fr.edge), W, H,
-                                        float(np.float32(edge_threshold)), stream_h), "ap_edge_detect")
+            _lib.launch(L.ap_edge_detect, _ptr(fr.iter), _ptr(fr.edge), W, H,
+                                        float(np.float32(edge_threshold)), stream_h, what="ap_edge_detect")
             q = _resolve_params(p, resolve_flags, cpu_sem)
             b = _buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla if cpu_sem else None)
-            _lib.check(L.ap_resolve_hist_pass(C.byref(q), C.byref(b), stream_h), "ap_resolve_hist_pass")
+            _lib.launch(L.ap_resolve_hist_pass, C.byref(q), C.byref(b), stream_h, what="ap_resolve_hist_pass")
     else:
         p.mode = abi.AP_MODE_COARSE
         p.flags = unified_flags
         b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
-        _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
+        _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
         if factor > 1:
             fr.edge_mask()
-            _lib.check(L.ap_edge_detect(_ptr(fr.iter), _ptr(fr.edge), W, H,
-                                        float(np.float32(edge_threshold)), stream_h), "ap_edge_detect")
+            _lib.launch(L.ap_edge_detect, _ptr(fr.iter), _ptr(fr.edge), W, H,
+                                        float(np.float32(edge_threshold)), stream_h, what="ap_edge_detect")
             p.mode = abi.AP_MODE_EDGE
             p.flags = unified_flags | (0 if cpu_sem else abi.AP_FLAG_ITER_LAST_SUB)
             b = _buffers(fr, lut, orbit=orbit, bla=bla)
-            _lib.check(L.ap_render_pass(C.byref(p), C.byref(b), stream_h), "ap_render_pass")
+            _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
 
     allow = strict == 1
     if not (allow and plot_width_dec < Decimal("1e-12")):
@@ -229,11 +235,14 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     while state.passes < MAX_REBASE_PASSES:
         st.synchronize()
         h_glitch = fr.glitch_out.cpu().numpy()
+        LAST_FRAME_STATS["d2h_bytes"] += h_glitch.nbytes
         n_gl = int(np.count_nonzero(h_glitch))
         if not state.should_continue(n_gl):
             break
         state.passes += 1
         h_iter = fr.iter.cpu().numpy()
+        LAST_FRAME_STATS["d2h_bytes"] += h_iter.nbytes
+        LAST_FRAME_STATS["rebase_passes"] = state.passes
         chosen = select_rebase_pixel(h_glitch, h_iter, max_iter, state.visited, W, H)
         if chosen is None:
             break
@@ -252,10 +261,12 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
                                      fractal_type=fractal_type, julia_cx=julia_cx,
                                      julia_cy=julia_cy, gen_n=gen_n, gen_kr=gen_kr,
                                      gen_ki=gen_ki, is_floatexp=floatexp)
-        d_re, d_im = _upload_orbit(torch, r_re, r_im, r_len, slot, "rebase")
-        fr.glitch_in.copy_(torch.from_numpy(h_glitch))
+        # Each pass keeps its own orbit and table, so a recorded frame can be replayed.
+        tag = f"rebase{state.passes}"
+        d_re, d_im = _upload_orbit(torch, r_re, r_im, r_len, slot, tag)
+        _lib.device_op(lambda: fr.glitch_in.copy_(fr.glitch_out))
         bla = _build_bla(L, d_re, d_im, r_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
-                         slot, stream_h) if use_bla else None
+                         slot, stream_h, tag) if use_bla else None
         q = _copy_params(p)
         q.ref_px, q.ref_py = float(g_col) * float(factor), float(g_row) * float(factor)
         q.ref_cx, q.ref_cy = float(r_cx), float(r_cy)
@@ -266,25 +277,25 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         if scheme == 11 and cdf is not None:
             q = _resolve_params(q, resolve_flags, cpu_sem)
             b = _buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla if cpu_sem else None, kmap=kmap, s64=s64)
-            _lib.check(L.ap_resolve_hist_pass(C.byref(q), C.byref(b), stream_h), "ap_resolve_hist_pass")
+            _lib.launch(L.ap_resolve_hist_pass, C.byref(q), C.byref(b), stream_h, what="ap_resolve_hist_pass")
         elif factor == 1:
             q.mode = abi.AP_MODE_COARSE
             q.flags = unified_flags
             b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
-            _lib.check(L.ap_render_pass(C.byref(q), C.byref(b), stream_h), "ap_render_pass")
+            _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
         else:
             b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
             if cpu_sem:
                 # CPU reference: coarse re-render of glitched pixels, then their supersample.
                 q.mode = abi.AP_MODE_COARSE
                 q.flags = unified_flags
-                _lib.check(L.ap_render_pass(C.byref(q), C.byref(b), stream_h), "ap_render_pass")
+                _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
                 q.mode = abi.AP_MODE_FULL
                 b = _buffers(fr, lut, orbit=orbit, bla=bla)
             else:
                 q.mode = abi.AP_MODE_FULL
                 q.flags = unified_flags | abi.AP_FLAG_ITER_LAST_SUB
-            _lib.check(L.ap_render_pass(C.byref(q), C.byref(b), stream_h), "ap_render_pass")
+            _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
     if exhaustive:
         st.synchronize()
         if int(torch.count_nonzero(fr.glitch_out)) > 0:

@@ -26,7 +26,7 @@ extern "C" {
 #define AP_API
 #endif
 
-#define AP_ABI_VERSION 1
+#define AP_ABI_VERSION 2
 
 /* Return codes. */
 #define AP_OK 0
@@ -107,6 +107,11 @@ typedef struct ApFrameBuffers {
     uint8_t* glitch_out;       /* [H, W] */
     int32_t* kmap;             /* optional [H, W]: escape step; -1 never escaped, -2 cardioid/bulb skip */
     double* s64;               /* optional [H, W]: smooth value in float64, -1 = interior */
+    int32_t* counters;         /* optional [H, W, 4]: work done for the pixel by this pass, summed
+                                  over its sub-samples: [0] iterations stepped one at a time
+                                  (direct tiers; perturbation stage 1), [1] BLA leaps taken,
+                                  [2] perturbation stage-2 (direct) steps, [3] zero.  16-byte aligned;
+                                  written only for pixels the pass evaluates. */
 } ApFrameBuffers;
 
 /* Library identity. */
@@ -160,6 +165,10 @@ AP_API int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stre
 AP_API int ap_build_bla(const double* ref_re, const double* ref_im, int32_t ref_len, int32_t fractal_type,
                  double tol, int32_t levels, int32_t gen_n, double gen_kr, double gen_ki,
                  double* out, void* stream);
+
+/* Measurement helper (no counterpart in the reference): number of kernels this
+ * library has launched in the process so far. */
+AP_API uint64_t ap_launch_counter(void);
 
 /* Measurement helper (no counterpart in the reference): dependent-FMA throughput
  * probe, precision 64 or 32, blocks x 256 threads x 8 chains x iters FMAs.

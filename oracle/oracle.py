@@ -88,7 +88,7 @@ def pert_grid(params, ref_re, ref_im, bla, xs, ys):
     k = np.empty((H, W), np.int32)
     _check(lib().apo_pert_grid(C.byref(params), C.byref(b), ptr(xs), ptr(ys), W, H, ptr(s), ptr(g),
                                ptr(k)), "pert_grid")
-    return s, g
+    return s, g, k
 
 
 def build_bla(ref_re, ref_im, ref_len, fractal_type, tol, levels, gen_n, gen_kr, gen_ki):

@@ -82,7 +82,7 @@ def test_perturbation_samples_bit_exact(name, variant):
                        bla_levels=m["bla_shape"][0] if use_bla else 0,
                        strict_glitch=1 if variant == "bla" else 0,
                        flags=abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD)
-    s, g = oracle.pert_grid(p, re, im, T, np.arange(0, W, st, dtype=np.float64),
+    s, g, _ = oracle.pert_grid(p, re, im, T, np.arange(0, W, st, dtype=np.float64),
                             np.arange(0, H, st, dtype=np.float64))
     assert np.array_equal(s.view(np.uint32), G[f"{name}__{variant}_s"].view(np.uint32))
     assert np.array_equal(g, G[f"{name}__{variant}_g"])
