@@ -103,7 +103,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
@@ -112,7 +112,13 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
+
+    def mark(self, start=True):
+        if start:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -125,7 +131,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+        for ts, ln in self.lines:
+            if not (t0 <= ts <= t1 + 0.05):
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -363,10 +372,13 @@ def our_arm(args, wl, rank, world, local_rank):
     barrier(world)
     c0 = L.ap_launch_counter()
     with ClockSampler(local_rank) as clocks:
+        time.sleep(0.5)  # let the sampler start before the timed region
         torch.cuda.synchronize()
+        clocks.mark(True)
         step_ms, pass_ev = timed_replay(torch, _lib, rec.ops, stream, args.steps, flush,
                                         record_pass=True)
         torch.cuda.synchronize()
+        clocks.mark(False)
     launches = L.ap_launch_counter() - c0
     barrier(world)
     total_ms = max_over_ranks(float(np.sum(step_ms)), world)
@@ -432,7 +444,7 @@ def our_arm(args, wl, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
