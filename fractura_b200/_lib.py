@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libapeiron_b200.so")
 EXPORTS = (
     "ap_abi_version", "ap_last_error", "ap_render_pass", "ap_resolve_hist_pass",
     "ap_edge_detect", "ap_histogram_cdf", "ap_colour", "ap_build_bla", "ap_fma_peak_launch",
-    "ap_histogram_cdf_noalloc", "ap_launch_counter",
+    "ap_histogram_cdf_noalloc", "ap_launch_counter", "ap_pack_orbit", "ap_pack_bla",
 )
 
 
@@ -57,6 +57,8 @@ def load():
     L.ap_fma_peak_launch.argtypes = [i32, i32, i32, vp, C.POINTER(C.c_double), vp]
     L.ap_histogram_cdf_noalloc.argtypes = [vp, i32, i32, i32, i32, vp, vp]
     L.ap_launch_counter.restype = C.c_uint64
+    L.ap_pack_orbit.argtypes = [vp, vp, i32, vp, vp]
+    L.ap_pack_bla.argtypes = [vp, i32, i32, vp, vp]
     for name in EXPORTS:
         fn = getattr(L, name)
         if fn.restype is None:

@@ -102,6 +102,7 @@ __global__ void __launch_bounds__(256) colour_kernel(const ApFrameParams p, cons
     const int j = blockIdx.y * 16 + (threadIdx.x >> 4);
     if (i >= p.width || j >= p.height) return;
     const size_t idx = (size_t)j * p.width + i;
+    if (p.rebase_pass > 0 && b.glitch_in != nullptr && b.glitch_in[idx] == 0) return;
     const double s = (double)b.iter_map[idx];
     double r = 0.0, g = 0.0, bb = 0.0;
     if (s >= 0.0) colour_of(p, b.lut, b.cdf, hist != 0, s, r, g, bb);

@@ -21,6 +21,10 @@ constexpr double kBailout = 65536.0;
 void set_error(const char* fmt, ...);
 int check_launch(const char* what);
 
+// Coarse-pass perturbation kernel on packed inputs (ap_perturb_fast.cu);
+// AP_E_UNSUPPORTED when the pass is not one it serves.
+int launch_perturb_fast(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st);
+
 struct SampleOut {
     float s;      // float32 smooth value (reference storage type), -1 interior
     double s64;   // float64 smooth value

@@ -1,0 +1,63 @@
+// ap_pack.cu -- device re-layout of the reference orbit and the BLA table into
+// the records the perturbation kernels read (one load per step, one 128-byte
+// row per level search).  Values are copied or computed exactly as the
+// per-step code computes them, so results do not change.
+#include "ap_common.cuh"
+
+namespace ap {
+
+__global__ void __launch_bounds__(256) pack_orbit_kernel(const double* __restrict__ re,
+                                                         const double* __restrict__ im, int n,
+                                                         double4* __restrict__ out) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const double rx = re[k], ry = im[k];
+    const double r_mag2 = rx * rx + ry * ry;
+    const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;
+    out[k] = make_double4(rx, ry, thr, r_mag2);
+}
+
+__global__ void __launch_bounds__(256) pack_bla_kernel(const double* __restrict__ T, int levels,
+                                                       int ref_len, double* __restrict__ R,
+                                                       double4* __restrict__ AB) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one (k, d) pair per thread
+    if (t >= ref_len * 16) return;
+    const int k = t >> 4, d = t & 15;
+    if (d < levels) {
+        const double* e = T + ((size_t)d * ref_len + k) * 5;
+        R[t] = e[4];
+        AB[t] = make_double4(e[0], e[1], e[2], e[3]);
+    } else {
+        R[t] = 0.0;
+        AB[t] = make_double4(0.0, 0.0, 0.0, 0.0);
+    }
+}
+
+}  // namespace ap
+
+extern "C" int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref_len,
+                             double* out, void* stream) {
+    if (!ref_re || !ref_im || !out || ref_len < 0 || (reinterpret_cast<uintptr_t>(out) & 31u)) {
+        ap::set_error("ap_pack_orbit: bad arguments (out must be 32-byte aligned)");
+        return AP_E_INVALID;
+    }
+    const int n = ref_len + 1;
+    ap::pack_orbit_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        ref_re, ref_im, n, reinterpret_cast<double4*>(out));
+    return ap::check_launch("pack_orbit_kernel");
+}
+
+extern "C" int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len, double* out,
+                           void* stream) {
+    if (!table || !out || levels < 1 || levels > 16 || ref_len < 1 ||
+        (reinterpret_cast<uintptr_t>(out) & 31u)) {
+        ap::set_error("ap_pack_bla: bad arguments (1 <= levels <= 16, out 32-byte aligned)");
+        return AP_E_INVALID;
+    }
+    double* R = out;
+    double4* AB = reinterpret_cast<double4*>(out + (size_t)ref_len * 16);
+    const int n = ref_len * 16;
+    ap::pack_bla_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        table, levels, ref_len, R, AB);
+    return ap::check_launch("pack_bla_kernel");
+}

@@ -208,6 +208,10 @@ static int dispatch(const ApFrameParams* p, const ApFrameBuffers* b, int hist_re
     int rc = validate_frame(p, b, hist_resolve);
     if (rc != AP_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (!hist_resolve) {
+        rc = launch_perturb_fast(*p, *b, st);
+        if (rc != AP_E_UNSUPPORTED) return rc;
+    }
     switch (p->tier) {
     case AP_TIER_FP64: return launch_arith<AP_TIER_FP64>(*p, *b, hist_resolve, st);
     case AP_TIER_DD: return launch_arith<AP_TIER_DD>(*p, *b, hist_resolve, st);

@@ -127,6 +127,37 @@ def _build_bla(L, d_re, d_im, ref_len, fractal_type, tol, gen_n, gen_kr, gen_ki,
     return table
 
 
+def _pack_orbit(L, d_re, d_im, ref_len, slot, tag, stream_h):
+    from .engine import get_scratch_device_array_1d
+    n = 4 * (ref_len + 1)
+    packed = get_scratch_device_array_1d(n, np.float64, f"{tag}_orbit_packed_{slot}")[:n]
+    _lib.launch(L.ap_pack_orbit, _ptr(d_re), _ptr(d_im), int(ref_len), _ptr(packed), stream_h,
+                what="ap_pack_orbit")
+    return packed
+
+
+def _pack_bla(L, table, ref_len, slot, tag, stream_h):
+    from .engine import get_scratch_device_array_1d
+    n = 80 * max(ref_len, 1)
+    packed = get_scratch_device_array_1d(n, np.float64, f"bla_packed_{tag}_{slot}")[:n]
+    _lib.launch(L.ap_pack_bla, _ptr(table), BLA_LEVELS, int(ref_len), _ptr(packed), stream_h,
+                what="ap_pack_bla")
+    return packed
+
+
+def _inputs(L, d_re, d_im, ref_len, bla, slot, tag, stream_h):
+    """Packed orbit (always) and packed BLA table (when leaps are used)."""
+    po = _pack_orbit(L, d_re, d_im, ref_len, slot, tag, stream_h)
+    pb = _pack_bla(L, bla, ref_len, slot, tag, stream_h) if (bla is not None and ref_len > 0) else None
+    return po, pb
+
+
+def _with_packed(b, packed):
+    b.orbit_packed = _ptr(packed[0])
+    b.bla_packed = _ptr(packed[1])
+    return b
+
+
 def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_iter, center_x_dec,
                               center_y_dec, plot_width_dec, tier, scheme, num_bins, fractal_type,
                               julia_cx, julia_cy, bbsa_tol, bbsa_order, glitch_mode, gen_n, gen_kr,
@@ -174,6 +205,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     use_bla = bbsa_order == 32 and fractal_type in (0, 2, 4) and not (cpu_sem and scheme == 11)
     bla = _build_bla(L, d_re, d_im, ref_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
                      slot, stream_h) if use_bla else None
+    packed = _inputs(L, d_re, d_im, ref_len, bla, slot, "ref", stream_h)
 
     p.dx_hi, p.dy_hi = dx_f / float(factor), dy_f / float(factor)
     p.ref_px = float(W - 1) * float(bu) * float(factor)
@@ -198,7 +230,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         cdf = get_scratch_device_array((num_bins,), np.float32, f"cdf_lut_{slot}")
         p.mode = abi.AP_MODE_COARSE
         p.flags = unified_flags | abi.AP_FLAG_NO_RGB
-        b = _buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
+        b = _with_packed(_buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed)
         _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
         _lib.launch(L.ap_histogram_cdf, _ptr(fr.iter), W, H, max_iter, num_bins, _ptr(hist), _ptr(cdf),
                                       stream_h, what="ap_histogram_cdf")
@@ -212,9 +244,11 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
             _lib.launch(L.ap_resolve_hist_pass, C.byref(q), C.byref(b), stream_h, what="ap_resolve_hist_pass")
     else:
         p.mode = abi.AP_MODE_COARSE
-        p.flags = unified_flags
-        b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
+        p.flags = unified_flags | abi.AP_FLAG_NO_RGB
+        b = _with_packed(_buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed)
         _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
+        _lib.launch(L.ap_colour, C.byref(p), C.byref(b), stream_h, what="ap_colour")
+        p.flags = unified_flags
         if factor > 1:
             fr.edge_mask()
             _lib.launch(L.ap_edge_detect, _ptr(fr.iter), _ptr(fr.edge), W, H,
@@ -267,6 +301,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         _lib.device_op(lambda: fr.glitch_in.copy_(fr.glitch_out))
         bla = _build_bla(L, d_re, d_im, r_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
                          slot, stream_h, tag) if use_bla else None
+        packed = _inputs(L, d_re, d_im, r_len, bla, slot, tag, stream_h)
         q = _copy_params(p)
         q.ref_px, q.ref_py = float(g_col) * float(factor), float(g_row) * float(factor)
         q.ref_cx, q.ref_cy = float(r_cx), float(r_cy)
@@ -280,16 +315,19 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
             _lib.launch(L.ap_resolve_hist_pass, C.byref(q), C.byref(b), stream_h, what="ap_resolve_hist_pass")
         elif factor == 1:
             q.mode = abi.AP_MODE_COARSE
-            q.flags = unified_flags
-            b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
+            q.flags = unified_flags | abi.AP_FLAG_NO_RGB
+            b = _with_packed(_buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed)
             _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
+            _lib.launch(L.ap_colour, C.byref(q), C.byref(b), stream_h, what="ap_colour")
         else:
             b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)
             if cpu_sem:
                 # CPU reference: coarse re-render of glitched pixels, then their supersample.
                 q.mode = abi.AP_MODE_COARSE
-                q.flags = unified_flags
+                q.flags = unified_flags | abi.AP_FLAG_NO_RGB
+                b = _with_packed(b, packed)
                 _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
+                q.flags = unified_flags
                 q.mode = abi.AP_MODE_FULL
                 b = _buffers(fr, lut, orbit=orbit, bla=bla)
             else:

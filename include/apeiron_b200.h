@@ -26,7 +26,7 @@ extern "C" {
 #define AP_API
 #endif
 
-#define AP_ABI_VERSION 2
+#define AP_ABI_VERSION 3
 
 /* Return codes. */
 #define AP_OK 0
@@ -112,6 +112,8 @@ typedef struct ApFrameBuffers {
                                   (direct tiers; perturbation stage 1), [1] BLA leaps taken,
                                   [2] perturbation stage-2 (direct) steps, [3] zero.  16-byte aligned;
                                   written only for pixels the pass evaluates. */
+    const double* orbit_packed; /* optional [ref_len + 1, 4] from ap_pack_orbit */
+    const double* bla_packed;   /* optional, from ap_pack_bla (needs orbit_packed) */
 } ApFrameBuffers;
 
 /* Library identity. */
@@ -141,6 +143,21 @@ AP_API int ap_edge_detect(const float* iter_map, uint8_t* edge_mask, int32_t wid
 AP_API int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height, int32_t max_iter,
                      int32_t num_bins, int32_t* hist, float* cdf, void* stream);
 
+/* Reference orbit in the layout the perturbation kernels read: per step the
+ * 32-byte record (Z_re, Z_im, Pauldelbrot threshold, |Z|^2), the threshold being
+ * 1e-6 |Z|^2 where |Z|^2 > 1e-8 and -1 elsewhere (the glitch test of
+ * math_core/cpu_kernels.py:428-431 as one compare).  out: [ref_len + 1, 4] float64. */
+AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref_len, double* out,
+                         void* stream);
+
+/* Chained-BLA table in the layout the perturbation kernels read: the 16 radii of
+ * step k in one 128-byte row ([ref_len, 16] float64), then the coefficients
+ * (A_re, A_im, B_re, B_im) per step and level ([ref_len, 16, 4] float64); levels
+ * at or above `levels` hold radius 0.  table: the [levels, ref_len, 5] layout of
+ * ap_build_bla.  out: 80 * ref_len float64. */
+AP_API int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len, double* out,
+                       void* stream);
+
 /* Largest num_bins ap_histogram_cdf_noalloc accepts (its built-in scratch, 256 KiB per GPU). */
 #define AP_NOALLOC_MAX_BINS 65536
 
@@ -156,7 +173,9 @@ AP_API int ap_histogram_cdf_noalloc(const float* iter_map, int32_t width, int32_
 
 /* Colour every pixel from its smooth value.  With scheme 11 the CDF table is used
  * (apply_histogram_equalization_kernel, math_core/cuda_kernels.py:2016); otherwise
- * the closed-form transfer function (recolor_iter_map_cuda_kernel, :3201). */
+ * the closed-form transfer function (recolor_iter_map_cuda_kernel, :3201).  With
+ * p->rebase_pass > 0 only pixels whose glitch_in is set are coloured (the pixels a
+ * rebase pass re-rendered). */
 AP_API int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stream);
 
 /* Chained-BLA table from a reference orbit, built on the device.

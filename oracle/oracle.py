@@ -21,10 +21,19 @@ def build():
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+def _stale():
+    if not os.path.exists(LIB_PATH):
+        return True
+    t = os.path.getmtime(LIB_PATH)
+    deps = [os.path.join(HERE, "ap_oracle.c"), os.path.join(HERE, "Makefile"),
+            os.path.join(os.path.dirname(HERE), "include", "apeiron_b200.h")]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
+        if _stale():
             build()
         L = C.CDLL(LIB_PATH)
         P = C.POINTER(abi.ApFrameParams)

@@ -81,3 +81,32 @@ def test_pert_frame_with_rebasing(name, arith):
     assert n_bad == 0, (n_bad, max_diff)
     if arith == "ref_cpu" and name != "cfg3_hist_ssaa2":
         assert np.array_equal(it.view(np.uint32), RS[name + "__iter"].view(np.uint32))
+
+
+def test_packed_orbit_and_bla_layouts():
+    """ap_pack_orbit / ap_pack_bla records hold exactly what the per-step code computes."""
+    import torch
+    m = next(x for x in PMETA if x["name"] == "cfg3")
+    re, im, rl = PS["cfg3__re"], PS["cfg3__im"], m["ref_len"]
+    L = _lib.load()
+    d_re, d_im = torch.from_numpy(re).cuda(), torch.from_numpy(im).cuda()
+    po = torch.empty((rl + 1, 4), dtype=torch.float64, device="cuda")
+    _lib.check(L.ap_pack_orbit(C.c_void_p(d_re.data_ptr()), C.c_void_p(d_im.data_ptr()), rl,
+                               C.c_void_p(po.data_ptr()), None), "ap_pack_orbit")
+    got = po.cpu().numpy()
+    r2 = re * re + im * im
+    assert np.array_equal(got[:, 0], re) and np.array_equal(got[:, 1], im)
+    assert np.array_equal(got[:, 3], r2)
+    assert np.array_equal(got[:, 2], np.where(r2 > 1e-8, 1e-6 * r2, -1.0))
+    T = oracle.build_bla(re, im, rl, 0, 1e-6, 16, 3, 0.25, 1.0)
+    d_T = torch.from_numpy(T).cuda()
+    pb = torch.empty(80 * rl, dtype=torch.float64, device="cuda")
+    _lib.check(L.ap_pack_bla(C.c_void_p(d_T.data_ptr()), 16, rl, C.c_void_p(pb.data_ptr()), None),
+               "ap_pack_bla")
+    pb = pb.cpu().numpy()
+    R = pb[:16 * rl].reshape(rl, 16)
+    AB = pb[16 * rl:].reshape(rl, 16, 4)
+    assert np.array_equal(R, T[:, :, 4].T)
+    assert np.array_equal(AB, np.transpose(T[:, :, :4], (1, 0, 2)))
+    # radii never increase with the level (the level search relies on it)
+    assert np.all(np.diff(R, axis=1) <= 0)
