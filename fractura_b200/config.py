@@ -54,6 +54,11 @@ GLITCH_CORRECTION_MODES = ["Off (Single-Ref)", "Pauldelbrot", "Strict Metric"]
 
 DYNAMIC_ITER_MODES = ["Off", "On (Sqrt Scaling)", "On (Linear Scaling)", "On (Adaptive Preview)"]
 
+# Per-step tolerance of the "accurate" chained-BLA form: the dropped quadratic term
+# of a leap stays within ~1e-14 of the linear one, i.e. at FP64 rounding level, so
+# leaps change smooth values no more than FP64 rounding of the skipped steps does.
+ACCURATE_BLA_EPS = 1e-14
+
 # Arithmetic profiles (see include/apeiron_b200.h): which multiply-adds are fused.
 ARITH_PROFILES = {"ref_cpu": 0, "ref_cuda": 1}
 
@@ -136,6 +141,13 @@ class RenderParameters:
     d_iter_buf: object = None
     h_iter_buf: object = None
     stream_slot: int = 0
+    # Engine options (no counterpart in the reference): arithmetic profile of the FP64
+    # tiers ("ref_cpu" / "ref_cuda") and the perturbation delta form ("fp64" / "fp32").
+    arith: str = "ref_cpu"
+    delta_form: str = "fp64"
+    # Chained-BLA table: "reference" (the reference's merge at bbsa_tol) or
+    # "accurate" (dc-aware merge at ACCURATE_BLA_EPS).
+    bla_form: str = "reference"
 
     def to_dict(self):
         return asdict(self)

@@ -108,6 +108,81 @@ __global__ void __launch_bounds__(256) bla_merge_kernel(double* __restrict__ T, 
     o[4] = rc <= 0.0 ? 0.0 : (rc > 0.25 ? 0.25 : rc);
 }
 
+// dc-aware merge (Zhuoran's chained BLA, fractalforums.org 2021): the second
+// leap starts from dz1 = A1 dz + B1 dc, so it is valid while
+// |A1| |dz| + |B1| |dc|max < r2, i.e.
+//   r = max(0, min(r1, (r2 - |B1| dcmax) / |A1|)).
+// Radii are stored squared as in the reference layout; the coefficients are
+// merged exactly as in bla_merge_kernel.
+__global__ void __launch_bounds__(256) bla_merge_dc_kernel(double* __restrict__ T, int ref_len, int d,
+                                                           int step, double dc_max) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ref_len - 2 * step) return;
+    const size_t L = (size_t)ref_len;
+    const double* e1 = T + ((size_t)(d - 1) * L + k) * 5;
+    const double* e2 = T + ((size_t)(d - 1) * L + k + step) * 5;
+    double* o = T + ((size_t)d * L + k) * 5;
+    const double r1s = e1[4], r2s = e2[4];
+    if (!(r1s > 0.0 && r2s > 0.0)) return;
+    const double a1r = e1[0], a1i = e1[1], b1r = e1[2], b1i = e1[3];
+    const double a2r = e2[0], a2i = e2[1], b2r = e2[2], b2i = e2[3];
+    const double ar = fma(a2r, a1r, -(a2i * a1i));
+    const double ai = fma(a2i, a1r, a2r * a1i);
+    const double br = fma(a2r, b1r, -(a2i * b1i)) + b2r;
+    const double bi = fma(a2i, b1r, fma(a2r, b1i, b2i));
+    if (fma(ar, ar, ai * ai) > 1e150 || fma(br, br, bi * bi) > 1e150) {
+        o[0] = o[1] = o[2] = o[3] = o[4] = 0.0;
+        return;
+    }
+    const double a1_mag = sqrt(fma(a1i, a1i, a1r * a1r));
+    const double b1_mag = sqrt(fma(b1i, b1i, b1r * b1r));
+    double r = sqrt(r1s);
+    if (a1_mag > 1e-300) {
+        const double r2c = (sqrt(r2s) - b1_mag * dc_max) / a1_mag;
+        r = r < r2c ? r : r2c;
+    }
+    if (!(r > 0.0)) return;
+    o[0] = ar;
+    o[1] = ai;
+    o[2] = br;
+    o[3] = bi;
+    const double rs = r * r;
+    o[4] = rs < r1s ? rs : r1s;  // sqrt then square may round up by an ulp
+}
+
+// Level 0 then one merge launch per level; dc_max < 0 selects the reference merge.
+static int build_bla_levels(const double* ref_re, const double* ref_im, int ref_len, int fractal_type,
+                            double tol, double dc_max, int levels, int gen_n, double gen_kr,
+                            double gen_ki, double* out, cudaStream_t st, const char* what) {
+    const size_t bytes = sizeof(double) * 5 * (size_t)levels * (size_t)ref_len;
+    if (bytes == 0) return AP_OK;
+    cudaError_t e = cudaMemsetAsync(out, 0, bytes, st);
+    if (e != cudaSuccess) {
+        set_error("%s: memset: %s", what, cudaGetErrorString(e));
+        return AP_E_CUDA;
+    }
+    if (!(fractal_type == 0 || fractal_type == 2 || fractal_type == 4) || ref_len < 4 || !(tol > 0.0))
+        return AP_OK;
+    const int blocks = (ref_len + 255) / 256;
+    bla_level0_kernel<<<blocks, 256, 0, st>>>(ref_re, ref_im, ref_len, fractal_type, tol, gen_n,
+                                              gen_kr, gen_ki, out);
+    int rc = check_launch("bla_level0_kernel");
+    int step = 1;
+    for (int d = 1; d < levels && rc == AP_OK; ++d) {
+        if (ref_len - 2 * step > 0) {
+            if (dc_max < 0.0) {
+                bla_merge_kernel<<<blocks, 256, 0, st>>>(out, ref_len, d, step);
+                rc = check_launch("bla_merge_kernel");
+            } else {
+                bla_merge_dc_kernel<<<blocks, 256, 0, st>>>(out, ref_len, d, step, dc_max);
+                rc = check_launch("bla_merge_dc_kernel");
+            }
+        }
+        step *= 2;
+    }
+    return rc;
+}
+
 }  // namespace ap
 
 extern "C" int ap_build_bla(const double* ref_re, const double* ref_im, int32_t ref_len,
@@ -118,27 +193,21 @@ extern "C" int ap_build_bla(const double* ref_re, const double* ref_im, int32_t 
         ap::set_error("ap_build_bla: bad arguments");
         return AP_E_INVALID;
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const size_t bytes = sizeof(double) * 5 * (size_t)levels * (size_t)ref_len;
-    if (bytes == 0) return AP_OK;
-    cudaError_t e = cudaMemsetAsync(out, 0, bytes, st);
-    if (e != cudaSuccess) {
-        ap::set_error("ap_build_bla: memset: %s", cudaGetErrorString(e));
-        return AP_E_CUDA;
+    return ap::build_bla_levels(ref_re, ref_im, ref_len, fractal_type, tol, -1.0, levels, gen_n,
+                                gen_kr, gen_ki, out, static_cast<cudaStream_t>(stream),
+                                "ap_build_bla");
+}
+
+extern "C" int ap_build_bla_dc(const double* ref_re, const double* ref_im, int32_t ref_len,
+                               int32_t fractal_type, double eps, double dc_max, int32_t levels,
+                               int32_t gen_n, double gen_kr, double gen_ki, double* out,
+                               void* stream) {
+    if (!ref_re || !ref_im || !out || ref_len < 0 || levels < 1 || levels > 31 || gen_n < 0 ||
+        gen_n > 64 || !(dc_max >= 0.0) || !(eps > 0.0)) {
+        ap::set_error("ap_build_bla_dc: bad arguments");
+        return AP_E_INVALID;
     }
-    if (!(fractal_type == 0 || fractal_type == 2 || fractal_type == 4) || ref_len < 4 || !(tol > 0.0))
-        return AP_OK;
-    const int blocks = (ref_len + 255) / 256;
-    ap::bla_level0_kernel<<<blocks, 256, 0, st>>>(ref_re, ref_im, ref_len, fractal_type, tol, gen_n,
-                                                  gen_kr, gen_ki, out);
-    int rc = ap::check_launch("bla_level0_kernel");
-    int step = 1;
-    for (int d = 1; d < levels && rc == AP_OK; ++d) {
-        if (ref_len - 2 * step > 0) {
-            ap::bla_merge_kernel<<<blocks, 256, 0, st>>>(out, ref_len, d, step);
-            rc = ap::check_launch("bla_merge_kernel");
-        }
-        step *= 2;
-    }
-    return rc;
+    return ap::build_bla_levels(ref_re, ref_im, ref_len, fractal_type, eps, dc_max, levels, gen_n,
+                                gen_kr, gen_ki, out, static_cast<cudaStream_t>(stream),
+                                "ap_build_bla_dc");
 }

@@ -25,6 +25,9 @@ int check_launch(const char* what);
 // AP_E_UNSUPPORTED when the pass is not one it serves.
 int launch_perturb_fast(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st);
 
+// FP32-mantissa FloatExp tier (ap_fe32.cu).
+int launch_fe32(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st);
+
 struct SampleOut {
     float s;      // float32 smooth value (reference storage type), -1 interior
     double s64;   // float64 smooth value

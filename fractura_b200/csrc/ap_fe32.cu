@@ -1,0 +1,356 @@
+// ap_fe32.cu -- FP32-mantissa FloatExp perturbation (AP_TIER_FLOATEXP32).
+//
+// The engine's fast form of the perturbation tiers.  The delta is held as
+//   dz = w * 2^e,  w a complex float32 with max(|w_re|, |w_im|) in [1, 2)
+// after renormalisation, e an int32 exponent; delta_c = dcm * 2^-E with dcm a
+// complex float32 and E the frame's exponent scale.  One Mandelbrot/Julia step
+//   w' = 2 Z w + S w^2 + D,   S = 2^e (float, 0 below 2^-149),  D = dcm 2^(-E-e)
+// runs in FP32; the exponent changes only when |w| leaves [2^-16, 2^16]
+// (exact power-of-two rescaling, as the FP64 FloatExp tier of the reference
+// does with its 2^16 steps, math_core/cuda_kernels.py:913-923).
+//
+// What stays FP64 (and how):
+//   * the reference orbit: FP64 records (ap_pack_orbit) feed every FP64
+//     decision; the FP32 step reads a float copy (ap_pack_fe32);
+//   * BLA validity radii: r^2 * 2^B in FP64 (B a power-of-two bias so that
+//     |dz|^2 * 2^B does not underflow near any radius), compared with
+//     (double)|w|^2 * 2^(2e + B);
+//   * the Pauldelbrot glitch test |Z + dz|^2 < 1e-6 |Z|^2 and the escape test:
+//     an FP32 screen decides whether they can trigger at this step; when it
+//     can, they are evaluated in FP64 on Z and the exactly converted delta;
+//   * the smooth value at escape and the stage-2 direct iteration (after the
+//     reference escapes) run in FP64.
+// BLA leaps: A = am 2^ea, B = bm 2^eb with float mantissas (ap_pack_fe32);
+// dz' = A dz + B dc keeps exponent e + ea.
+//
+// FP64 slow path.  Two cases leave the FP32 range and take one step (or leap)
+// in FP64 on the same normalised quantities, renormalised in FP64 before the
+// result is narrowed to float: steps where the reference orbit passes close to
+// zero (|Z| < 2^-50: Z itself underflows in float, and 2 Z w loses its
+// exponent; marked by ap_pack_fe32), and deltas whose scale is so far from
+// dc's that the power-of-two factor of the dc term leaves [2^-120, 2^120].
+//
+// The radius bias is a constant 2^600: radii lie in [2^-1074, 1/4], so r^2 2^600
+// stays finite and normal, and |dz|^2 2^600 only saturates (to 0 or inf) where
+// it is far from every radius -- where the comparison's outcome is certain.
+#include "ap_common.cuh"
+
+namespace ap {
+
+constexpr int kRadiusBias = 600;
+
+struct Fe32Bla {        // 32 bytes per (step, level)
+    float ar, ai, br, bi;
+    int ea, eb, pad0, pad1;
+};
+
+__device__ __forceinline__ float exp2i_f(int n) {  // 2^n as float: 0 below 2^-126, 2^127 above
+    n = min(n, 127);
+    return (n < -126) ? 0.0f : __int_as_float((n + 127) << 23);
+}
+
+__device__ __forceinline__ double exp2i_d(int n) {  // 2^n as double: 0 below 2^-1022, inf above 2^1023
+    return (n < -1022) ? 0.0 : (n > 1023 ? __longlong_as_double(0x7ff0000000000000LL)
+                                         : __longlong_as_double((long long)(n + 1023) << 52));
+}
+
+// Exponent of max(|x|, |y|) (floor(log2)), for non-zero finite inputs.
+__device__ __forceinline__ int ilogb_max(float x, float y) {
+    const float m = fmaxf(fabsf(x), fabsf(y));
+    return ((__float_as_int(m) >> 23) & 0xff) - 127;
+}
+
+// Split a double into (float mantissa in [1, 2), exponent); 0 -> (0, 0).
+__device__ __forceinline__ void split_pair(double re, double im, float& mr, float& mi, int& e) {
+    const double m = fmax(fabs(re), fabs(im));
+    if (!(m > 0.0) || !isfinite(m)) {
+        mr = mi = 0.0f;
+        e = 0;
+        return;
+    }
+    int ex = ((int)((__double_as_longlong(m) >> 52) & 0x7ff)) - 1023;
+    if (ex < -1022) ex = ilogb(m);  // subnormal
+    const double s = ldexp(1.0, -ex);
+    mr = (float)(re * s);
+    mi = (float)(im * s);
+    e = ex;
+}
+
+__global__ void __launch_bounds__(256) pack_fe32_kernel(const double4* __restrict__ orb, int n,
+                                                        const double* __restrict__ T, int levels,
+                                                        int ref_len, float4* __restrict__ orb32,
+                                                        double* __restrict__ Rs,
+                                                        Fe32Bla* __restrict__ AB) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) {
+        const double4 Z = orb[t];
+        // .w = 1 marks a close approach (|Z|^2 < 2^-100) that takes the FP64 slow path
+        orb32[t] = make_float4((float)Z.x, (float)Z.y, (float)Z.w, Z.w < 0x1p-100 ? 1.0f : 0.0f);
+    }
+    if (T == nullptr || Rs == nullptr || t >= ref_len * 16) return;
+    const int k = t >> 4, d = t & 15;
+    Fe32Bla r{0.0f, 0.0f, 0.0f, 0.0f, 0, 0, 0, 0};
+    double rs = 0.0;
+    if (d < levels) {
+        const double* e = T + ((size_t)d * ref_len + k) * 5;
+        rs = ldexp(e[4], kRadiusBias);
+        split_pair(e[0], e[1], r.ar, r.ai, r.ea);
+        split_pair(e[2], e[3], r.br, r.bi, r.eb);
+    }
+    Rs[t] = rs;
+    AB[t] = r;
+}
+
+// Normalise a double pair into (float mantissa with max component in [1, 2), exponent
+// added to e).  Zero stays zero with e unchanged.
+__device__ __forceinline__ void renorm_to_float(double x, double y, float& wx, float& wy, int& e) {
+    const double m = fmax(fabs(x), fabs(y));
+    if (!(m > 0.0) || !isfinite(m)) {
+        wx = (float)x;
+        wy = (float)y;
+        return;
+    }
+    const int ex = ilogb(m);
+    const double f = ldexp(1.0, -ex);
+    wx = (float)(x * f);
+    wy = (float)(y * f);
+    e += ex;
+}
+
+template <bool BLA>
+__global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams p,
+                                                             const ApFrameBuffers b) {
+    constexpr int bias = kRadiusBias;
+    const int i = blockIdx.x * 16 + (threadIdx.x & 15);
+    const int j = blockIdx.y * 16 + (threadIdx.x >> 4);
+    if (i >= p.width || j >= p.height) return;
+    const int idx = j * p.width + i;
+    if (p.rebase_pass > 0 && b.glitch_in[idx] == 0) return;
+
+    const int ref_len = p.ref_len, max_iter = p.max_iter;
+    const double4* __restrict__ orb = reinterpret_cast<const double4*>(b.orbit_packed);
+    const float4* __restrict__ orb32 =
+        reinterpret_cast<const float4*>(b.orbit_packed + 4 * (size_t)(ref_len + 1));
+    const double* __restrict__ Rs = b.bla_packed;
+    const Fe32Bla* __restrict__ AB =
+        reinterpret_cast<const Fe32Bla*>(b.bla_packed + (size_t)ref_len * 16);
+
+    // delta_c = dcm * 2^ec (normalised units: dx_hi = true spacing * 2^E).
+    const double sub_offset = ((double)p.factor - 1.0) * 0.5;
+    const double sub_i = (double)(i * p.factor) + sub_offset;
+    const double sub_j = (double)(j * p.factor) + sub_offset;
+    const double dcy_n = (p.ref_py - sub_j) * p.dy_hi;
+    const double dcx_n = (sub_i - p.ref_px) * p.dx_hi;
+    const bool julia = (p.fractal_type == 2);
+    const int ec = -p.e_scale;
+    const float dcmx = (float)dcx_n, dcmy = (float)dcy_n;
+    const float pdx = julia ? 0.0f : dcmx, pdy = julia ? 0.0f : dcmy;
+
+    float wx = julia ? dcmx : 0.0f, wy = julia ? dcmy : 0.0f;
+    int e = ec;
+    // Renormalise w into [1, 2) and refresh the exponent-dependent scales.
+    float S, Dx, Dy;
+    double P2;
+    auto rescale = [&]() {
+        if (wx != 0.0f || wy != 0.0f) {
+            const int ex = ilogb_max(wx, wy);
+            if (ex != 0) {
+                const float f = exp2i_f(-ex);
+                wx *= f;
+                wy *= f;
+                e += ex;
+            }
+        }
+        S = exp2i_f(e);
+        const float dsc = exp2i_f(ec - e);
+        Dx = pdx * dsc;
+        Dy = pdy * dsc;
+        P2 = exp2i_d(2 * e + bias);
+    };
+    rescale();
+
+    const bool strict = p.strict_glitch > 0;
+    int k = 0, glitch = 0, leaps = 0, skipped = 0, k2 = -1;
+    const int max_level = p.bla_levels - 1;
+    SampleOut o = interior_sample();
+    bool finished = false;
+    const double inv_ln = inv_ln_for(p.fractal_type, p.gen_n);
+
+    while (k < ref_len) {
+        const float4 Z = __ldg(orb32 + k);
+        const float wm2 = wx * wx + wy * wy;
+        // Escape and Pauldelbrot tests can only fire once the delta is not negligible.
+        if (e >= -40 || (strict && k > 15 && e >= -75)) {
+            const float zx = Z.x + wx * S, zy = Z.y + wy * S;
+            const float zm2 = zx * zx + zy * zy;
+            const bool near_escape = e >= -40 && zm2 > 65535.0f;
+            const bool near_glitch = strict && k > 15 && zm2 < 2e-6f * Z.z;
+            if (near_escape || near_glitch) {
+                const double2 Z64 = __ldg(reinterpret_cast<const double2*>(orb + k));
+                const double sc = ldexp(1.0, e);
+                const double ax = Z64.x + (double)wx * sc, ay = Z64.y + (double)wy * sc;
+                const double mag2 = ax * ax + ay * ay;
+                if (mag2 > kBailout) {
+                    o = escaped_sample(k, mag2, inv_ln);
+                    finished = true;
+                    break;
+                }
+                if (near_glitch) {
+                    const double thr = __ldg(reinterpret_cast<const double*>(orb + k) + 2);
+                    if (mag2 < thr) glitch = 1;
+                }
+            }
+        }
+        if (BLA && k < ref_len - 1) {
+            const double dzs = (double)wm2 * P2;
+            const double* row = Rs + (size_t)k * 16;
+            if (dzs < __ldg(row)) {
+                int lo = 0, hi = max_level;
+#pragma unroll 4
+                for (int it = 0; it < 4; ++it) {
+                    if (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (dzs < __ldg(row + mid)) lo = mid;
+                        else hi = mid - 1;
+                    }
+                }
+                const Fe32Bla c = AB[(size_t)k * 16 + lo];
+                // dz' = A dz + B dc = 2^(e + ea) [am w + bm dcm 2^(eb + ec - e - ea)]
+                const int fe = c.eb + ec - e - c.ea;
+                if (fe >= -120 && fe <= 120) {
+                    const float f = exp2i_f(fe);
+                    const float bx = (c.br * pdx - c.bi * pdy) * f;
+                    const float by = (c.br * pdy + c.bi * pdx) * f;
+                    const float nx = fmaf(c.ar, wx, fmaf(-c.ai, wy, bx));
+                    const float ny = fmaf(c.ar, wy, fmaf(c.ai, wx, by));
+                    wx = nx;
+                    wy = ny;
+                    e += c.ea;
+                } else {  // FP64 slow path: the dc term's scale leaves the float range
+                    const double f = ldexp(1.0, fe);
+                    const double bx = ((double)c.br * pdx - (double)c.bi * pdy) * f;
+                    const double by = ((double)c.br * pdy + (double)c.bi * pdx) * f;
+                    const double nx = (double)c.ar * wx - (double)c.ai * wy + bx;
+                    const double ny = (double)c.ar * wy + (double)c.ai * wx + by;
+                    e += c.ea;
+                    renorm_to_float(nx, ny, wx, wy, e);
+                }
+                rescale();
+                k += 1 << lo;
+                ++leaps;
+                skipped += 1 << lo;
+                continue;
+            }
+        }
+        if (Z.w != 0.0f || ec - e > 120) {
+            // FP64 slow path: w' = 2 Z w + 2^e w^2 + dcm 2^(ec - e) on the FP64 orbit.
+            const double2 Z64 = __ldg(reinterpret_cast<const double2*>(orb + k));
+            const double x = wx, y = wy;
+            const double se = ldexp(1.0, e), sd = ldexp(1.0, ec - e);
+            const double nx = 2.0 * (Z64.x * x - Z64.y * y) + se * (x - y) * (x + y) + (double)pdx * sd;
+            const double ny = 2.0 * (Z64.x * y + Z64.y * x) + se * 2.0 * x * y + (double)pdy * sd;
+            renorm_to_float(nx, ny, wx, wy, e);
+            rescale();
+            ++k;
+            continue;
+        }
+        // w' = 2 Z w + S w^2 + D
+        const float tx = fmaf(Z.x, wx, -Z.y * wy);
+        const float ty = fmaf(Z.x, wy, Z.y * wx);
+        const float sq_x = (wx - wy) * (wx + wy);
+        const float sq_y = 2.0f * wx * wy;
+        const float nx = fmaf(2.0f, tx, fmaf(S, sq_x, Dx));
+        const float ny = fmaf(2.0f, ty, fmaf(S, sq_y, Dy));
+        wx = nx;
+        wy = ny;
+        const float mx = fmaxf(fabsf(wx), fabsf(wy));
+        if (mx > 65536.0f || (mx < 1.52587890625e-05f && mx > 0.0f)) rescale();
+        ++k;
+    }
+
+    if (!finished) {
+        // Stage 2: FP64 direct iteration from Z_ref_len + dz, c = ref_c + dc.
+        const double2 Zend = __ldg(reinterpret_cast<const double2*>(orb + ref_len));
+        const double sc = ldexp(1.0, e);
+        double zx = Zend.x + (double)wx * sc, zy = Zend.y + (double)wy * sc;
+        const double dct_x = dcx_n * ldexp(1.0, ec), dct_y = dcy_n * ldexp(1.0, ec);
+        const double cx = julia ? p.julia_cx_hi : p.ref_cx + dct_x;
+        const double cy = julia ? p.julia_cy_hi : p.ref_cy + dct_y;
+        if (ref_len < max_iter) glitch = 1;
+        k2 = k;
+        const bool nan_guard = (p.flags & AP_FLAG_NAN_GUARD) != 0;
+        while (k < max_iter) {
+            const double zx2 = zx * zx, zy2 = zy * zy;
+            const double mag2 = zx2 + zy2;
+            if (nan_guard && (isnan(mag2) || isinf(mag2))) {
+                o.s = (float)k;
+                o.s64 = (double)k;
+                o.k = k;
+                glitch = 1;
+                break;
+            }
+            if (mag2 > kBailout) {
+                o = escaped_sample(k, mag2, inv_ln);
+                break;
+            }
+            zy = 2.0 * zx * zy + cy;
+            zx = zx2 - zy2 + cx;
+            ++k;
+        }
+    }
+    const int k_end = (o.k == -1) ? max_iter : k;
+    b.iter_map[idx] = o.s;
+    if (b.kmap) b.kmap[idx] = o.k;
+    if (b.s64) b.s64[idx] = o.s64;
+    if (b.glitch_out) b.glitch_out[idx] = glitch ? 1 : 0;
+    if (b.counters) {
+        const int it1 = (k2 < 0 ? k_end : k2) - skipped;
+        const int it2 = k2 < 0 ? 0 : k_end - k2;
+        reinterpret_cast<int4*>(b.counters)[idx] = make_int4(it1, leaps, it2, 0);
+    }
+}
+
+int launch_fe32(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
+    const bool bla = p.bla_levels > 1;
+    if (p.tier != AP_TIER_FLOATEXP32)
+        return AP_E_UNSUPPORTED;
+    if (p.mode != AP_MODE_COARSE || !(p.flags & AP_FLAG_NO_RGB)) {
+        set_error("AP_TIER_FLOATEXP32 serves coarse passes without in-kernel colour (set AP_FLAG_NO_RGB)");
+        return AP_E_INVALID;
+    }
+    if (p.fractal_type != 0 && p.fractal_type != 2) {
+        set_error("AP_TIER_FLOATEXP32 serves Mandelbrot and Julia (fractal_type 0, 2)");
+        return AP_E_UNSUPPORTED;
+    }
+    if (!b.orbit_packed || (bla && !b.bla_packed) || p.bla_levels > 16 || p.bbsa_skip > 0) {
+        set_error("AP_TIER_FLOATEXP32 needs ap_pack_fe32 inputs (orbit_packed, bla_packed) and no series start");
+        return AP_E_INVALID;
+    }
+    dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
+    if (bla)
+        fe32_coarse_kernel<true><<<grid, 256, 0, st>>>(p, b);
+    else
+        fe32_coarse_kernel<false><<<grid, 256, 0, st>>>(p, b);
+    return check_launch("fe32_coarse_kernel");
+}
+
+}  // namespace ap
+
+extern "C" int ap_pack_fe32(const double* orbit_packed, int32_t ref_len, const double* table,
+                            int32_t levels, double* orbit32_out, double* bla_out, void* stream) {
+    if (!orbit_packed || !orbit32_out || ref_len < 0 || (table && (!bla_out || levels < 1 ||
+        levels > 16)) || (reinterpret_cast<uintptr_t>(orbit32_out) & 15u) ||
+        (bla_out && (reinterpret_cast<uintptr_t>(bla_out) & 31u))) {
+        ap::set_error("ap_pack_fe32: bad arguments");
+        return AP_E_INVALID;
+    }
+    const int n = ref_len + 1;
+    const int m = table ? ref_len * 16 : 0;
+    const int total = n > m ? n : m;
+    double* Rs = bla_out;
+    ap::Fe32Bla* AB = bla_out ? reinterpret_cast<ap::Fe32Bla*>(bla_out + (size_t)ref_len * 16) : nullptr;
+    ap::pack_fe32_kernel<<<(total + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        reinterpret_cast<const double4*>(orbit_packed), n, table, levels, ref_len,
+        reinterpret_cast<float4*>(orbit32_out), Rs, AB);
+    return ap::check_launch("pack_fe32_kernel");
+}

@@ -208,6 +208,13 @@ static int dispatch(const ApFrameParams* p, const ApFrameBuffers* b, int hist_re
     int rc = validate_frame(p, b, hist_resolve);
     if (rc != AP_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (p->tier == AP_TIER_FLOATEXP32) {
+        if (hist_resolve) {
+            set_error("histogram resolve passes use the FP64 tiers");
+            return AP_E_UNSUPPORTED;
+        }
+        return launch_fe32(*p, *b, st);
+    }
     if (!hist_resolve) {
         rc = launch_perturb_fast(*p, *b, st);
         if (rc != AP_E_UNSUPPORTED) return rc;

@@ -26,7 +26,7 @@ import numpy as np
 from . import abi
 from . import _lib
 from .config import (
-    ARITH_PROFILES, GLOBAL_MAX_ITER, RenderParameters, compute_floatexp_scale,
+    ACCURATE_BLA_EPS, ARITH_PROFILES, GLOBAL_MAX_ITER, RenderParameters, compute_floatexp_scale,
     compute_required_prec_bits, decimal_context,
 )
 from .palette import LUT_SIZE, check_lut, synthetic_lut
@@ -328,13 +328,17 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
                       compute_device="GPU", cpu_threads=2, palette_offset=0.0,
                       color_density=1.0, color_contrast=1.0, sync_stream=True,
                       d_iter_buf=None, h_iter_buf=None, stream_slot=None, arith=None,
-                      _extra_out=None):
+                      delta_form=None, bla_form=None, _extra_out=None):
     """Render one frame and return its RGB image (math_core/engine.py:1339-2135).
 
     Same arguments as the reference; ``arith`` optionally selects the
-    arithmetic profile ("ref_cpu" default, or "ref_cuda").  The smooth
-    iteration map is left in ``d_iter_buf`` (and copied to ``h_iter_buf``
-    when one is given).
+    arithmetic profile ("ref_cpu" default, or "ref_cuda"), ``delta_form``
+    the perturbation delta arithmetic: "fp64" (default, the reference's) or
+    "fp32" (FP32 mantissas with integer exponents on coarse passes of
+    Mandelbrot/Julia frames), ``bla_form`` the chained-BLA table: "reference"
+    (default: the reference's merge at ``bbsa_tol``) or "accurate" (the
+    dc-aware merge at ``ACCURATE_BLA_EPS``).  The smooth iteration map is left in
+    ``d_iter_buf`` (and copied to ``h_iter_buf`` when one is given).
     """
     if isinstance(target_w, RenderParameters):
         q = target_w
@@ -354,7 +358,8 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
             d_iter_buf=getattr(q, "d_iter_buf", d_iter_buf),
             h_iter_buf=getattr(q, "h_iter_buf", h_iter_buf),
             stream_slot=getattr(q, "stream_slot", stream_slot),
-            arith=getattr(q, "arith", arith), _extra_out=_extra_out)
+            arith=getattr(q, "arith", arith), delta_form=getattr(q, "delta_form", delta_form),
+            bla_form=getattr(q, "bla_form", bla_form), _extra_out=_extra_out)
 
     if compute_device == "CPU":
         raise NotImplementedError("this engine renders on the GPU only (compute_device='CPU')")
@@ -377,6 +382,10 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
     if not isinstance(center_y_dec, Decimal):
         center_y_dec = Decimal(str(center_y_dec))
     arith_code = _arith_code(arith if arith is not None else DEFAULT_ARITH)
+    if delta_form not in (None, "fp64", "fp32"):
+        raise ValueError(f"delta_form must be 'fp64' or 'fp32', not {delta_form!r}")
+    if bla_form not in (None, "reference", "accurate"):
+        raise ValueError(f"bla_form must be 'reference' or 'accurate', not {bla_form!r}")
     tier = select_tier(plot_width_dec, precision_mode)
     lut = get_device_lut(cmap_name, is_hdr)
     scheme = int(color_scheme_id)
@@ -407,7 +416,9 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
                 fractal_type=int(fractal_type), julia_cx=julia_cx, julia_cy=julia_cy,
                 bbsa_tol=bbsa_tol, bbsa_order=bbsa_order, glitch_mode=glitch_mode,
                 gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki, edge_threshold=edge_threshold,
-                slot=slot, arith_code=arith_code, extra_out=_extra_out)
+                slot=slot, arith_code=arith_code, extra_out=_extra_out,
+                fp32_deltas=(delta_form == "fp32"),
+                bla_eps=ACCURATE_BLA_EPS if bla_form == "accurate" else None)
 
         out = _copy_to_host(fr.rgb, h_rgb_buf, st)
         if h_iter_buf is not None:

@@ -117,19 +117,35 @@ def _upload_orbit(torch, re, im, ref_len, slot, tag):
 
 
 def _build_bla(L, d_re, d_im, ref_len, fractal_type, tol, gen_n, gen_kr, gen_ki, slot, stream_h,
-               tag="ref"):
+               tag="ref", eps=None, dc_max=None):
+    """The chained-BLA table of one reference orbit: the reference's merge at
+    ``tol``, or with ``eps`` the dc-aware merge for deltas up to ``dc_max``."""
     from .engine import get_scratch_device_array_1d
     n = BLA_LEVELS * max(ref_len, 1) * 5
     table = get_scratch_device_array_1d(n, np.float64, f"bla_table_{tag}_{slot}")[:n]
-    _lib.launch(L.ap_build_bla, _ptr(d_re), _ptr(d_im), int(ref_len), int(fractal_type),
-                              float(tol), BLA_LEVELS, int(gen_n), float(gen_kr), float(gen_ki),
-                              _ptr(table), stream_h, what="ap_build_bla")
+    if eps is None:
+        _lib.launch(L.ap_build_bla, _ptr(d_re), _ptr(d_im), int(ref_len), int(fractal_type),
+                    float(tol), BLA_LEVELS, int(gen_n), float(gen_kr), float(gen_ki),
+                    _ptr(table), stream_h, what="ap_build_bla")
+    else:
+        _lib.launch(L.ap_build_bla_dc, _ptr(d_re), _ptr(d_im), int(ref_len), int(fractal_type),
+                    float(eps), float(dc_max), BLA_LEVELS, int(gen_n), float(gen_kr), float(gen_ki),
+                    _ptr(table), stream_h, what="ap_build_bla_dc")
     return table
+
+
+def max_delta_c(ref_px, ref_py, w_sub, h_sub, dx, dy):
+    """Largest |dc| over a w_sub x h_sub sub-sample grid for a reference at
+    sub-sample (ref_px, ref_py): the farthest corner, widened by 1e-6 so that
+    rounding of the per-pixel deltas stays inside."""
+    ex = max(abs(ref_px), abs(float(w_sub - 1) - ref_px)) * abs(dx)
+    ey = max(abs(ref_py), abs(float(h_sub - 1) - ref_py)) * abs(dy)
+    return float(np.hypot(ex, ey)) * (1.0 + 1e-6)
 
 
 def _pack_orbit(L, d_re, d_im, ref_len, slot, tag, stream_h):
     from .engine import get_scratch_device_array_1d
-    n = 4 * (ref_len + 1)
+    n = 6 * (ref_len + 1)  # FP64 records, then the FP32 copy of the FP32 FloatExp tier
     packed = get_scratch_device_array_1d(n, np.float64, f"{tag}_orbit_packed_{slot}")[:n]
     _lib.launch(L.ap_pack_orbit, _ptr(d_re), _ptr(d_im), int(ref_len), _ptr(packed), stream_h,
                 what="ap_pack_orbit")
@@ -145,23 +161,45 @@ def _pack_bla(L, table, ref_len, slot, tag, stream_h):
     return packed
 
 
-def _inputs(L, d_re, d_im, ref_len, bla, slot, tag, stream_h):
-    """Packed orbit (always) and packed BLA table (when leaps are used)."""
+def _inputs(L, d_re, d_im, ref_len, bla, slot, tag, stream_h, fp32=False):
+    """Packed orbit (always), packed BLA table (when leaps are used) and, for the
+    FP32 FloatExp tier, the FP32 orbit copy and BLA records."""
+    from .engine import get_scratch_device_array_1d
     po = _pack_orbit(L, d_re, d_im, ref_len, slot, tag, stream_h)
     pb = _pack_bla(L, bla, ref_len, slot, tag, stream_h) if (bla is not None and ref_len > 0) else None
-    return po, pb
+    pf = None
+    if fp32:
+        n4 = 4 * (ref_len + 1)
+        if bla is not None and ref_len > 0:
+            nb = 80 * ref_len
+            pf = get_scratch_device_array_1d(nb, np.float64, f"bla_fe32_{tag}_{slot}")[:nb]
+        _lib.launch(L.ap_pack_fe32, _ptr(po), int(ref_len), _ptr(bla) if pf is not None else None,
+                    BLA_LEVELS, _ptr(po[n4:]), _ptr(pf), stream_h, what="ap_pack_fe32")
+    return po, pb, pf
 
 
-def _with_packed(b, packed):
+def _with_packed(b, packed, fp32=False):
     b.orbit_packed = _ptr(packed[0])
-    b.bla_packed = _ptr(packed[1])
+    b.bla_packed = _ptr(packed[2] if fp32 else packed[1])
     return b
+
+
+def _coarse_params(p, fe32):
+    """Params of a coarse pass: the FP32 FloatExp tier in normalised units when enabled."""
+    if fe32 is None:
+        return p
+    q = _copy_params(p)
+    q.tier = abi.AP_TIER_FLOATEXP32
+    q.dx_hi, q.dy_hi, q.e_scale = fe32
+    q.bbsa_skip = 0
+    return q
 
 
 def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_iter, center_x_dec,
                               center_y_dec, plot_width_dec, tier, scheme, num_bins, fractal_type,
                               julia_cx, julia_cy, bbsa_tol, bbsa_order, glitch_mode, gen_n, gen_kr,
-                              gen_ki, edge_threshold, slot, arith_code, extra_out=None):
+                              gen_ki, edge_threshold, slot, arith_code, extra_out=None,
+                              fp32_deltas=False, bla_eps=None):
     """All device passes of one perturbation-tier frame (math_core/engine.py:1718-2113)."""
     import torch
     from .engine import _buffers, get_scratch_device_array
@@ -188,6 +226,13 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
                     bbsa_tol = 1e-6
         else:
             e_scale = 0
+        # FP32 FloatExp tier: the same spacing in units of 2^-E (E from config.py:51).
+        fe32 = None
+        if fp32_deltas and fractal_type in (0, 2):
+            fe_e = compute_floatexp_scale(plot_width_dec)
+            fe32 = (float(plot_width_dec * (Decimal(2) ** fe_e) / Decimal(max(1, W - 1))) / float(factor),
+                    float(plot_height_dec * (Decimal(2) ** fe_e) / Decimal(max(1, H - 1))) / float(factor),
+                    int(fe_e))
     strict = 1 if ("Auto Rebasing" in glitch_mode or "Strict" in glitch_mode
                    or "Pauldelbrot" in glitch_mode) else 0
     LAST_FRAME_STATS.update(h2d_bytes=0, d2h_bytes=0, rebase_passes=0)
@@ -203,13 +248,15 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     # The CPU reference's histogram path evaluates samples without BLA leaps
     # (math_core/engine.py:624-637, cpu_kernels.py:1887); every other path leaps.
     use_bla = bbsa_order == 32 and fractal_type in (0, 2, 4) and not (cpu_sem and scheme == 11)
-    bla = _build_bla(L, d_re, d_im, ref_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
-                     slot, stream_h) if use_bla else None
-    packed = _inputs(L, d_re, d_im, ref_len, bla, slot, "ref", stream_h)
-
     p.dx_hi, p.dy_hi = dx_f / float(factor), dy_f / float(factor)
     p.ref_px = float(W - 1) * float(bu) * float(factor)
     p.ref_py = float(H - 1) * float(bv) * float(factor)
+    ws, hs = W * factor, H * factor
+    bla = _build_bla(L, d_re, d_im, ref_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
+                     slot, stream_h, eps=bla_eps,
+                     dc_max=max_delta_c(p.ref_px, p.ref_py, ws, hs, p.dx_hi, p.dy_hi)) if use_bla else None
+    packed = _inputs(L, d_re, d_im, ref_len, bla, slot, "ref", stream_h, fp32=fe32 is not None)
+
     p.ref_cx, p.ref_cy = float(bcx), float(bcy)
     p.julia_cx_hi, p.julia_cy_hi = float(julia_cx), float(julia_cy)
     p.ref_len = int(ref_len)
@@ -230,8 +277,10 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         cdf = get_scratch_device_array((num_bins,), np.float32, f"cdf_lut_{slot}")
         p.mode = abi.AP_MODE_COARSE
         p.flags = unified_flags | abi.AP_FLAG_NO_RGB
-        b = _with_packed(_buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed)
-        _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
+        b = _with_packed(_buffers(fr, lut, cdf=cdf, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed,
+                         fe32 is not None)
+        q = _coarse_params(p, fe32)
+        _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
         _lib.launch(L.ap_histogram_cdf, _ptr(fr.iter), W, H, max_iter, num_bins, _ptr(hist), _ptr(cdf),
                                       stream_h, what="ap_histogram_cdf")
         _lib.launch(L.ap_colour, C.byref(p), C.byref(b), stream_h, what="ap_colour")
@@ -245,8 +294,10 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     else:
         p.mode = abi.AP_MODE_COARSE
         p.flags = unified_flags | abi.AP_FLAG_NO_RGB
-        b = _with_packed(_buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed)
-        _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
+        b = _with_packed(_buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed,
+                         fe32 is not None)
+        q = _coarse_params(p, fe32)
+        _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
         _lib.launch(L.ap_colour, C.byref(p), C.byref(b), stream_h, what="ap_colour")
         p.flags = unified_flags
         if factor > 1:
@@ -300,8 +351,10 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         d_re, d_im = _upload_orbit(torch, r_re, r_im, r_len, slot, tag)
         _lib.device_op(lambda: fr.glitch_in.copy_(fr.glitch_out))
         bla = _build_bla(L, d_re, d_im, r_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
-                         slot, stream_h, tag) if use_bla else None
-        packed = _inputs(L, d_re, d_im, r_len, bla, slot, tag, stream_h)
+                         slot, stream_h, tag, eps=bla_eps,
+                         dc_max=max_delta_c(float(g_col) * factor, float(g_row) * factor, ws, hs,
+                                            p.dx_hi, p.dy_hi)) if use_bla else None
+        packed = _inputs(L, d_re, d_im, r_len, bla, slot, tag, stream_h, fp32=fe32 is not None)
         q = _copy_params(p)
         q.ref_px, q.ref_py = float(g_col) * float(factor), float(g_row) * float(factor)
         q.ref_cx, q.ref_cy = float(r_cx), float(r_cy)
@@ -316,8 +369,10 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         elif factor == 1:
             q.mode = abi.AP_MODE_COARSE
             q.flags = unified_flags | abi.AP_FLAG_NO_RGB
-            b = _with_packed(_buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed)
-            _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
+            b = _with_packed(_buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed,
+                             fe32 is not None)
+            qc = _coarse_params(q, fe32)
+            _lib.launch(L.ap_render_pass, C.byref(qc), C.byref(b), stream_h, what="ap_render_pass")
             _lib.launch(L.ap_colour, C.byref(q), C.byref(b), stream_h, what="ap_colour")
         else:
             b = _buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64)

@@ -158,6 +158,17 @@ AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref
 AP_API int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len, double* out,
                        void* stream);
 
+/* Inputs of AP_TIER_FLOATEXP32 (the FP32-mantissa FloatExp fast form).
+ * orbit_packed: the ap_pack_orbit records; orbit32_out: [ref_len + 1] float4 (Z_re,
+ * Z_im, |Z|^2, f) in float32, f = 1 where |Z|^2 < 2^-100 (steps the kernel takes in
+ * FP64) else 0, placed by convention right after the ap_pack_orbit
+ * records so a frame passes one orbit_packed buffer of 6 (ref_len + 1) doubles.
+ * table (optional): the ap_build_bla layout; bla_out then receives 80 ref_len
+ * doubles: the radii r^2 * 2^600 as [ref_len, 16] float64 and per (step, level) a
+ * 32-byte record of float mantissas (A_re, A_im, B_re, B_im) and int exponents. */
+AP_API int ap_pack_fe32(const double* orbit_packed, int32_t ref_len, const double* table,
+                        int32_t levels, double* orbit32_out, double* bla_out, void* stream);
+
 /* Largest num_bins ap_histogram_cdf_noalloc accepts (its built-in scratch, 256 KiB per GPU). */
 #define AP_NOALLOC_MAX_BINS 65536
 
@@ -184,6 +195,16 @@ AP_API int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stre
 AP_API int ap_build_bla(const double* ref_re, const double* ref_im, int32_t ref_len, int32_t fractal_type,
                  double tol, int32_t levels, int32_t gen_n, double gen_kr, double gen_ki,
                  double* out, void* stream);
+
+/* The same table with the dc-aware merge of the published chained-BLA method
+ * (Zhuoran, fractalforums.org 2021): a merged leap is valid while
+ * |dz| < min(r1, (r2 - |B1| dc_max) / |A1|), dc_max being the largest |dc| of the
+ * frame; level 0 is ap_build_bla's with tol = eps.  The reference's merge
+ * (high_precision.py:1195-1230) drops the |B1| dc term, which makes its leaps
+ * inaccurate where dc dominates.  No counterpart in the reference. */
+AP_API int ap_build_bla_dc(const double* ref_re, const double* ref_im, int32_t ref_len,
+                           int32_t fractal_type, double eps, double dc_max, int32_t levels,
+                           int32_t gen_n, double gen_kr, double gen_ki, double* out, void* stream);
 
 /* Measurement helper (no counterpart in the reference): number of kernels this
  * library has launched in the process so far. */

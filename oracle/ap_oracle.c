@@ -781,8 +781,8 @@ static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, do
 /* The reference builds it with a fastmath Numba kernel; the fused forms      */
 /* below are the ones its compiled x86-64 code evaluates.                     */
 /* ------------------------------------------------------------------------- */
-APO_EXPORT int apo_build_bla(const double* re, const double* im, int ref_len, int ft, double tol,
-                             int levels, int gen_n, double kr, double ki, double* T) {
+static int build_bla_impl(const double* re, const double* im, int ref_len, int ft, double tol,
+                          double dc_max, int levels, int gen_n, double kr, double ki, double* T) {
     const size_t L = (size_t)ref_len;
     memset(T, 0, sizeof(double) * (size_t)levels * L * 5);
     if (!(ft == 0 || ft == 2 || ft == 4) || ref_len < 4 || tol <= 0.0) return AP_OK;
@@ -850,6 +850,26 @@ APO_EXPORT int apo_build_bla(const double* re, const double* im, int ref_len, in
             const double a2r = e2[0], a2i = e2[1], b2r = e2[2], b2i = e2[3];
             const double ar = fma(a2r, a1r, -(a2i * a1i));
             const double ai = fma(a2i, a1r, a2r * a1i);
+            if (dc_max >= 0.0) {
+                /* dc-aware merge: the second leap sees |dz1| <= |A1| |dz| + |B1| dcmax. */
+                const double br = fma(a2r, b1r, -(a2i * b1i)) + b2r;
+                const double bi = fma(a2i, b1r, fma(a2r, b1i, b2i));
+                if (fma(ar, ar, ai * ai) > 1e150 || fma(br, br, bi * bi) > 1e150) continue;
+                const double a1_mag = sqrt(fma(a1i, a1i, a1r * a1r));
+                const double b1_mag = sqrt(fma(b1i, b1i, b1r * b1r));
+                double r = sqrt(r1);
+                if (a1_mag > 1e-300) {
+                    const double r2c = (sqrt(r2) - b1_mag * dc_max) / a1_mag;
+                    r = r < r2c ? r : r2c;
+                }
+                if (!(r > 0.0)) continue;
+                o[0] = ar;
+                o[1] = ai;
+                o[2] = br;
+                o[3] = bi;
+                o[4] = r * r < r1 ? r * r : r1; /* sqrt then square may round up by an ulp */
+                continue;
+            }
             const double a_mag2 = fma(ar, ar, ai * ai);
             if (a_mag2 > 1e150) {
                 o[0] = o[1] = o[2] = o[3] = o[4] = 0.0;
@@ -877,6 +897,21 @@ APO_EXPORT int apo_build_bla(const double* re, const double* im, int ref_len, in
         step = step_next;
     }
     return AP_OK;
+}
+
+APO_EXPORT int apo_build_bla(const double* re, const double* im, int ref_len, int ft, double tol,
+                             int levels, int gen_n, double kr, double ki, double* T) {
+    return build_bla_impl(re, im, ref_len, ft, tol, -1.0, levels, gen_n, kr, ki, T);
+}
+
+/* Chained BLA with the dc-aware merge of Zhuoran's published method
+ * (fractalforums.org, 2021): r = max(0, min(r1, (r2 - |B1| dcmax) / |A1|)).
+ * Level 0 is the reference's (high_precision.py:1126-1175) with tol = eps.
+ * No counterpart in the reference. */
+APO_EXPORT int apo_build_bla_dc(const double* re, const double* im, int ref_len, int ft, double eps,
+                                double dc_max, int levels, int gen_n, double kr, double ki, double* T) {
+    if (!(dc_max >= 0.0)) return AP_E_INVALID;
+    return build_bla_impl(re, im, ref_len, ft, eps, dc_max, levels, gen_n, kr, ki, T);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -1019,6 +1054,7 @@ static void pert_grid_row(void* vctx, int j) {
         Sample o = pert_sample_at(c->p, c->b, c->xs[i], c->ys[j]);
         size_t idx = (size_t)j * c->W + i;
         c->s32[idx] = o.s;
+        if (c->b->s64) c->b->s64[idx] = o.s64;
         c->glitch[idx] = (uint8_t)(o.glitch > 0);
         if (c->kmap) c->kmap[idx] = o.k;
     }

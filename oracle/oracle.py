@@ -51,6 +51,9 @@ def lib():
                                     C.c_void_p, C.c_void_p]
         L.apo_build_bla.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
                                     C.c_int, C.c_double, C.c_double, C.c_void_p]
+        L.apo_build_bla_dc.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double,
+                                       C.c_double, C.c_int, C.c_int, C.c_double, C.c_double,
+                                       C.c_void_p]
         _lib = L
     return _lib
 
@@ -80,8 +83,11 @@ def fp64_grid(params, xs, ys):
     return s32, s64, k
 
 
-def pert_grid(params, ref_re, ref_im, bla, xs, ys):
-    """Perturbation samples at sub-sample coordinates xs (columns) x ys (rows)."""
+def pert_grid(params, ref_re, ref_im, bla, xs, ys, with_s64=False):
+    """Perturbation samples at sub-sample coordinates xs (columns) x ys (rows).
+
+    Returns (s float32, glitch, k) and, with ``with_s64``, the float64 smooth value too.
+    """
     re = np.ascontiguousarray(ref_re, np.float64)
     im = np.ascontiguousarray(ref_im, np.float64)
     xs = np.ascontiguousarray(xs, np.float64)
@@ -95,9 +101,22 @@ def pert_grid(params, ref_re, ref_im, bla, xs, ys):
     s = np.empty((H, W), np.float32)
     g = np.empty((H, W), np.uint8)
     k = np.empty((H, W), np.int32)
+    s64 = np.empty((H, W), np.float64)
+    b.s64 = ptr(s64)
     _check(lib().apo_pert_grid(C.byref(params), C.byref(b), ptr(xs), ptr(ys), W, H, ptr(s), ptr(g),
                                ptr(k)), "pert_grid")
+    if with_s64:
+        return s, g, k, s64
     return s, g, k
+
+
+def build_bla_dc(ref_re, ref_im, ref_len, fractal_type, eps, dc_max, levels, gen_n, gen_kr, gen_ki):
+    T = np.zeros((levels, ref_len, 5), np.float64)
+    _check(lib().apo_build_bla_dc(ptr(np.ascontiguousarray(ref_re, np.float64)),
+                                  ptr(np.ascontiguousarray(ref_im, np.float64)), int(ref_len),
+                                  int(fractal_type), float(eps), float(dc_max), int(levels), int(gen_n),
+                                  float(gen_kr), float(gen_ki), ptr(T)), "build_bla_dc")
+    return T
 
 
 def build_bla(ref_re, ref_im, ref_len, fractal_type, tol, levels, gen_n, gen_kr, gen_ki):

@@ -359,7 +359,63 @@ def gen_render3():
     save("render_pert.npz", meta=json.dumps(meta), **out)
 
 
-SECTIONS = {"fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
+# ---------------------------------------------------------------------------
+# Ground truth for precision checks: direct iteration in 700-bit arithmetic
+# (mpmath), independent of the reference and of perturbation theory.
+# ---------------------------------------------------------------------------
+LN_BAIL_CONFIG = 1.7129177284488854  # config.py:26 of the reference
+
+
+def _truth_row(args):
+    import mpmath
+    (cx, cy, width, W, H, cols, row, mi, bits) = args
+    mpmath.mp.prec = bits
+    pw = mpmath.mpf(width)
+    ph = pw * H / W
+    x_min = mpmath.mpf(cx) - pw / 2
+    y_max = mpmath.mpf(cy) + ph / 2
+    y = y_max - ph * row / (H - 1)
+    out = []
+    big = mpmath.mpf(65536)
+    # The smooth term uses the reference's hard-coded LN_BAILOUT_LOG (config.py:26,
+    # 1.09e-5 below ln(0.5 ln 65536)) that its render passes use, so that only the
+    # escape dynamics differ.
+    ln_bailout = mpmath.mpf(LN_BAIL_CONFIG)
+    for col in cols:
+        x = x_min + pw * col / (W - 1)
+        zx = zy = mpmath.mpf(0)
+        val = -1.0
+        for k in range(mi):
+            zx2, zy2 = zx * zx, zy * zy
+            m2 = zx2 + zy2
+            if m2 > big:
+                lm = mpmath.log(m2)
+                val = float(k + 1 - (mpmath.log(lm / 2) - ln_bailout) / mpmath.log(2))
+                break
+            zy = 2 * zx * zy + y
+            zx = zx2 - zy2 + x
+        out.append(val)
+    return out
+
+
+def gen_truth():
+    from multiprocessing import get_context
+    wl = json.load(open(os.path.join(HERE, "workloads.json")))
+    cx, cy = wl["config3_centre"]
+    W, H, mi = 1920, 1080, 20000
+    cols = list(range(0, W, 30))
+    rows = list(range(0, H, 17))
+    t0 = time.time()
+    with get_context("spawn").Pool(os.cpu_count()) as pool:
+        res = pool.map(_truth_row, [(cx, cy, "1e-160", W, H, cols, r, mi, 700) for r in rows])
+    truth = np.array(res, dtype=np.float64)
+    print(f"  truth {truth.shape} in {time.time() - t0:.0f}s, escaped {np.mean(truth >= 0):.3f}")
+    save("truth_cfg3.npz", s=truth, cols=np.array(cols), rows=np.array(rows),
+         meta=json.dumps(dict(width="1e-160", W=W, H=H, max_iter=mi, bits=700,
+                              note="direct z^2+c iteration in 700-bit mpmath at the exact pixel c; smooth term with the reference's LN_BAILOUT_LOG constant")))
+
+
+SECTIONS = {"truth": gen_truth, "fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
             "render3": gen_render3}
 
 if __name__ == "__main__":

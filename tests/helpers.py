@@ -66,12 +66,14 @@ def rgb_mismatch(a, b):
     return int(diff.any(axis=-1).sum()), int(diff.max()) if diff.size else 0
 
 
-def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max_passes=4):
+def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max_passes=4,
+                      bla_eps=None):
     """A perturbation-tier frame through the oracle, pass for pass as the engine issues it
-    (fractura_b200.perturbation.render_perturbation_frame), including the rebase loop."""
+    (fractura_b200.perturbation.render_perturbation_frame), including the rebase loop.
+    ``bla_eps`` selects the dc-aware BLA table (the engine's bla_form="accurate")."""
     from fractura_b200 import high_precision as hp
     from fractura_b200.config import compute_required_prec_bits
-    from fractura_b200.perturbation import RebaseState, select_rebase_pixel
+    from fractura_b200.perturbation import RebaseState, max_delta_c, select_rebase_pixel
     W, H, f, mi = m["W"], m["H"], m["factor"], m["max_iter"]
     ft, scheme = m["fractal_type"], m["scheme"]
     cpu_sem = arith == abi.AP_ARITH_REF_CPU
@@ -90,12 +92,17 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
     use_bla = order == 32 and ft in (0, 2, 4) and not (cpu_sem and scheme == 11)
     tol = 1e-6
 
-    def table(r_re, r_im, r_len):
+    def table(r_re, r_im, r_len, rpx, rpy):
+        if bla_eps is not None:
+            dcm = max_delta_c(rpx, rpy, W * f, H * f, dx_f / f, dy_f / f)
+            return oracle.build_bla_dc(r_re, r_im, r_len, ft, bla_eps, dcm, 16, m["gen_n"], m["gen_kr"],
+                                       m["gen_ki"])
         return oracle.build_bla(r_re, r_im, r_len, ft, tol, 16, m["gen_n"], m["gen_kr"], m["gen_ki"])
 
     fr = oracle.Frame(W, H, lut=synthetic_lut() if lut is None else lut)
     fr.ref_re, fr.ref_im = np.ascontiguousarray(re[:rl + 1]), np.ascontiguousarray(im[:rl + 1])
-    fr.bla = table(re, im, rl) if use_bla else None
+    fr.bla = table(re, im, rl, float(W - 1) * float(bu) * float(f),
+                   float(H - 1) * float(bv) * float(f)) if use_bla else None
     strict = 1 if "Pauldelbrot" in m["glitch_mode"] or "Strict" in m["glitch_mode"] else 0
     p = abi.new_params(width=W, height=H, factor=f, max_iter=mi, fractal_type=ft,
                        tier=abi.AP_TIER_PERTURB, arith=arith, gen_n=m["gen_n"], gen_kr=m["gen_kr"],
@@ -157,7 +164,7 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
             r_cx, r_cy, mi, ft, m["julia_cx"], m["julia_cy"], bits,
             gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"])
         fr.ref_re, fr.ref_im = np.ascontiguousarray(r_re[:r_len + 1]), np.ascontiguousarray(r_im[:r_len + 1])
-        fr.bla = table(r_re, r_im, r_len) if use_bla else None
+        fr.bla = table(r_re, r_im, r_len, float(gc) * f, float(gr) * f) if use_bla else None
         fr.glitch_in[...] = g
         q = abi.ApFrameParams.from_buffer_copy(p)
         q.ref_px, q.ref_py = float(gc) * f, float(gr) * f
