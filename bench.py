@@ -4,26 +4,31 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
 
 Workload (default "cfg3"): 1920x1080 Mandelbrot at width 1e-160 around the
-600-digit centre of tests/golden/workloads.json, max_iter 200000, chained BLA
-(16 levels, tol 1e-6), Pauldelbrot glitch detection and up to 4 rebase
-passes.  A step renders one frame.  The metric is nominal iterations per
+600-digit centre of tests/golden/workloads.json, max_iter 200000, Pauldelbrot
+glitch detection with up to 4 rebase passes.  The measured ("chosen") form
+uses FP64 deltas and the dc-aware chained-BLA table (bla_form="accurate");
+the comparator is the plain FP64-delta form (no BLA) with the same glitch
+handling.  A step renders one frame.  The metric is nominal iterations per
 second: the sum over pixels of the escape step (max_iter for pixels that never
 escape, 0 for cardioid skips), BLA leaps counting the steps they skip.
 
 Rank 0 prints one JSON line:
-  value     device-resident throughput: the frame's recorded device work
-            (render passes, device BLA builds, rebase passes, device copies)
-            replayed with every reference orbit already in HBM; CUDA events
-            per step on the launching stream, a 512 MiB write between steps
-            (L2 flush), max over ranks;
+  value     device-resident throughput of the chosen form: the frame's recorded
+            device work (render passes, device BLA builds, rebase passes, device
+            copies) replayed with every reference orbit already in HBM; CUDA
+            events per step on the launching stream, a 512 MiB write between
+            steps (L2 flush), max over ranks;
   e2e       the same metric through engine.render_frame_ssaa with host
             buffers: orbit search (LRU-cached like the reference's), the
-            four rebase orbits in Decimal, H2D of orbits, D2H of the glitch
-            and iteration maps per rebase pass and of the RGB frame;
-  plain     the plain FP64-delta form (no BLA, no rebasing) on the same view;
-  roofline  FP64 pipe of render_pass_kernel: executed FP64 operations (from
-            the kernel's work counters) / its event-timed duration, against
-            the measured dependent-FMA FP64 peak;
+            rebase orbits in Decimal, H2D of orbits, D2H of the glitch and
+            iteration maps per rebase pass and of the RGB frame;
+  plain_fp64_delta, chosen, forms
+            per form: G iter/s, and (for the 1e-160 view) the smooth error and
+            escape-step agreement against the 700-bit ground truth
+            (tests/golden/truth_cfg3.npz) and against the plain form;
+  roofline  FP64 pipe of the render passes: executed FP64 operations (from the
+            kernels' work counters) / their event-timed duration, against the
+            measured dependent-FMA FP64 peak;
   cpu_baseline, clocks, gpu_launches (kernels launched by the library in
             the timed region, from its own counter).
 Multi-GPU: one process per GPU, every rank renders its own frame (weak
@@ -67,14 +72,17 @@ def workload_cfg3():
     return dict(name="mandelbrot_perturb_bla_pauldelbrot_1920x1080_w1e-160", W=1920, H=1080,
                 max_iter=200000, cx=cx, cy=cy, width="1e-160", scheme=0, factor=1, fractal_type=0,
                 precision_mode="1e-300 (Perturbation)", bbsa_order=32, bbsa_tol=1e-6,
-                glitch_mode="Pauldelbrot", arith="ref_cpu", dtype="f64")
+                glitch_mode="Pauldelbrot", arith="ref_cpu", dtype="f64", bla_form="accurate",
+                form="FP64 deltas, dc-aware chained BLA (eps 1e-14), Pauldelbrot with up to 4 "
+                     "rebase passes")
 
 
 def workload_cfg1():
     return dict(name="mandelbrot_fp64_640x360_hist", W=640, H=360, max_iter=1000, cx="-0.65",
                 cy="0.0", width="4.0", scheme=11, factor=1, fractal_type=0,
                 precision_mode="1e-12 (FP64)", bbsa_order=0, bbsa_tol=0.0,
-                glitch_mode="Off (Single-Ref)", arith="ref_cpu", dtype="f64")
+                glitch_mode="Off (Single-Ref)", arith="ref_cpu", dtype="f64",
+                form="FP64 direct iteration, histogram colouring")
 
 
 WORKLOADS = {"cfg3": workload_cfg3, "cfg1": workload_cfg1}
@@ -191,6 +199,7 @@ def config_of(wl, n_gpus):
     return {"workload": wl["name"], "width": wl["W"], "height": wl["H"], "max_iter": wl["max_iter"],
             "view_width": wl["width"], "ssaa": wl["factor"], "bla": wl["bbsa_order"] == 32,
             "glitch_mode": wl["glitch_mode"], "max_rebase_passes": 4, "arith": wl["arith"],
+            "form": wl.get("form"), "bla_form": wl.get("bla_form", "reference"),
             "l2": "flushed between timed steps (512 MiB write)",
             "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single"}
 
@@ -341,10 +350,59 @@ def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla):
     return total, launches
 
 
+def truth_errors(kmap, s64):
+    """Smooth error and escape-step agreement against the 700-bit ground truth of the
+    1e-160 view (64 x 64 subsample, tests/golden/truth_cfg3.npz)."""
+    path = os.path.join(ROOT, "tests", "golden", "truth_cfg3.npz")
+    t = np.load(path)
+    truth, rows, cols = t["s"], t["rows"], t["cols"]
+    k = kmap[np.ix_(rows, cols)]
+    err = np.abs(s64[np.ix_(rows, cols)] - truth)
+    return {"p50": float(np.median(err)), "p99": float(np.percentile(err, 99)),
+            "p99.9": float(np.percentile(err, 99.9)), "max": float(err.max()),
+            "k_identical": float(np.mean(k == np.floor(truth))), "samples": int(err.size)}
+
+
+class Form:
+    """One engine form of the workload: a recorded frame and its replay timings."""
+
+    def __init__(self, name, over, desc):
+        self.name, self.over, self.desc = name, over, desc
+
+
+def record_form(torch, _lib, engine, wl, stream, form, kmap, s64, warm=2):
+    from fractura_b200 import high_precision as hp
+    hp.clear_reference_orbit_cache()
+    for _ in range(warm):
+        render_call(engine, wl, stream, (kmap, s64), **form.over)
+    torch.cuda.synchronize()
+    with _lib.recording() as rec:
+        render_call(engine, wl, stream, (kmap, s64), **form.over)
+    torch.cuda.synchronize()
+    form.ops = rec.ops
+    form.kmap = kmap.cpu().numpy()
+    form.s64 = s64.cpu().numpy()
+    form.iters = nominal_iterations(form.kmap, wl["max_iter"])
+    from fractura_b200 import perturbation
+    form.stats = dict(perturbation.LAST_FRAME_STATS)
+    return form
+
+
+def summarise_form(form, ms, plain=None, wl=None):
+    out = {"form": form.desc, "ms_per_frame": float(np.median(ms)),
+           "value": form.iters / (float(np.median(ms)) * 1e-3) / 1e9, "unit": "G iter/s",
+           "render_passes": 1 + int(form.stats.get("rebase_passes", 0))}
+    if wl is not None and wl["width"] == "1e-160" and wl["W"] == 1920 and wl["H"] == 1080:
+        out["error_vs_truth"] = truth_errors(form.kmap, form.s64)
+    if plain is not None:
+        out["k_identical_vs_plain"] = float(np.mean(form.kmap == plain.kmap))
+        out["smooth_diff_vs_plain_p99.9"] = float(np.percentile(np.abs(form.s64 - plain.s64), 99.9))
+    return out
+
+
 def our_arm(args, wl, rank, world, local_rank):
     import torch
     from fractura_b200 import _lib, abi, engine
-    from fractura_b200 import high_precision as hp
 
     torch.cuda.set_device(local_rank)
     stream = torch.cuda.Stream()
@@ -353,21 +411,10 @@ def our_arm(args, wl, rank, world, local_rank):
     s64 = torch.empty((H, W), dtype=torch.float64, device="cuda")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     L = _lib.load()
+    perturb = wl["bbsa_order"] == 32
 
-    # Warm-up renders through the public entry point (also fills the orbit cache).
-    hp.clear_reference_orbit_cache()
-    for _ in range(args.warmup):
-        render_call(engine, wl, stream, (kmap, s64))
-    torch.cuda.synchronize()
-    # Record one frame's device work.
-    with _lib.recording() as rec:
-        render_call(engine, wl, stream, (kmap, s64))
-    torch.cuda.synchronize()
-    iters = nominal_iterations(kmap.cpu().numpy(), wl["max_iter"])
-    from fractura_b200 import perturbation
-    n_rebase = perturbation.LAST_FRAME_STATS["rebase_passes"]
-    h2d = perturbation.LAST_FRAME_STATS["h2d_bytes"]
-    d2h = perturbation.LAST_FRAME_STATS["d2h_bytes"] + H * W * 3
+    chosen = Form("chosen", dict(bla_form=wl.get("bla_form", "reference")), wl.get("form", ""))
+    record_form(torch, _lib, engine, wl, stream, chosen, kmap, s64, warm=args.warmup)
 
     barrier(world)
     c0 = L.ap_launch_counter()
@@ -375,43 +422,66 @@ def our_arm(args, wl, rank, world, local_rank):
         time.sleep(0.5)  # let the sampler start before the timed region
         torch.cuda.synchronize()
         clocks.mark(True)
-        step_ms, pass_ev = timed_replay(torch, _lib, rec.ops, stream, args.steps, flush,
+        # NVTX range "timed_region": lets a profiler select exactly the timed launches
+        torch.cuda.nvtx.range_push("timed_region")
+        step_ms, pass_ev = timed_replay(torch, _lib, chosen.ops, stream, args.steps, flush,
                                         record_pass=True)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         clocks.mark(False)
     launches = L.ap_launch_counter() - c0
     barrier(world)
     total_ms = max_over_ranks(float(np.sum(step_ms)), world)
-    value = iters * args.steps * world / (total_ms * 1e-3) / 1e9
+    value = chosen.iters * args.steps * world / (total_ms * 1e-3) / 1e9
 
     # End to end through render_frame_ssaa with a pinned host RGB buffer.
+    e2e_steps = max(3, args.steps // 10)
     h_rgb = torch.empty((H, W, 3), dtype=torch.uint8).pin_memory().numpy()
     barrier(world)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        render_call(engine, wl, stream, h_rgb_buf=h_rgb)
+    for _ in range(e2e_steps):
+        render_call(engine, wl, stream, h_rgb_buf=h_rgb, **chosen.over)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     barrier(world)
-    e2e = iters * args.steps * world / e2e_s / 1e9
+    e2e = chosen.iters * e2e_steps * world / e2e_s / 1e9
+    from fractura_b200 import perturbation
+    h2d = perturbation.LAST_FRAME_STATS["h2d_bytes"] if perturb else 0
+    d2h = (perturbation.LAST_FRAME_STATS["d2h_bytes"] if perturb else 0) + H * W * 3
 
     if rank != 0:
         return
-    # Plain FP64-delta comparator on the same view (no BLA, no rebasing).
-    plain = None
-    if wl["bbsa_order"] == 32:
-        for _ in range(2):
-            render_call(engine, wl, stream, (kmap, s64), bbsa_order=0, glitch_mode="Off (Single-Ref)")
-        with _lib.recording() as prec:
-            render_call(engine, wl, stream, (kmap, s64), bbsa_order=0, glitch_mode="Off (Single-Ref)")
-        torch.cuda.synchronize()
-        p_iters = nominal_iterations(kmap.cpu().numpy(), wl["max_iter"])
-        p_ms, _ = timed_replay(torch, _lib, prec.ops, stream, max(2, args.steps // 2), flush)
-        plain = {"value": p_iters / (float(np.mean(p_ms)) * 1e-3) / 1e9, "unit": "G iter/s",
-                 "ms_per_frame": float(np.mean(p_ms)), "form": "fp64 deltas, no BLA, no rebasing"}
+    line_extra = {}
+    if perturb:
+        n_cmp = max(3, args.steps // 10)
+        plain = record_form(torch, _lib, engine, wl, stream,
+                            Form("plain", dict(bbsa_order=0), "plain FP64 deltas, no BLA, same glitch handling"),
+                            kmap, s64)
+        p_ms, _ = timed_replay(torch, _lib, plain.ops, stream, n_cmp, flush)
+        plain_sum = summarise_form(plain, p_ms, wl=wl)
+        chosen_sum = summarise_form(chosen, step_ms, plain=plain, wl=wl)
+        forms = {}
+        single = dict(glitch_mode="Off (Single-Ref)")
+        extra = [
+            Form("plain_single_reference", dict(bbsa_order=0, **single),
+                 "plain FP64 deltas, one reference, no rebasing"),
+            Form("chosen_single_reference", dict(chosen.over, **single),
+                 chosen.desc + ", one reference, no rebasing"),
+            Form("reference_bla", dict(bla_form="reference"),
+                 "FP64 deltas with the reference's BLA table (tol 1e-6), same glitch handling"),
+            Form("fp32_floatexp", dict(chosen.over, delta_form="fp32"),
+                 "FP32 mantissa + int exponent deltas, accurate BLA, same glitch handling"),
+        ]
+        for f in extra:
+            record_form(torch, _lib, engine, wl, stream, f, kmap, s64)
+            f_ms, _ = timed_replay(torch, _lib, f.ops, stream, n_cmp, flush)
+            forms[f.name] = summarise_form(f, f_ms, plain=plain, wl=wl)
+        single_ratio = forms["chosen_single_reference"]["value"] / forms["plain_single_reference"]["value"]
+        line_extra = {"plain_fp64_delta": plain_sum, "chosen": chosen_sum,
+                      "speedup_vs_plain": value / plain_sum["value"],
+                      "speedup_vs_plain_single_reference": single_ratio, "forms": forms}
 
     strict = "Pauldelbrot" in wl["glitch_mode"] or "Strict" in wl["glitch_mode"]
-    flops, n_pass = pass_flops(torch, _lib, abi, rec.ops, stream, H, W, strict,
-                               wl["bbsa_order"] == 32)
+    flops, n_pass = pass_flops(torch, _lib, abi, chosen.ops, stream, H, W, strict, perturb)
     pass_ms = float(np.sum([a.elapsed_time(b) for a, b in pass_ev])) / args.steps
     peak64 = fma_peak_tflops(64, torch)
     achieved = flops / (pass_ms * 1e-3) / 1e12 if pass_ms > 0 else None
@@ -422,12 +492,13 @@ def our_arm(args, wl, rank, world, local_rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
         "data": "synthetic", "impl": "ours", "config": config_of(wl, world),
-        "nominal_iterations_per_frame": iters, "rebase_passes": n_rebase,
+        "nominal_iterations_per_frame": chosen.iters,
+        "rebase_passes": int(chosen.stats.get("rebase_passes", 0)),
         "e2e": {"value": e2e, "unit": "G iter/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
-        "plain_fp64_delta": plain,
-        "speedup_vs_plain": (value / plain["value"]) if plain else None,
-        "roofline": {"bound": "fp64", "kernel": "render_pass_kernel", "achieved": achieved,
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+        **line_extra,
+        "roofline": {"bound": "fp64", "kernel": "render passes (perturb_coarse_kernel)" if perturb
+                     else "render passes (render_pass_kernel)", "achieved": achieved,
                      "peak": peak64, "unit": "TFLOP/s",
                      "frac": achieved / peak64 if (achieved and peak64) else None,
                      "peak_source": "measured dependent-FMA FP64 probe (ap_fma_peak_launch), this run",
@@ -444,7 +515,7 @@ def our_arm(args, wl, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
