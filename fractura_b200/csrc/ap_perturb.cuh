@@ -214,12 +214,264 @@ __device__ __forceinline__ SampleOut perturb_sample_at(const ApFrameParams& p,
     return done(o, max_iter);
 }
 
+// ---------------------------------------------------------------- FloatExp
+// pow2_f64 of the reference (math_core/cuda_kernels.py:97-102): 2^e, the
+// largest double at e >= 1023 and 0 at e <= -1022, built from its bits.
+__device__ __forceinline__ double pow2_f64(int e) {
+    if (e >= 1023) return 1.7976931348623157e+308;
+    if (e <= -1022) return 0.0;
+    return __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+// Python's max(a, b) on floats: b when b > a, else a (NaN-order preserving).
+__device__ __forceinline__ double py_max(double a, double b) { return b > a ? b : a; }
+
+// Keep the mantissa pair within [2^-16, 2^16] by exact 2^16 rescaling
+// (math_core/cuda_kernels.py:913-923).  The loops stop on non-finite values,
+// where some reference variants would not.
+__device__ __forceinline__ void renorm16(double& x, double& y, int& e) {
+    double mag = py_max(fabs(x), fabs(y));
+    while (mag > 65536.0 && isfinite(mag)) {
+        x *= 1.52587890625e-05;
+        y *= 1.52587890625e-05;
+        e += 16;
+        mag = py_max(fabs(x), fabs(y));
+    }
+    while (mag < 1.52587890625e-05 && mag > 0.0 && isfinite(mag)) {
+        x *= 65536.0;
+        y *= 65536.0;
+        e -= 16;
+        mag = py_max(fabs(x), fabs(y));
+    }
+}
+
+// Pauldelbrot test on the scaled pair (check_glitch_cancellation_floatexp,
+// math_core/cuda_kernels.py:105-135, cpu_kernels.py:171-201).
+__device__ __forceinline__ bool floatexp_glitch(double rx, double ry, double dzx, double dzy,
+                                                int eff_exp) {
+    const double r_max = py_max(fabs(rx), fabs(ry));
+    if (r_max < 1e-4) return false;
+    const double dz_max = py_max(fabs(dzx), fabs(dzy));
+    if (dz_max <= 0.0) return false;
+    const int r_exp = (int)(log(r_max) * 1.4426950408889634);
+    const int dz_exp = (int)(log(dz_max) * 1.4426950408889634);
+    const int diff = r_exp - (eff_exp + dz_exp);
+    if (diff > 10 || diff < -10) return false;
+    const double scale_r = pow2_f64(-r_exp), scale_dz = pow2_f64(eff_exp - r_exp);
+    const double rxs = rx * scale_r, rys = ry * scale_r;
+    const double zx = rxs + dzx * scale_dz, zy = rys + dzy * scale_dz;
+    return zx * zx + zy * zy < 1e-6 * (rxs * rxs + rys * rys);
+}
+
+// FloatExp perturbation: the true delta is (dzx, dzy) 2^(z_exp - E) with the
+// mantissa pair kept in [2^-16, 2^16]; delta_c = dc_norm 2^-E (dx/dy are the
+// normalised spacings).  Semantics of cpu_compute_perturbation_sample_floatexp
+// (math_core/cpu_kernels.py:606-1021) and of the CUDA variants
+// compute_perturbation_sample_floatexp[_bla] (math_core/cuda_kernels.py:819-1499):
+// they differ in the Burning Ship delta form (ARITH), the BLA leap's fused
+// multiply-adds (ARITH) and the stage-2 NaN guard (AP_FLAG_NAN_GUARD).  BBSA
+// starts are never used: the reference maps orders 4/8 to chained BLA here.
 template <int ARITH>
 __device__ __forceinline__ SampleOut floatexp_sample_at(const ApFrameParams& p,
                                                         const ApFrameBuffers& b, double sub_i,
                                                         double sub_j) {
-    (void)p; (void)b; (void)sub_i; (void)sub_j;
-    return interior_sample();
+    constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
+    const int ft = p.fractal_type;
+    const bool julia = (ft == 2 || ft == 3);
+    const int ref_len = p.ref_len, max_iter = p.max_iter, E = p.e_scale;
+    const double* __restrict__ re = b.ref_re;
+    const double* __restrict__ im = b.ref_im;
+    const bool strict = p.strict_glitch > 0;
+    const double dcy = (p.ref_py - sub_j) * p.dy_hi;
+    const double dcx = (sub_i - p.ref_px) * p.dx_hi;
+    double dzx = julia ? dcx : 0.0, dzy = julia ? dcy : 0.0;
+    int z_exp = 0, k = 0;
+    const double dcpx = julia ? 0.0 : dcx, dcpy = julia ? 0.0 : dcy;
+    int glitch = 0, leaps = 0, skipped = 0, k2 = -1;
+    auto done = [&](SampleOut o, int k_end) {
+        o.iters = (k2 < 0 ? k_end : k2) - skipped;
+        o.iters2 = k2 < 0 ? 0 : k_end - k2;
+        o.leaps = leaps;
+        return o;
+    };
+    const int levels = p.bla_levels;
+    const bool has_bla = levels > 1 && b.bla != nullptr && (ft == 0 || ft == 2 || ft == 4);
+    const size_t L = (size_t)ref_len;
+    const double inv_ln = inv_ln_for(ft, p.gen_n);
+
+    while (k < ref_len) {
+        const double rx = __ldg(re + k), ry = __ldg(im + k);
+        const int eff_exp = z_exp - E;
+        if (eff_exp >= -50) {
+            const double sc = pow2_f64(eff_exp);
+            const double zx = rx + dzx * sc, zy = ry + dzy * sc;
+            const double mag2 = zx * zx + zy * zy;
+            if (mag2 > kBailout) {
+                SampleOut o = escaped_sample(k, mag2, inv_ln);
+                o.glitch = glitch;
+                return done(o, k);
+            }
+        }
+        if (strict && k > 15 && floatexp_glitch(rx, ry, dzx, dzy, eff_exp)) glitch = 1;
+
+        if (has_bla && k < ref_len - 1) {
+            // |delta|^2 against r^2 in scaled form, or via square roots far below 2^-510
+            const int shift_r = eff_exp;
+            const bool scaled = shift_r >= -510;
+            double dz_mag2 = 0.0, dz_lin = 0.0;
+            if (scaled) {
+                const double sr = pow2_f64(shift_r);
+                dz_mag2 = (dzx * dzx + dzy * dzy) * (sr * sr);
+            } else {
+                dz_lin = sqrt(dzx * dzx + dzy * dzy) * pow2_f64(max(-1020, shift_r));
+            }
+            auto fits = [&](double r_sq) {
+                return scaled ? (dz_mag2 < r_sq) : (r_sq > 0.0 && dz_lin < sqrt(r_sq));
+            };
+            if (fits(__ldg(b.bla + (size_t)k * 5 + 4))) {
+                int best = 0;
+                for (int d = levels - 1; d > 0; --d) {
+                    if (k + (1 << d) < ref_len && fits(__ldg(b.bla + ((size_t)d * L + k) * 5 + 4))) {
+                        best = d;
+                        break;
+                    }
+                }
+                const double* e = b.bla + ((size_t)best * L + k) * 5;
+                const double ar = __ldg(e), ai = __ldg(e + 1), br = __ldg(e + 2), bi = __ldg(e + 3);
+                const double scale_c = (z_exp >= -1020 && z_exp <= 1020) ? pow2_f64(-z_exp) : 0.0;
+                const double cxs = dcpx * scale_c, cys = dcpy * scale_c;
+                double nx, ny;
+                if (kCpu) {
+                    nx = (ar * dzx - ai * dzy) + (br * cxs - bi * cys);
+                    ny = (ar * dzy + ai * dzx) + (br * cys + bi * cxs);
+                } else {
+                    nx = fma(ar, dzx, fma(-ai, dzy, fma(br, cxs, -bi * cys)));
+                    ny = fma(ar, dzy, fma(ai, dzx, fma(br, cys, bi * cxs)));
+                }
+                dzx = nx;
+                dzy = ny;
+                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) return done(glitch_sample(k), k);
+                renorm16(dzx, dzy, z_exp);
+                k += 1 << best;
+                ++leaps;
+                skipped += 1 << best;
+                continue;
+            }
+        }
+
+        const int shift_nl = z_exp - E;
+        const double scale_c = (z_exp >= -1020 && z_exp <= 1020) ? pow2_f64(-z_exp) : 0.0;
+        if (ft == 0 || ft == 2) {
+            double lx = 2.0 * (rx * dzx - ry * dzy);
+            double ly = 2.0 * (rx * dzy + ry * dzx);
+            if (shift_nl >= -1020) {
+                const double sn = pow2_f64(shift_nl);
+                lx += (dzx * dzx - dzy * dzy) * sn;
+                ly += (2.0 * dzx * dzy) * sn;
+            }
+            dzx = lx + dcpx * scale_c;
+            dzy = ly + dcpy * scale_c;
+        } else if (ft == 1 || ft == 3) {
+            const double sn = shift_nl >= -1020 ? pow2_f64(shift_nl) : 0.0;
+            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+            if (kCpu) {  // math_core/cpu_kernels.py:795-829
+                const double se = eff_exp >= -1020 ? pow2_f64(eff_exp) : 0.0;
+                const double inv = eff_exp <= 1020 ? pow2_f64(-eff_exp) : 0.0;
+                double fx, ex, fy, ey;
+                if ((rx + dzx * se) * sx >= 0.0) { fx = sx; ex = 0.0; }
+                else { fx = -sx; ex = eff_exp <= 1020 ? ((-sx * 2.0) * rx) * inv : 0.0; }
+                if ((ry + dzy * se) * sy >= 0.0) { fy = sy; ey = 0.0; }
+                else { fy = -sy; ey = eff_exp <= 1020 ? ((-sy * 2.0) * ry) * inv : 0.0; }
+                const double lx = (2.0 * rx + dzx * sn) * dzx - (2.0 * ry + dzy * sn) * dzy + dcpx * scale_c;
+                const double dxn = fx * dzx + ex, dyn = fy * dzy + ey;
+                const double ly = 2.0 * (fabs(rx) * dyn + fabs(ry) * dxn + dxn * dyn * sn) - dcpy * scale_c;
+                dzx = lx;
+                dzy = ly;
+            } else {  // math_core/cuda_kernels.py:964-985
+                const double sd = eff_exp >= -60 ? pow2_f64(eff_exp) : 0.0;
+                const double inv = pow2_f64(-eff_exp);
+                const double ddx = (rx + dzx * sd) * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx * inv + dzx);
+                const double ddy = (ry + dzy * sd) * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry * inv + dzy);
+                double lx = 2.0 * (rx * dzx - ry * dzy);
+                double ly = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx);
+                if (shift_nl >= -1020) {
+                    lx += (dzx * dzx - dzy * dzy) * sn;
+                    ly += (2.0 * ddx * ddy) * sn;
+                }
+                dzx = lx + dcpx * scale_c;
+                dzy = ly - dcpy * scale_c;
+            }
+        } else {
+            const double sn = shift_nl >= -1020 ? pow2_f64(shift_nl) : 0.0;
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p.gen_n - 1; ++t) {
+                const cplx t1 = cmul(pr, pi, rx, ry);
+                const cplx t2 = cmul(qr, qi, dzx, dzy);
+                const cplx t3 = cmul(pr, pi, dzx, dzy);
+                pr = t1.r + t2.r + t3.r * sn;
+                pi = t1.i + t2.i + t3.i * sn;
+                const cplx q = cmul(qr, qi, rx, ry);
+                qr = q.r;
+                qi = q.i;
+            }
+            const cplx kz = cmul(p.gen_kr, p.gen_ki, dzx, dzy);
+            dzx = pr + kz.r + dcpx * scale_c;
+            dzy = pi + kz.i + dcpy * scale_c;
+        }
+        renorm16(dzx, dzy, z_exp);
+        ++k;
+    }
+
+    // Stage 2: z = Z_ref_len + delta, then direct FP64 iteration with c = ref_c + dc.
+    const int eff_exp = z_exp - E;
+    const double sfb = eff_exp >= -60 ? pow2_f64(eff_exp) : 0.0;
+    double zx = __ldg(re + ref_len) + dzx * sfb, zy = __ldg(im + ref_len) + dzy * sfb;
+    const double scf = E <= 1020 ? pow2_f64(-E) : 0.0;
+    const double cx = julia ? p.julia_cx_hi : p.ref_cx + dcpx * scf;
+    const double cy = julia ? p.julia_cy_hi : p.ref_cy + dcpy * scf;
+    k2 = k;
+    {
+        const double mag2 = zx * zx + zy * zy;
+        if (mag2 > kBailout) {  // escaped together with the reference at k = ref_len
+            SampleOut o = escaped_sample(ref_len, mag2, inv_ln);
+            o.glitch = glitch;
+            return done(o, k);
+        }
+    }
+    if (ref_len < max_iter) glitch = 1;
+    const bool nan_guard = (p.flags & AP_FLAG_NAN_GUARD) != 0;
+    while (k < max_iter) {
+        const double zx2 = zx * zx, zy2 = zy * zy;
+        const double mag2 = zx2 + zy2;
+        if (nan_guard && (isnan(mag2) || isinf(mag2))) return done(glitch_sample(k), k);
+        if (mag2 > kBailout) {
+            SampleOut o = escaped_sample(k, mag2, inv_ln);
+            o.glitch = glitch;
+            return done(o, k);
+        }
+        if (ft == 0 || ft == 2) {
+            zy = 2.0 * zx * zy + cy;
+            zx = zx2 - zy2 + cx;
+        } else if (ft == 1 || ft == 3) {
+            zy = 2.0 * fabs(zx) * fabs(zy) - cy;
+            zx = zx2 - zy2 + cx;
+        } else {
+            double zr = zx, zi = zy;
+            for (int t = 0; t < p.gen_n - 1; ++t) {
+                const double nr = zr * zx - zi * zy, ni = zr * zy + zi * zx;
+                zr = nr;
+                zi = ni;
+            }
+            const double kzr = p.gen_kr * zx - p.gen_ki * zy;
+            const double kzi = p.gen_kr * zy + p.gen_ki * zx;
+            zx = zr + kzr + cx;
+            zy = zi + kzi + cy;
+        }
+        ++k;
+    }
+    SampleOut o = interior_sample();
+    o.glitch = glitch;
+    return done(o, max_iter);
 }
 
 }  // namespace ap

@@ -10,6 +10,7 @@ and iteration maps back, picks a new reference pixel on the host
 (select_rebase_pixel) and re-renders only the glitched pixels.
 """
 import ctypes as C
+import math
 from decimal import Decimal, localcontext
 
 import numpy as np
@@ -252,9 +253,13 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     p.ref_px = float(W - 1) * float(bu) * float(factor)
     p.ref_py = float(H - 1) * float(bv) * float(factor)
     ws, hs = W * factor, H * factor
+    # |dc|max of the dc-aware table in absolute units (the FloatExp tier's spacing is in 2^-E units)
+    def dc_max_at(rpx, rpy):
+        return math.ldexp(max_delta_c(rpx, rpy, ws, hs, p.dx_hi, p.dy_hi), -int(e_scale))
+
     bla = _build_bla(L, d_re, d_im, ref_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
                      slot, stream_h, eps=bla_eps,
-                     dc_max=max_delta_c(p.ref_px, p.ref_py, ws, hs, p.dx_hi, p.dy_hi)) if use_bla else None
+                     dc_max=dc_max_at(p.ref_px, p.ref_py)) if use_bla else None
     packed = _inputs(L, d_re, d_im, ref_len, bla, slot, "ref", stream_h, fp32=fe32 is not None)
 
     p.ref_cx, p.ref_cy = float(bcx), float(bcy)
@@ -352,8 +357,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         _lib.device_op(lambda: fr.glitch_in.copy_(fr.glitch_out))
         bla = _build_bla(L, d_re, d_im, r_len, fractal_type, bbsa_tol, gen_n, gen_kr, gen_ki,
                          slot, stream_h, tag, eps=bla_eps,
-                         dc_max=max_delta_c(float(g_col) * factor, float(g_row) * factor, ws, hs,
-                                            p.dx_hi, p.dy_hi)) if use_bla else None
+                         dc_max=dc_max_at(float(g_col) * factor, float(g_row) * factor)) if use_bla else None
         packed = _inputs(L, d_re, d_im, r_len, bla, slot, tag, stream_h, fp32=fe32 is not None)
         q = _copy_params(p)
         q.ref_px, q.ref_py = float(g_col) * float(factor), float(g_row) * float(factor)

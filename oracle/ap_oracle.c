@@ -367,6 +367,8 @@ static void put_rgb(const ApFrameParams* p, void* rgb, size_t idx, double r, dou
 static Sample dd_sample_at(const ApFrameParams* p, double sub_i, double sub_j);
 static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
                              double sub_j);
+static Sample floatexp_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
+                                 double sub_j);
 
 /* Sub-sample coordinates (sub_i, sub_j) -> sample, as each unified kernel maps them. */
 static Sample sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i, double sub_j) {
@@ -384,6 +386,8 @@ static Sample sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double 
     }
     case AP_TIER_DD:
         return dd_sample_at(p, sub_i, sub_j);
+    case AP_TIER_FLOATEXP:
+        return floatexp_sample_at(p, b, sub_i, sub_j);
     default:
         return pert_sample_at(p, b, sub_i, sub_j);
     }
@@ -777,6 +781,244 @@ static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, do
 }
 
 /* ------------------------------------------------------------------------- */
+/* FloatExp tier: cpu_compute_perturbation_sample_floatexp                    */
+/* (cpu_kernels.py:606-1021) and compute_perturbation_sample_floatexp[_bla]   */
+/* (cuda_kernels.py:819-1499).  The delta is (dzx, dzy) 2^(z_exp - E); the    */
+/* pixel offsets are in units of 2^-E.  Every operation is written in source  */
+/* order, unfused, except the CUDA BLA leap's explicit fma.                   */
+/* ------------------------------------------------------------------------- */
+static double pow2_f64(int e) { /* cuda_kernels.py:97-102 */
+    if (e >= 1023) return 1.7976931348623157e+308;
+    if (e <= -1022) return 0.0;
+    return ldexp(1.0, e);
+}
+
+static double py_max(double a, double b) { return b > a ? b : a; }
+
+static void renorm16(double* x, double* y, int* e) {
+    double mag = py_max(fabs(*x), fabs(*y));
+    while (mag > 65536.0 && isfinite(mag)) {
+        *x *= 1.52587890625e-05;
+        *y *= 1.52587890625e-05;
+        *e += 16;
+        mag = py_max(fabs(*x), fabs(*y));
+    }
+    while (mag < 1.52587890625e-05 && mag > 0.0 && isfinite(mag)) {
+        *x *= 65536.0;
+        *y *= 65536.0;
+        *e -= 16;
+        mag = py_max(fabs(*x), fabs(*y));
+    }
+}
+
+/* cpu_kernels.py:171-201 */
+static int floatexp_glitch(double rx, double ry, double dzx, double dzy, int eff_exp) {
+    const double r_max = py_max(fabs(rx), fabs(ry));
+    if (r_max < 1e-4) return 0;
+    const double dz_max = py_max(fabs(dzx), fabs(dzy));
+    if (dz_max <= 0.0) return 0;
+    const int r_exp = (int)(log(r_max) * 1.4426950408889634);
+    const int dz_exp = (int)(log(dz_max) * 1.4426950408889634);
+    const int diff = r_exp - (eff_exp + dz_exp);
+    if (diff > 10 || diff < -10) return 0;
+    const double scale_r = pow2_f64(-r_exp), scale_dz = pow2_f64(eff_exp - r_exp);
+    const double rxs = rx * scale_r, rys = ry * scale_r;
+    const double zx = rxs + dzx * scale_dz, zy = rys + dzy * scale_dz;
+    return zx * zx + zy * zy < 1e-6 * (rxs * rxs + rys * rys);
+}
+
+static int bla_fits(int scaled, double dz_mag2, double dz_lin, double r_sq) {
+    return scaled ? (dz_mag2 < r_sq) : (r_sq > 0.0 && dz_lin < sqrt(r_sq));
+}
+
+static Sample floatexp_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
+                                 double sub_j) {
+    const int cpu = p->arith == AP_ARITH_REF_CPU;
+    const int ft = p->fractal_type;
+    const int julia = (ft == 2 || ft == 3);
+    const int ref_len = p->ref_len, max_iter = p->max_iter, E = p->e_scale;
+    const double* re = b->ref_re;
+    const double* im = b->ref_im;
+    const int strict = p->strict_glitch > 0;
+    const double dcy = (p->ref_py - sub_j) * p->dy_hi;
+    const double dcx = (sub_i - p->ref_px) * p->dx_hi;
+    double dzx = julia ? dcx : 0.0, dzy = julia ? dcy : 0.0;
+    int z_exp = 0, k = 0, glitch = 0;
+    const double dcpx = julia ? 0.0 : dcx, dcpy = julia ? 0.0 : dcy;
+    const int levels = p->bla_levels;
+    const int has_bla = levels > 1 && b->bla != NULL && (ft == 0 || ft == 2 || ft == 4);
+    const size_t L = (size_t)ref_len;
+    const double inv_ln = inv_ln_for(ft, p->gen_n);
+
+    while (k < ref_len) {
+        const double rx = re[k], ry = im[k];
+        const int eff_exp = z_exp - E;
+        if (eff_exp >= -50) {
+            const double sc = pow2_f64(eff_exp);
+            const double zx = rx + dzx * sc, zy = ry + dzy * sc;
+            const double mag2 = zx * zx + zy * zy;
+            if (mag2 > BAILOUT) {
+                Sample o = escaped(k, mag2, inv_ln);
+                o.glitch = glitch;
+                return o;
+            }
+        }
+        if (strict && k > 15 && floatexp_glitch(rx, ry, dzx, dzy, eff_exp)) glitch = 1;
+
+        if (has_bla && k < ref_len - 1) {
+            const int scaled = eff_exp >= -510;
+            double dz_mag2 = 0.0, dz_lin = 0.0;
+            if (scaled) {
+                const double sr = pow2_f64(eff_exp);
+                dz_mag2 = (dzx * dzx + dzy * dzy) * (sr * sr);
+            } else {
+                dz_lin = sqrt(dzx * dzx + dzy * dzy) * pow2_f64(eff_exp > -1020 ? eff_exp : -1020);
+            }
+            if (bla_fits(scaled, dz_mag2, dz_lin, b->bla[(size_t)k * 5 + 4])) {
+                int best = 0;
+                for (int d = levels - 1; d > 0; d--) {
+                    if (k + (1 << d) < ref_len &&
+                        bla_fits(scaled, dz_mag2, dz_lin, b->bla[((size_t)d * L + k) * 5 + 4])) {
+                        best = d;
+                        break;
+                    }
+                }
+                const double* e = b->bla + ((size_t)best * L + k) * 5;
+                const double ar = e[0], ai = e[1], br = e[2], bi = e[3];
+                const double scale_c = (z_exp >= -1020 && z_exp <= 1020) ? pow2_f64(-z_exp) : 0.0;
+                const double cxs = dcpx * scale_c, cys = dcpy * scale_c;
+                double nx, ny;
+                if (cpu) {
+                    nx = (ar * dzx - ai * dzy) + (br * cxs - bi * cys);
+                    ny = (ar * dzy + ai * dzx) + (br * cys + bi * cxs);
+                } else {
+                    nx = fma(ar, dzx, fma(-ai, dzy, fma(br, cxs, -bi * cys)));
+                    ny = fma(ar, dzy, fma(ai, dzx, fma(br, cys, bi * cxs)));
+                }
+                dzx = nx;
+                dzy = ny;
+                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) return glitch_at(k);
+                renorm16(&dzx, &dzy, &z_exp);
+                k += 1 << best;
+                continue;
+            }
+        }
+
+        const int shift_nl = z_exp - E;
+        const double scale_c = (z_exp >= -1020 && z_exp <= 1020) ? pow2_f64(-z_exp) : 0.0;
+        if (ft == 0 || ft == 2) {
+            double lx = 2.0 * (rx * dzx - ry * dzy);
+            double ly = 2.0 * (rx * dzy + ry * dzx);
+            if (shift_nl >= -1020) {
+                const double sn = pow2_f64(shift_nl);
+                lx += (dzx * dzx - dzy * dzy) * sn;
+                ly += (2.0 * dzx * dzy) * sn;
+            }
+            dzx = lx + dcpx * scale_c;
+            dzy = ly + dcpy * scale_c;
+        } else if (ft == 1 || ft == 3) {
+            const double sn = shift_nl >= -1020 ? pow2_f64(shift_nl) : 0.0;
+            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+            if (cpu) { /* cpu_kernels.py:795-829 */
+                const double se = eff_exp >= -1020 ? pow2_f64(eff_exp) : 0.0;
+                const double inv = eff_exp <= 1020 ? pow2_f64(-eff_exp) : 0.0;
+                double fx, ex, fy, ey;
+                if ((rx + dzx * se) * sx >= 0.0) { fx = sx; ex = 0.0; }
+                else { fx = -sx; ex = eff_exp <= 1020 ? ((-sx * 2.0) * rx) * inv : 0.0; }
+                if ((ry + dzy * se) * sy >= 0.0) { fy = sy; ey = 0.0; }
+                else { fy = -sy; ey = eff_exp <= 1020 ? ((-sy * 2.0) * ry) * inv : 0.0; }
+                const double lx = (2.0 * rx + dzx * sn) * dzx - (2.0 * ry + dzy * sn) * dzy + dcpx * scale_c;
+                const double dxn = fx * dzx + ex, dyn = fy * dzy + ey;
+                const double ly = 2.0 * (fabs(rx) * dyn + fabs(ry) * dxn + dxn * dyn * sn) - dcpy * scale_c;
+                dzx = lx;
+                dzy = ly;
+            } else { /* cuda_kernels.py:964-985 */
+                const double sd = eff_exp >= -60 ? pow2_f64(eff_exp) : 0.0;
+                const double inv = pow2_f64(-eff_exp);
+                const double ddx = (rx + dzx * sd) * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx * inv + dzx);
+                const double ddy = (ry + dzy * sd) * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry * inv + dzy);
+                double lx = 2.0 * (rx * dzx - ry * dzy);
+                double ly = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx);
+                if (shift_nl >= -1020) {
+                    lx += (dzx * dzx - dzy * dzy) * sn;
+                    ly += (2.0 * ddx * ddy) * sn;
+                }
+                dzx = lx + dcpx * scale_c;
+                dzy = ly - dcpy * scale_c;
+            }
+        } else {
+            const double sn = shift_nl >= -1020 ? pow2_f64(shift_nl) : 0.0;
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p->gen_n - 1; t++) {
+                double t1r, t1i, t2r, t2i, t3r, t3i;
+                c_mul(pr, pi, rx, ry, &t1r, &t1i);
+                c_mul(qr, qi, dzx, dzy, &t2r, &t2i);
+                c_mul(pr, pi, dzx, dzy, &t3r, &t3i);
+                pr = t1r + t2r + t3r * sn;
+                pi = t1i + t2i + t3i * sn;
+                c_mul(qr, qi, rx, ry, &qr, &qi);
+            }
+            double kr, ki;
+            c_mul(p->gen_kr, p->gen_ki, dzx, dzy, &kr, &ki);
+            dzx = pr + kr + dcpx * scale_c;
+            dzy = pi + ki + dcpy * scale_c;
+        }
+        renorm16(&dzx, &dzy, &z_exp);
+        k++;
+    }
+
+    /* Stage 2 (cpu_kernels.py:948-1018) */
+    const int eff_exp = z_exp - E;
+    const double sfb = eff_exp >= -60 ? pow2_f64(eff_exp) : 0.0;
+    double zx = re[ref_len] + dzx * sfb, zy = im[ref_len] + dzy * sfb;
+    const double scf = E <= 1020 ? pow2_f64(-E) : 0.0;
+    const double cx = julia ? p->julia_cx_hi : p->ref_cx + dcpx * scf;
+    const double cy = julia ? p->julia_cy_hi : p->ref_cy + dcpy * scf;
+    {
+        const double mag2 = zx * zx + zy * zy;
+        if (mag2 > BAILOUT) {
+            Sample o = escaped(ref_len, mag2, inv_ln);
+            o.glitch = glitch;
+            return o;
+        }
+    }
+    if (ref_len < max_iter) glitch = 1;
+    const int nan_guard = (p->flags & AP_FLAG_NAN_GUARD) != 0;
+    while (k < max_iter) {
+        const double zx2 = zx * zx, zy2 = zy * zy;
+        const double mag2 = zx2 + zy2;
+        if (nan_guard && (isnan(mag2) || isinf(mag2))) return glitch_at(k);
+        if (mag2 > BAILOUT) {
+            Sample o = escaped(k, mag2, inv_ln);
+            o.glitch = glitch;
+            return o;
+        }
+        if (ft == 0 || ft == 2) {
+            zy = 2.0 * zx * zy + cy;
+            zx = zx2 - zy2 + cx;
+        } else if (ft == 1 || ft == 3) {
+            zy = 2.0 * fabs(zx) * fabs(zy) - cy;
+            zx = zx2 - zy2 + cx;
+        } else {
+            double zr = zx, zi = zy;
+            for (int t = 0; t < p->gen_n - 1; t++) {
+                const double nr = zr * zx - zi * zy, ni = zr * zy + zi * zx;
+                zr = nr;
+                zi = ni;
+            }
+            const double kzr = p->gen_kr * zx - p->gen_ki * zy;
+            const double kzi = p->gen_kr * zy + p->gen_ki * zx;
+            zx = zr + kzr + cx;
+            zy = zi + kzi + cy;
+        }
+        k++;
+    }
+    Sample o = interior();
+    o.glitch = glitch;
+    return o;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Chained BLA table: _jit_build_bla_table (high_precision.py:1101-1238).     */
 /* The reference builds it with a fastmath Numba kernel; the fused forms      */
 /* below are the ones its compiled x86-64 code evaluates.                     */
@@ -1051,7 +1293,8 @@ typedef struct {
 static void pert_grid_row(void* vctx, int j) {
     const PertGridCtx* c = (const PertGridCtx*)vctx;
     for (int i = 0; i < c->W; i++) {
-        Sample o = pert_sample_at(c->p, c->b, c->xs[i], c->ys[j]);
+        Sample o = c->p->tier == AP_TIER_FLOATEXP ? floatexp_sample_at(c->p, c->b, c->xs[i], c->ys[j])
+                                                  : pert_sample_at(c->p, c->b, c->xs[i], c->ys[j]);
         size_t idx = (size_t)j * c->W + i;
         c->s32[idx] = o.s;
         if (c->b->s64) c->b->s64[idx] = o.s64;

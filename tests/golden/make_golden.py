@@ -315,6 +315,82 @@ def gen_pert():
     save("pert_samples.npz", meta=json.dumps(meta), **out)
 
 
+FEXP_SPECS = [
+    # name, fractal_type, width, W, H, max_iter, stride, jx, jy, n, kr, ki  (centre: the pert case's)
+    ("fexp_mandel", 0, "1e-320", 480, 270, 20000, 10, 0.0, 0.0, 3, 0.25, 1.0),
+    ("fexp_ship", 1, "1e-320", 480, 270, 6000, 10, 0.0, 0.0, 3, 0.25, 1.0),
+    ("fexp_julia", 2, "1e-400", 480, 270, 6000, 10, -0.8, 0.156, 3, 0.25, 1.0),
+    ("fexp_multibrot3", 4, "1e-320", 480, 270, 6000, 10, 0.0, 0.0, 3, 0.1, 0.2),
+]
+
+
+def fexp_cases():
+    wl = json.load(open(os.path.join(HERE, "workloads.json")))
+    pc = {c[0]: c for c in pert_cases()}
+    src = {0: "cfg3", 1: "ship", 2: "julia", 4: "multibrot3"}
+    cases = []
+    for (name, ft, w, W, H, mi, stride, jx, jy, n, kr, ki) in FEXP_SPECS:
+        c = pc[src[ft]]
+        cx, cy = (c[2], c[3]) if c[2] is not None else tuple(wl["config3_centre"])
+        cases.append((name, ft, cx, cy, w, W, H, mi, stride, jx, jy, n, kr, ki))
+    cx3, cy3 = wl["config3_centre"]
+    # config 3 at 1e-1000 (the reference's FloatExp tier), every 60th pixel
+    cases.append(("fexp_cfg3", 0, cx3, cy3, "1e-1000", 1920, 1080, 20000, 60, 0.0, 0.0, 3, 0.25, 1.0))
+    return cases
+
+
+def gen_fexp():
+    """Per-sample FloatExp perturbation values (cpu_compute_perturbation_sample_floatexp)."""
+    hp, ck, cfg = R.hp, R.ck, R.config
+    out = {}
+    meta = []
+    for (name, ft, cx, cy, w, W, H, mi, stride, jx, jy, n, kr, ki) in fexp_cases():
+        cfg.ensure_decimal_precision(Decimal(w))
+        pw = Decimal(w)
+        ph = pw * (Decimal(H) / Decimal(W))
+        E = cfg.compute_floatexp_scale(pw)
+        hp.clear_reference_orbit_cache()
+        t0 = time.time()
+        bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
+            Decimal(cx), Decimal(cy), pw, ph, mi, W, H, fractal_type=ft, julia_cx=jx, julia_cy=jy,
+            gen_n=n, gen_kr=kr, gen_ki=ki, is_floatexp=True)
+        t_orbit = time.time() - t0
+        two_e = Decimal(2) ** E
+        dx = float(pw * two_e / Decimal(max(1, W - 1)))
+        dy = float(ph * two_e / Decimal(max(1, H - 1)))
+        ref_px = float(W - 1) * float(bu)
+        ref_py = float(H - 1) * float(bv)
+        tab = hp.build_bla_table(re, im, rl, fractal_type=ft, tol=1e-6, gen_n=n, gen_kr=kr, gen_ki=ki)
+        zero16 = (0.0,) * 16
+        si = np.arange(0, W, stride, dtype=np.float64)
+        sj = np.arange(0, H, stride, dtype=np.float64)
+        res = {}
+        for variant, table, strict in (("plain", np.zeros((1, 1, 1)), 0), ("bla", tab, 1)):
+            s = np.empty((len(sj), len(si)), np.float32)
+            g = np.empty((len(sj), len(si)), np.uint8)
+            for a, jj in enumerate(sj):
+                for b, ii in enumerate(si):
+                    sv, gl = ck.cpu_compute_perturbation_sample_floatexp(
+                        re, im, rl, mi, ref_px, ref_py, float(ii), float(jj), dx, dy, E,
+                        float(bcx), float(bcy), ft, float(jx), float(jy), 0, 1.0, *zero16,
+                        n, kr, ki, strict, INV_LN2, LN_BAIL, bla_table=table)
+                    s[a, b] = sv
+                    g[a, b] = gl
+            res[variant] = (s, g)
+        print(f"  {name}: E {E} ref_len {rl} orbit {t_orbit:.1f}s total {time.time() - t0:.1f}s "
+              f"escaped {np.mean(res['plain'][0] >= 0):.3f} glitched(bla) {res['bla'][1].mean():.3f}")
+        out[name + "__re"] = re[:rl + 1]
+        out[name + "__im"] = im[:rl + 1]
+        for variant in res:
+            out[f"{name}__{variant}_s"] = res[variant][0]
+            out[f"{name}__{variant}_g"] = res[variant][1]
+        meta.append(dict(name=name, fractal_type=ft, cx=cx, cy=cy, width=w, W=W, H=H, max_iter=mi,
+                         stride=stride, julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki,
+                         ref_cx=str(bcx), ref_cy=str(bcy), u=bu, v=bv, ref_len=int(rl), e_scale=int(E),
+                         bla_shape=list(tab.shape), dx=dx, dy=dy, ref_px=ref_px, ref_py=ref_py))
+    save("fexp_samples.npz", meta=json.dumps(meta), **out)
+
+
 def render3_cases():
     wl = json.load(open(os.path.join(HERE, "workloads.json")))
     cx3, cy3 = wl["config3_centre"]
@@ -416,7 +492,7 @@ def gen_truth():
 
 
 SECTIONS = {"truth": gen_truth, "fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
-            "render3": gen_render3}
+            "fexp": gen_fexp, "render3": gen_render3}
 
 if __name__ == "__main__":
     wanted = sys.argv[1:] or list(SECTIONS)

@@ -1,5 +1,6 @@
 """Shared helpers of the test-suite: golden fixtures and oracle frames."""
 import json
+import math
 import os
 from decimal import Decimal, localcontext
 
@@ -7,7 +8,7 @@ import numpy as np
 
 import oracle
 from fractura_b200 import abi
-from fractura_b200.config import decimal_context
+from fractura_b200.config import compute_floatexp_scale, decimal_context
 from fractura_b200.engine import plan_direct_view
 from fractura_b200.palette import synthetic_lut
 
@@ -80,21 +81,26 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
     pw = Decimal(m["width"])
     cxd, cyd = Decimal(m["cx"]), Decimal(m["cy"])
     ctx = decimal_context(pw)
+    floatexp = pw < Decimal("1e-300")
+    e_scale = compute_floatexp_scale(pw) if floatexp else 0
     with localcontext(ctx):
         ph = pw * (Decimal(H) / Decimal(W))
-        dx_f = float(pw / Decimal(max(1, W - 1)))
-        dy_f = float(ph / Decimal(max(1, H - 1)))
+        two_e = Decimal(2) ** e_scale
+        dx_f = float(pw * two_e / Decimal(max(1, W - 1)))
+        dy_f = float(ph * two_e / Decimal(max(1, H - 1)))
     hp.clear_reference_orbit_cache()
     bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
         cxd, cyd, pw, ph, mi, W, H, fractal_type=ft, julia_cx=m["julia_cx"], julia_cy=m["julia_cy"],
-        gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"])
+        gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"], is_floatexp=floatexp)
     order = m["bbsa_order"]
+    if floatexp and order in (4, 8):
+        order = 32  # the reference maps series starts to chained BLA on this tier
     use_bla = order == 32 and ft in (0, 2, 4) and not (cpu_sem and scheme == 11)
     tol = 1e-6
 
     def table(r_re, r_im, r_len, rpx, rpy):
         if bla_eps is not None:
-            dcm = max_delta_c(rpx, rpy, W * f, H * f, dx_f / f, dy_f / f)
+            dcm = math.ldexp(max_delta_c(rpx, rpy, W * f, H * f, dx_f / f, dy_f / f), -e_scale)
             return oracle.build_bla_dc(r_re, r_im, r_len, ft, bla_eps, dcm, 16, m["gen_n"], m["gen_kr"],
                                        m["gen_ki"])
         return oracle.build_bla(r_re, r_im, r_len, ft, tol, 16, m["gen_n"], m["gen_kr"], m["gen_ki"])
@@ -105,7 +111,8 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
                    float(H - 1) * float(bv) * float(f)) if use_bla else None
     strict = 1 if "Pauldelbrot" in m["glitch_mode"] or "Strict" in m["glitch_mode"] else 0
     p = abi.new_params(width=W, height=H, factor=f, max_iter=mi, fractal_type=ft,
-                       tier=abi.AP_TIER_PERTURB, arith=arith, gen_n=m["gen_n"], gen_kr=m["gen_kr"],
+                       tier=abi.AP_TIER_FLOATEXP if floatexp else abi.AP_TIER_PERTURB, arith=arith,
+                       e_scale=e_scale, gen_n=m["gen_n"], gen_kr=m["gen_kr"],
                        gen_ki=m["gen_ki"], scheme_id=scheme, num_bins=65536 if scheme == 11 else 2048,
                        dx_hi=dx_f / f, dy_hi=dy_f / f, ref_px=float(W - 1) * float(bu) * float(f),
                        ref_py=float(H - 1) * float(bv) * float(f), ref_cx=float(bcx), ref_cy=float(bcy),
