@@ -135,6 +135,28 @@ def _build_bla(L, d_re, d_im, ref_len, fractal_type, tol, gen_n, gen_kr, gen_ki,
     return table
 
 
+def bbsa_coefficients(L, re, im, ref_len, max_r, fractal_type, tol, order, gen_n, gen_kr, gen_ki,
+                      e_scale):
+    """(skip, a1_re, a1_im, ..., a8_re, a8_im) of the series start for one reference orbit
+    (ap_bbsa_coeffs, host code of the library; compute_bbsa_coeffs,
+    math_core/high_precision.py:537)."""
+    out = np.zeros(17, np.float64)
+    r = np.ascontiguousarray(re[:max(ref_len, 1) + 1], np.float64)
+    i = np.ascontiguousarray(im[:max(ref_len, 1) + 1], np.float64)
+    _lib.check(L.ap_bbsa_coeffs(r.ctypes.data_as(C.c_void_p), i.ctypes.data_as(C.c_void_p),
+                                int(ref_len), float(max_r), int(fractal_type), float(tol), int(order),
+                                int(gen_n), float(gen_kr), float(gen_ki), int(e_scale),
+                                out.ctypes.data_as(C.c_void_p)), "ap_bbsa_coeffs")
+    return out
+
+
+def _set_series(p, series, inv_r):
+    p.bbsa_skip = int(series[0])
+    p.bbsa_inv_r = float(inv_r)
+    for q in range(16):
+        p.bbsa[q] = float(series[1 + q])
+
+
 def max_delta_c(ref_px, ref_py, w_sub, h_sub, dx, dy):
     """Largest |dc| over a w_sub x h_sub sub-sample grid for a reference at
     sub-sample (ref_px, ref_py): the farthest corner, widened by 1e-6 so that
@@ -242,9 +264,12 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         center_x_dec, center_y_dec, plot_width_dec, plot_height_dec, max_iter, W, H,
         fractal_type=fractal_type, julia_cx=julia_cx, julia_cy=julia_cy, gen_n=gen_n,
         gen_kr=gen_kr, gen_ki=gen_ki, is_floatexp=floatexp)
-    if bbsa_order not in (0, 32) and fractal_type in (0, 2, 4) and bbsa_tol > 0:
-        raise NotImplementedError(
-            "series-approximation starts (bbsa_order 4/8) are not served yet; use 0 or 32")
+    # Series-approximation start (math_core/engine.py:1816-1840): radius 0.75 w, same
+    # inverse radius for every reference of the frame.
+    max_r = float(plot_width_dec) * 0.75
+    bbsa_inv_r = 1.0 / max_r if max_r > 0.0 else 1.0
+    series = bbsa_coefficients(L, re, im, ref_len, max_r, fractal_type, bbsa_tol, bbsa_order,
+                               gen_n, gen_kr, gen_ki, e_scale)
     d_re, d_im = _upload_orbit(torch, re, im, ref_len, slot, "ref")
     # The CPU reference's histogram path evaluates samples without BLA leaps
     # (math_core/engine.py:624-637, cpu_kernels.py:1887); every other path leaps.
@@ -268,6 +293,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     p.e_scale = int(e_scale)
     p.strict_glitch = strict
     p.bla_levels = BLA_LEVELS if use_bla else 0
+    _set_series(p, series, bbsa_inv_r)
     p.rebase_pass = 0
     # Sample variant: the CPU reference flags both; the CUDA unified kernels use the
     # BLA variant (NaN guard), their histogram resolve passes the plain one (escape glitch).
@@ -365,6 +391,8 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
         q.ref_len = int(r_len)
         q.bla_levels = BLA_LEVELS if bla is not None else 0
         q.rebase_pass = state.passes
+        _set_series(q, bbsa_coefficients(L, r_re, r_im, r_len, max_r, fractal_type, bbsa_tol,
+                                         bbsa_order, gen_n, gen_kr, gen_ki, e_scale), bbsa_inv_r)
         orbit = (d_re, d_im)
         if scheme == 11 and cdf is not None:
             q = _resolve_params(q, resolve_flags, cpu_sem)

@@ -206,6 +206,17 @@ AP_API int ap_build_bla_dc(const double* ref_re, const double* ref_im, int32_t r
                            int32_t fractal_type, double eps, double dc_max, int32_t levels,
                            int32_t gen_n, double gen_kr, double gen_ki, double* out, void* stream);
 
+/* Series-approximation ("BBSA") start for the perturbation tier, computed on the HOST
+ * from the host copy of the reference orbit (no device work).  Replaces
+ * compute_bbsa_coeffs / _jit_compute_bbsa_coeffs (math_core/high_precision.py:50-578,
+ * called from math_core/engine.py:426-470).  out[17]: out[0] = number of steps the
+ * start skips, out[1..16] = (a1_re, a1_im, ..., a8_re, a8_im) for ApFrameParams.bbsa;
+ * all zero where the reference returns no start (types other than 0, 2 and Multibrot
+ * n = 3, order 32, e_scale > 0, bad radius). */
+AP_API int ap_bbsa_coeffs(const double* ref_re, const double* ref_im, int32_t ref_len, double max_r,
+                          int32_t fractal_type, double tol, int32_t order, int32_t gen_n,
+                          double gen_kr, double gen_ki, int32_t e_scale, double* out);
+
 /* Measurement helper (no counterpart in the reference): number of kernels this
  * library has launched in the process so far. */
 AP_API uint64_t ap_launch_counter(void);

@@ -25,6 +25,7 @@ same inputs without the reference.  Sections:
 """
 import hashlib
 import json
+import math
 import os
 import sys
 import time
@@ -315,6 +316,84 @@ def gen_pert():
     save("pert_samples.npz", meta=json.dumps(meta), **out)
 
 
+def gen_bbsa():
+    """Series-approximation starts: compute_bbsa_coeffs (math_core/high_precision.py:537) on
+    the perturbation goldens' orbits, orders 4 and 8, and per-sample values that start from
+    them (cpu_compute_perturbation_sample, no BLA)."""
+    hp, ck, cfg = R.hp, R.ck, R.config
+    G = np.load(os.path.join(HERE, "pert_samples.npz"))
+    pmeta = json.loads(str(G["meta"]))
+    out = {}
+    meta = []
+    for m in pmeta:
+        name, ft = m["name"], m["fractal_type"]
+        if ft not in (0, 2, 4):
+            continue
+        re, im, rl = G[name + "__re"], G[name + "__im"], m["ref_len"]
+        max_r = float(Decimal(m["width"])) * 0.75
+        for order in (4, 8):
+            for tol in (1e-4, 1e-6):
+                tag = f"{name}__o{order}_t{int(-math.log10(tol))}"
+                res = hp.compute_bbsa_coeffs(re, im, rl, max_r, ft, bbsa_tol=tol, bbsa_order=order,
+                                             gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"],
+                                             E_scale=0)
+                coeffs = np.array(res, np.float64)
+                out[tag + "__coeffs"] = coeffs
+                meta.append(dict(name=name, tag=tag, order=order, tol=tol, max_r=max_r,
+                                 skip=int(res[0])))
+                if tol != 1e-4:
+                    continue
+                st = m["stride"] * 2
+                si = np.arange(0, m["W"], st, dtype=np.float64)
+                sj = np.arange(0, m["H"], st, dtype=np.float64)
+                sv = np.empty((len(sj), len(si)), np.float32)
+                for a, jj in enumerate(sj):
+                    for b, ii in enumerate(si):
+                        sv[a, b], _ = ck.cpu_compute_perturbation_sample(
+                            re, im, rl, m["max_iter"], m["ref_px"], m["ref_py"], float(ii), float(jj),
+                            m["dx"], m["dy"], float(Decimal(m["ref_cx"])), float(Decimal(m["ref_cy"])), ft,
+                            float(m["julia_cx"]), float(m["julia_cy"]), int(res[0]), 1.0 / max_r,
+                            *res[1:17], m["gen_n"], m["gen_kr"], m["gen_ki"], 0, INV_LN2, LN_BAIL,
+                            bla_table=np.zeros((1, 1, 1)))
+                out[tag + "__s"] = sv
+                out[tag + "__stride"] = np.array([st])
+                print(f"  {tag}: skip {int(res[0])} escaped {np.mean(sv >= 0):.3f}")
+    save("bbsa_samples.npz", meta=json.dumps(meta), **out)
+
+
+def gen_render_bbsa():
+    """Frames with series-approximation starts (bbsa_order 4 and 8, tol 1e-4) through
+    render_frame_cpu, Pauldelbrot rebasing on."""
+    G = np.load(os.path.join(HERE, "pert_samples.npz"))
+    pm = {m["name"]: m for m in json.loads(str(G["meta"]))}
+    out = {}
+    meta = []
+    for (name, src, order, W, H, gm) in (("bbsa4_cfg3", "cfg3", 4, 160, 90, "Pauldelbrot"),
+                                         ("bbsa8_cfg3", "cfg3", 8, 160, 90, "Off (Single-Ref)"),
+                                         ("bbsa4_julia", "julia", 4, 160, 90, "Pauldelbrot"),
+                                         ("bbsa8_multibrot3", "multibrot3", 8, 160, 90, "Off (Single-Ref)")):
+        m = pm[src]
+        mi = min(m["max_iter"], 20000)
+        R.hp.clear_reference_orbit_cache()
+        it = np.zeros((H, W), np.float32)
+        t0 = time.time()
+        rgb = R.engine.render_frame_cpu(
+            W, H, mi, Decimal(m["cx"]), Decimal(m["cy"]), Decimal(m["width"]), "synthetic",
+            ssaa_factor=1, edge_threshold=0.35, color_scheme_id=0,
+            precision_mode="1e-300 (Perturbation)", fractal_type=m["fractal_type"],
+            julia_cx=m["julia_cx"], julia_cy=m["julia_cy"], bbsa_tol=1e-4, bbsa_order=order,
+            glitch_mode=gm, gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"], cpu_threads=8,
+            palette_offset=0.0, color_density=1.0, color_contrast=1.0, h_iter_buf=it)
+        print(f"  {name}: {time.time() - t0:.2f}s escaped {np.mean(it >= 0):.3f}")
+        out[name + "__rgb"] = rgb
+        out[name + "__iter"] = it
+        meta.append(dict(name=name, W=W, H=H, max_iter=mi, cx=m["cx"], cy=m["cy"], width=m["width"],
+                         scheme=0, factor=1, bbsa_order=order, bbsa_tol=1e-4, glitch_mode=gm,
+                         fractal_type=m["fractal_type"], julia_cx=m["julia_cx"], julia_cy=m["julia_cy"],
+                         gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"]))
+    save("render_bbsa.npz", meta=json.dumps(meta), **out)
+
+
 FEXP_SPECS = [
     # name, fractal_type, width, W, H, max_iter, stride, jx, jy, n, kr, ki  (centre: the pert case's)
     ("fexp_mandel", 0, "1e-320", 480, 270, 20000, 10, 0.0, 0.0, 3, 0.25, 1.0),
@@ -492,7 +571,8 @@ def gen_truth():
 
 
 SECTIONS = {"truth": gen_truth, "fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
-            "fexp": gen_fexp, "render3": gen_render3}
+            "fexp": gen_fexp, "bbsa": gen_bbsa, "render_bbsa": gen_render_bbsa,
+            "render3": gen_render3}
 
 if __name__ == "__main__":
     wanted = sys.argv[1:] or list(SECTIONS)

@@ -95,6 +95,22 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
     order = m["bbsa_order"]
     if floatexp and order in (4, 8):
         order = 32  # the reference maps series starts to chained BLA on this tier
+    # Series-start coefficients come from the library's host function, which
+    # tests/test_bbsa.py pins against the reference's compute_bbsa_coeffs.
+    from fractura_b200 import _lib
+    from fractura_b200.perturbation import bbsa_coefficients
+    max_r = float(pw) * 0.75
+    inv_r = 1.0 / max_r if max_r > 0.0 else 1.0
+    bbsa_tol = m.get("bbsa_tol", 1e-4)
+
+    def series(r_re, r_im, r_len):
+        return bbsa_coefficients(_lib.load(), r_re, r_im, r_len, max_r, ft, bbsa_tol, order,
+                                 m["gen_n"], m["gen_kr"], m["gen_ki"], e_scale)
+
+    def set_series(q, c):
+        q.bbsa_skip, q.bbsa_inv_r = int(c[0]), inv_r
+        for t in range(16):
+            q.bbsa[t] = float(c[1 + t])
     use_bla = order == 32 and ft in (0, 2, 4) and not (cpu_sem and scheme == 11)
     tol = 1e-6
 
@@ -120,6 +136,7 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
                        ref_len=int(rl), bla_levels=16 if use_bla else 0, strict_glitch=strict,
                        palette_offset=m.get("offset", 0.0), color_density=m.get("density", 1.0),
                        color_contrast=m.get("contrast", 1.0))
+    set_series(p, series(re, im, rl))
     uf = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_NAN_GUARD
     rf = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_ESCAPE_GLITCH
 
@@ -179,6 +196,7 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
         q.ref_len = int(r_len)
         q.bla_levels = 16 if use_bla else 0
         q.rebase_pass = state.passes
+        set_series(q, series(r_re, r_im, r_len))
         if scheme == 11:
             resolve(q)
         elif f == 1:

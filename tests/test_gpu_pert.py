@@ -110,3 +110,27 @@ def test_packed_orbit_and_bla_layouts():
     assert np.array_equal(AB, np.transpose(T[:, :, :4], (1, 0, 2)))
     # radii never increase with the level (the level search relies on it)
     assert np.all(np.diff(R, axis=1) <= 0)
+
+
+BS, BSMETA = load_golden("render_bbsa.npz")
+
+
+@pytest.mark.parametrize("name", [m["name"] for m in BSMETA])
+@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda"])
+def test_series_started_frame_matches_oracle(name, arith):
+    """bbsa_order 4/8 frames through the engine equal the oracle's, value for value."""
+    m = next(x for x in BSMETA if x["name"] == name)
+    W, H = m["W"], m["H"]
+    hp.clear_reference_orbit_cache()
+    it = np.zeros((H, W), np.float32)
+    rgb = engine.render_frame_ssaa(
+        W, H, m["max_iter"], Decimal(m["cx"]), Decimal(m["cy"]), Decimal(m["width"]), None,
+        color_scheme_id=0, precision_mode="1e-300 (Perturbation)", fractal_type=m["fractal_type"],
+        julia_cx=m["julia_cx"], julia_cy=m["julia_cy"], bbsa_tol=m["bbsa_tol"],
+        bbsa_order=m["bbsa_order"], glitch_mode=m["glitch_mode"], gen_n=m["gen_n"],
+        gen_kr=m["gen_kr"], gen_ki=m["gen_ki"], h_iter_buf=it, arith=arith)
+    fr, _ = oracle_pert_frame(m, arith=0 if arith == "ref_cpu" else 1)
+    assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32)), \
+        int((it.view(np.uint32) != fr.iter_map.view(np.uint32)).sum())
+    n_bad, max_diff = rgb_mismatch(rgb, fr.rgb)
+    assert n_bad == 0, (n_bad, max_diff)
