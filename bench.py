@@ -91,8 +91,8 @@ DEFAULT_WORKLOAD = "cfg3"
 
 # ------------------------------------------------------------------ helpers
 def dist_env():
-    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
-            int(os.environ.get("LOCAL_RANK", "0")))
+    from fractura_b200 import dist
+    return dist.env()
 
 
 class ClockSampler:
@@ -205,19 +205,13 @@ def config_of(wl, n_gpus):
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from fractura_b200 import dist
+    dist.barrier()
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from fractura_b200 import dist
+    return dist.max_over_ranks(x)
 
 
 # ----------------------------------------------------------- CPU baseline
@@ -432,7 +426,8 @@ def our_arm(args, wl, rank, world, local_rank):
     launches = L.ap_launch_counter() - c0
     barrier(world)
     total_ms = max_over_ranks(float(np.sum(step_ms)), world)
-    value = chosen.iters * args.steps * world / (total_ms * 1e-3) / 1e9
+    from fractura_b200 import dist
+    value = dist.whole_job_rate(chosen.iters, args.steps, world, total_ms) / 1e9
 
     # End to end through render_frame_ssaa with a pinned host RGB buffer.
     e2e_steps = max(3, args.steps // 10)
