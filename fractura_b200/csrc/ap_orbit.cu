@@ -1,0 +1,325 @@
+// ap_orbit.cu -- reference orbits in binary fixed point, on the host.
+//
+// The perturbation tiers need the orbit Z_0, Z_1, ... of one point at the
+// precision of the view (math_core/high_precision.py:706-875 iterates it in
+// Decimal with int(bits / 3.32) + 30 digits).  Here every number is a signed
+// fixed-point value X / 2^F held in L little-endian 64-bit limbs (two's
+// complement, F = 64 (L - I): the top I limbs are the signed integer part, wide
+// enough for |Z|^2 of the first escaped Z, at most (256^n + ...)^2 for z^n).
+// The caller runs two precisions that bracket the Decimal one; where both give
+// the same float64 orbit, so does the Decimal iteration.
+//
+// Products are truncated: partial products more than two limbs below the unit
+// of the last kept limb are skipped (their total is below 2^-F).  Each stored
+// orbit value is rounded to float64 correctly (round half to even), as
+// float(Decimal) rounds.  The loop is serial; callers run candidates of the
+// 16-point probe in parallel threads.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "ap_common.cuh"
+
+namespace {
+
+using u64 = uint64_t;
+using u128 = unsigned __int128;
+
+constexpr int kMaxLimbs = 160;  // 10176 fractional bits: views down to ~1e-3000
+
+struct Fx {  // sign-magnitude working form
+    int neg;
+    u64 m[kMaxLimbs];
+};
+
+inline bool is_zero(const u64* a, int L) {
+    for (int i = 0; i < L; ++i)
+        if (a[i]) return false;
+    return true;
+}
+
+inline int cmp_mag(const u64* a, const u64* b, int L) {
+    for (int i = L - 1; i >= 0; --i) {
+        if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+    }
+    return 0;
+}
+
+inline void add_mag(u64* r, const u64* a, const u64* b, int L) {  // r = a + b
+    u64 carry = 0;
+    for (int i = 0; i < L; ++i) {
+        const u128 s = (u128)a[i] + b[i] + carry;
+        r[i] = (u64)s;
+        carry = (u64)(s >> 64);
+    }
+}
+
+inline void sub_mag(u64* r, const u64* a, const u64* b, int L) {  // r = a - b, a >= b
+    u64 borrow = 0;
+    for (int i = 0; i < L; ++i) {
+        const u128 d = (u128)a[i] - b[i] - borrow;
+        r[i] = (u64)d;
+        borrow = (u64)((d >> 64) & 1);
+    }
+}
+
+// r = (-1)^an |a| + (-1)^bn |b| on sign-magnitude values (r may alias a or b).
+inline void add_s(Fx& r, const Fx& a, int an, const Fx& b, int bn, int L) {
+    if (an == bn) {
+        add_mag(r.m, a.m, b.m, L);
+        r.neg = an && !is_zero(r.m, L);
+        return;
+    }
+    const int c = cmp_mag(a.m, b.m, L);
+    if (c >= 0) {
+        sub_mag(r.m, a.m, b.m, L);
+        r.neg = c == 0 ? 0 : an;
+    } else {
+        sub_mag(r.m, b.m, a.m, L);
+        r.neg = bn;
+    }
+}
+
+inline void add(Fx& r, const Fx& a, const Fx& b, int L) { add_s(r, a, a.neg, b, b.neg, L); }
+inline void sub(Fx& r, const Fx& a, const Fx& b, int L) { add_s(r, a, a.neg, b, !b.neg, L); }
+
+// r = a * b (fixed point, truncated).  Product limb k (of 2L) has weight
+// 2^(64 k - 2F); the result keeps limbs [L - I, 2L - I).  Partial products with
+// index i + j < L - I - 2 are not formed: together they are worth less than one
+// unit of the last kept limb.
+inline void mul(Fx& r, const Fx& a, const Fx& b, int L, int I) {
+    u64 acc[2 * kMaxLimbs + 2];
+    std::memset(acc, 0, sizeof(u64) * (2 * L + 2));
+    const int lo = L - I - 2 > 0 ? L - I - 2 : 0;
+    for (int i = 0; i < L; ++i) {
+        const u64 ai = a.m[i];
+        if (!ai) continue;
+        const int j0 = lo - i > 0 ? lo - i : 0;
+        u64 carry = 0;
+        int j = j0;
+        for (; j < L; ++j) {
+            const u128 p = (u128)ai * b.m[j] + acc[i + j] + carry;
+            acc[i + j] = (u64)p;
+            carry = (u64)(p >> 64);
+        }
+        int k = i + j;
+        while (carry) {
+            const u128 s = (u128)acc[k] + carry;
+            acc[k] = (u64)s;
+            carry = (u64)(s >> 64);
+            ++k;
+        }
+    }
+    std::memcpy(r.m, acc + (L - I), sizeof(u64) * L);
+    r.neg = (a.neg ^ b.neg) && !is_zero(r.m, L);
+}
+
+inline void twice(Fx& r, const Fx& a, int L) {
+    u64 carry = 0;
+    for (int i = 0; i < L; ++i) {
+        const u64 v = a.m[i];
+        r.m[i] = (v << 1) | carry;
+        carry = v >> 63;
+    }
+    r.neg = a.neg;
+}
+
+// Correctly rounded float64 (round half to even) of a sign-magnitude value.
+double to_double(const Fx& a, int L, int I) {
+    int top = L - 1;
+    while (top >= 0 && a.m[top] == 0) --top;
+    if (top < 0) return a.neg ? -0.0 : 0.0;
+    const int lz = __builtin_clzll(a.m[top]);
+    const int p = 64 * top + (63 - lz);  // index of the leading one bit
+    // 64-bit window with the leading bit at its top, then a sticky bit below it.
+    auto bit_window = [&](int hi_bit) -> u64 {  // bits [hi_bit - 63, hi_bit]
+        const int lo_bit = hi_bit - 63;
+        u64 w = 0;
+        if (lo_bit >= 0) {
+            const int li = lo_bit >> 6, sh = lo_bit & 63;
+            w = a.m[li] >> sh;
+            if (sh && li + 1 < L) w |= a.m[li + 1] << (64 - sh);
+        } else {
+            w = a.m[0] << (-lo_bit);
+        }
+        return w;
+    };
+    const u64 win = bit_window(p);
+    bool sticky = false;
+    const int lo_bit = p - 63;
+    if (lo_bit > 0) {
+        const int li = lo_bit >> 6, sh = lo_bit & 63;
+        for (int i = 0; i < li && !sticky; ++i) sticky = a.m[i] != 0;
+        if (!sticky && sh) sticky = (a.m[li] & ((1ULL << sh) - 1)) != 0;
+    }
+    u64 mant = win >> 11;
+    const u64 rest = win & 0x7FF;
+    int e2 = p;
+    if (rest > 0x400 || (rest == 0x400 && (sticky || (mant & 1)))) {
+        ++mant;
+        if (mant == (1ULL << 53)) {
+            mant >>= 1;
+            ++e2;
+        }
+    }
+    const int F = 64 * (L - I);
+    const double v = std::ldexp((double)mant, e2 - 52 - F);
+    return a.neg ? -v : v;
+}
+
+void load(Fx& r, const u64* twos, int L) {  // two's complement limbs -> sign-magnitude
+    const int neg = (twos[L - 1] >> 63) & 1;
+    if (!neg) {
+        std::memcpy(r.m, twos, sizeof(u64) * L);
+        r.neg = 0;
+        return;
+    }
+    u64 carry = 1;
+    for (int i = 0; i < L; ++i) {
+        const u128 s = (u128)(~twos[i]) + carry;
+        r.m[i] = (u64)s;
+        carry = (u64)(s >> 64);
+    }
+    r.neg = !is_zero(r.m, L);
+}
+
+inline bool equal(const Fx& a, const Fx& b, int L) {
+    return a.neg == b.neg && cmp_mag(a.m, b.m, L) == 0;
+}
+
+}  // namespace
+
+extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_limbs,
+                                  int32_t fractal_type,
+                                  int32_t gen_n, int32_t max_iter, int32_t escape_only,
+                                  double* ref_re, double* ref_im, int32_t* ref_len,
+                                  double* escape_mag2, uint64_t* trace_hash) {
+    if (!seeds || !ref_len || max_iter < 0 || fractal_type < 0 || fractal_type > 4 ||
+        (fractal_type == 4 && (gen_n < 1 || gen_n > 64)) || (!escape_only && (!ref_re || !ref_im))) {
+        ap::set_error("ap_reference_orbit: bad arguments");
+        return AP_E_INVALID;
+    }
+    // integer bits needed: |Z|^2 of the first escaped Z (|Z_prev| <= 256) plus sign
+    const int n = fractal_type == 4 ? (gen_n > 2 ? gen_n : 2) : 2;
+    const int need = (16 * n + 8 + 1 + 63) / 64;
+    if (int_limbs < need || limbs <= int_limbs || limbs > kMaxLimbs) {
+        ap::set_error("ap_reference_orbit: %d limbs with %d integer limbs (need >= %d integer limbs, "
+                      "at most %d limbs)", limbs, int_limbs, need, kMaxLimbs);
+        return AP_E_INVALID;
+    }
+    const int L = limbs, I = int_limbs;
+    // seeds: z0_re, z0_im, c_re, c_im, k_re, k_im, each L limbs
+    std::vector<Fx> v(16);
+    Fx &zx = v[0], &zy = v[1], &cx = v[2], &cy = v[3], &kr = v[4], &ki = v[5];
+    Fx &zx2 = v[6], &zy2 = v[7], &t0 = v[8], &t1 = v[9], &t2 = v[10], &t3 = v[11];
+    Fx &sx = v[12], &sy = v[13], &bail = v[14], &mag = v[15];
+    load(zx, seeds, L);
+    load(zy, seeds + L, L);
+    load(cx, seeds + 2 * L, L);
+    load(cy, seeds + 3 * L, L);
+    load(kr, seeds + 4 * L, L);
+    load(ki, seeds + 5 * L, L);
+    std::memset(bail.m, 0, sizeof(u64) * L);
+    bail.m[L - I] = 65536;
+    bail.neg = 0;
+
+    const bool periodic = (fractal_type == 0 || fractal_type == 2) && !escape_only;
+    int check_step = 8, saved_k = 0;
+    sx = zx;
+    sy = zy;
+    int len = max_iter;
+    // FNV-1a over the float64 bits of every Z_k: lets two runs at different
+    // precisions confirm they followed the same float64 trajectory.
+    u64 hash = 1469598103934665603ULL;
+    auto mix = [&](double d) {
+        u64 b;
+        std::memcpy(&b, &d, 8);
+        for (int q = 0; q < 8; ++q) {
+            hash ^= (b >> (8 * q)) & 0xff;
+            hash *= 1099511628211ULL;
+        }
+    };
+    for (int k = 0; k < max_iter; ++k) {
+        if (!escape_only || trace_hash) {
+            const double re = to_double(zx, L, I), im = to_double(zy, L, I);
+            if (!escape_only) {
+                ref_re[k] = re;
+                ref_im[k] = im;
+            }
+            if (trace_hash) {
+                mix(re);
+                mix(im);
+            }
+        }
+        mul(zx2, zx, zx, L, I);
+        mul(zy2, zy, zy, L, I);
+        add(mag, zx2, zy2, L);
+        if (!mag.neg && cmp_mag(mag.m, bail.m, L) > 0) {
+            len = k;
+            if (escape_only && escape_mag2) *escape_mag2 = to_double(mag, L, I);
+            break;
+        }
+        if (periodic) {
+            if (k == check_step) {
+                check_step <<= 1;
+                saved_k = k;
+                sx = zx;
+                sy = zy;
+            } else if (k > saved_k && equal(zx, sx, L) && equal(zy, sy, L)) {
+                const int period = k - saved_k;
+                for (int j = k; j <= max_iter; ++j) {
+                    ref_re[j] = ref_re[j - period];
+                    ref_im[j] = ref_im[j - period];
+                }
+                *ref_len = max_iter;
+                if (trace_hash) *trace_hash = hash;
+                return AP_OK;
+            }
+        }
+        if (fractal_type == 0 || fractal_type == 2) {  // z^2 + c
+            mul(t0, zx, zy, L, I);
+            sub(t1, zx2, zy2, L);
+            add(zx, t1, cx, L);
+            twice(t0, t0, L);
+            add(zy, t0, cy, L);
+        } else if (fractal_type == 1 || fractal_type == 3) {  // Burning Ship: 2|x||y| - c_y
+            mul(t0, zx, zy, L, I);
+            t0.neg = 0;  // |x| |y|
+            sub(t1, zx2, zy2, L);
+            add(zx, t1, cx, L);
+            twice(t0, t0, L);
+            sub(zy, t0, cy, L);
+        } else {  // Multibrot z^n + K z + c
+            Fx& nr = v[12];  // the checkpoint slots are free: no period detection here
+            Fx& ni = v[13];
+            nr = zx;
+            ni = zy;
+            for (int t = 0; t < gen_n - 1; ++t) {
+                mul(t0, nr, zx, L, I);
+                mul(t1, ni, zy, L, I);
+                mul(t2, nr, zy, L, I);
+                mul(t3, ni, zx, L, I);
+                sub(nr, t0, t1, L);
+                add(ni, t2, t3, L);
+            }
+            mul(t0, kr, zx, L, I);
+            mul(t1, ki, zy, L, I);
+            mul(t2, kr, zy, L, I);
+            mul(t3, ki, zx, L, I);
+            sub(t0, t0, t1, L);  // Re(K z)
+            add(t2, t2, t3, L);  // Im(K z)
+            add(t0, nr, t0, L);
+            add(zx, t0, cx, L);
+            add(t2, ni, t2, L);
+            add(zy, t2, cy, L);
+        }
+    }
+    if (!escape_only) {
+        ref_re[len] = to_double(zx, L, I);
+        ref_im[len] = to_double(zy, L, I);
+    }
+    *ref_len = len;
+    if (trace_hash) *trace_hash = hash;
+    return AP_OK;
+}

@@ -1,16 +1,18 @@
 """Host-side high-precision inputs of the perturbation tiers.
 
-Restates math_core/high_precision.py's reference-orbit machinery with the
-reference's Decimal arithmetic (its path when gmpy2 is absent,
-math_core/high_precision.py:657-703 and :802-873), so the orbit arrays are
-bit-identical to the reference's:
+Restates math_core/high_precision.py's reference-orbit machinery.  The
+reference iterates orbits in Decimal (its path when gmpy2 is absent,
+math_core/high_precision.py:657-703 and :802-873); here the orbit loop runs in
+native binary fixed point with more bits than those Decimal digits
+(ap_reference_orbit, host code of the library), and the orbit arrays equal the
+reference's:
 
   compute_single_highprec_orbit   math_core/high_precision.py:706-875
   compute_highprec_escape_scalar  math_core/high_precision.py:581-703
   find_optimal_reference_orbit    math_core/high_precision.py:919-1097
   cache_reference_orbit / clear_reference_orbit_cache (16-entry LRU)
 
-Every computation runs in a local Decimal context; the caller's context is
+Every Decimal computation runs in a local context; the caller's context is
 never modified.
 """
 import math
@@ -28,6 +30,151 @@ _ORBIT_LOCK = threading.Lock()
 _CACHE_SIZE = 16
 
 
+def _orbit_digits(prec_bits):
+    """Decimal digits the reference's orbit uses (math_core/high_precision.py:720)."""
+    return int(prec_bits / 3.32) + 30
+
+
+def orbit_int_limbs(fractal_type, gen_n):
+    """Integer limbs of the fixed-point orbit: room for |Z|^2 of the first escaped Z
+    (|Z| <= 256 the step before, so at most about 2^(16 n) for z^n), plus the sign."""
+    n = max(int(gen_n), 2) if fractal_type == 4 else 2
+    return (16 * n + 8 + 1 + 63) // 64
+
+
+def orbit_limbs(prec_bits, int_limbs=1):
+    """(low, high) limb counts of the two fixed-point orbits: 64 fractional bits fewer
+    and at least 64 more than the reference's Decimal precision, plus int_limbs."""
+    dec_bits = _orbit_digits(prec_bits) * 3.3219280948873626
+    lo = max(1, int(math.floor((dec_bits - 64.0) / 64.0)))
+    hi = int(math.ceil((dec_bits + 64.0) / 64.0))
+    return lo + int_limbs, hi + int_limbs
+
+
+def to_fixed(value, limbs, int_limbs=1):
+    """A Decimal (or a number's str) as two's-complement fixed point,
+    value * 2^(64 (limbs - int_limbs)) rounded half to even, in little-endian uint64 limbs."""
+    d = value if isinstance(value, Decimal) else Decimal(str(value))
+    sign, digits, exp = d.as_tuple()
+    n = int("".join(map(str, digits))) if digits else 0
+    shift = 64 * (limbs - int_limbs)
+    if exp >= 0:
+        q = (n * 10 ** exp) << shift
+    else:
+        den = 10 ** (-exp)
+        q, r = divmod(n << shift, den)
+        if 2 * r > den or (2 * r == den and q & 1):
+            q += 1
+    if sign:
+        q = -q
+    if not -(1 << (64 * limbs - 1)) <= q < (1 << (64 * limbs - 1)):
+        raise OverflowError("value outside the fixed-point range")
+    return np.frombuffer((q % (1 << (64 * limbs))).to_bytes(8 * limbs, "little"), dtype=np.uint64)
+
+
+def _seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki, limbs, int_limbs=1):
+    """(z0, c, K) of the orbit, as the reference starts it (math_core/high_precision.py:722-735)."""
+    if fractal_type in (2, 3):
+        z0x, z0y, c_x, c_y = Decimal(cand_cx), Decimal(cand_cy), Decimal(str(julia_cx)), Decimal(str(julia_cy))
+    else:
+        z0x, z0y, c_x, c_y = Decimal(0), Decimal(0), Decimal(cand_cx), Decimal(cand_cy)
+    vals = (z0x, z0y, c_x, c_y, Decimal(str(gen_kr)), Decimal(str(gen_ki)))
+    return np.ascontiguousarray(np.concatenate([to_fixed(v, limbs, int_limbs) for v in vals]))
+
+
+def _native():
+    from . import _lib
+    return _lib.load()
+
+
+def _native_orbit(seeds_fn, L, max_iter, fractal_type, gen_n):
+    import ctypes as C
+    from . import _lib
+    I = orbit_int_limbs(fractal_type, gen_n)
+    seeds = seeds_fn(L, I)
+    ref_re = np.zeros(max_iter + 1, dtype=np.float64)
+    ref_im = np.zeros(max_iter + 1, dtype=np.float64)
+    ref_len = C.c_int32(0)
+    _lib.check(_native().ap_reference_orbit(
+        seeds.ctypes.data_as(C.c_void_p), L, I, int(fractal_type), int(gen_n), int(max_iter), 0,
+        ref_re.ctypes.data_as(C.c_void_p), ref_im.ctypes.data_as(C.c_void_p), C.byref(ref_len),
+        None, None), "ap_reference_orbit")
+    return ref_re, ref_im, int(ref_len.value)
+
+
+def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
+                                  julia_cx=0.0, julia_cy=0.0, prec_bits=256,
+                                  gen_n=3, gen_kr=0.25, gen_ki=1.0):
+    """Reference orbit Z_0..Z_ref_len as float64 arrays of length max_iter + 1.
+
+    ref_len is the step at which |Z|^2 > 65536 (max_iter if it never does).  For
+    Mandelbrot and its Julia set an exactly repeating orbit is detected at
+    power-of-two checkpoints and its cycle is copied to the end of the arrays
+    (math_core/high_precision.py:706-875).
+
+    The orbit runs natively (ap_reference_orbit) in binary fixed point twice, with
+    64 fractional bits fewer and 64 more than the reference's Decimal digits
+    carry.  When both give the same float64 orbit, the Decimal orbit, whose
+    precision lies between them, gives it too, and that orbit is returned.  When
+    they differ, the orbit has run through the available precision (a bounded
+    chaotic orbit): it is then iterated in Decimal exactly as the reference does.
+    """
+    lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+
+    def seeds(L, I):
+        return _seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki, L, I)
+
+    a = _native_orbit(seeds, hi, max_iter, fractal_type, gen_n)
+    b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
+    if a[2] == b[2] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]):
+        return a
+    return decimal_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,
+                         prec_bits, gen_n, gen_kr, gen_ki)
+
+
+def _native_escape(seeds_fn, L, max_iter, fractal_type, gen_n):
+    import ctypes as C
+    from . import _lib
+    I = orbit_int_limbs(fractal_type, gen_n)
+    seeds = seeds_fn(L, I)
+    k = C.c_int32(0)
+    mag2 = C.c_double(0.0)
+    trace = C.c_uint64(0)
+    _lib.check(_native().ap_reference_orbit(
+        seeds.ctypes.data_as(C.c_void_p), L, I, int(fractal_type), int(gen_n), int(max_iter), 1,
+        None, None, C.byref(k), C.byref(mag2), C.byref(trace)), "ap_reference_orbit")
+    return int(k.value), float(mag2.value), int(trace.value)
+
+
+def compute_highprec_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
+                                   julia_cx=0.0, julia_cy=0.0, prec_bits=256,
+                                   gen_n=3, gen_kr=0.25, gen_ki=1.0):
+    """Smooth escape value of one point (max_iter if it stays bounded), as
+    math_core/high_precision.py:581-703 computes it.  The orbit runs natively at
+    two precisions bracketing the reference's (see compute_single_highprec_orbit);
+    if they disagree on the float64 trajectory, the escape step or |Z|^2 there, it
+    runs in Decimal."""
+    lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+
+    def seeds(L, I):
+        return _seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki, L, I)
+
+    a = _native_escape(seeds, hi, max_iter, fractal_type, gen_n)
+    if a != _native_escape(seeds, lo, max_iter, fractal_type, gen_n):
+        return decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy,
+                                     prec_bits, gen_n, gen_kr, gen_ki)
+    k, mag2, _ = a
+    if k >= max_iter:
+        return float(max_iter)
+    inv_n = (1.0 / math.log(float(gen_n))) if (fractal_type == 4 and gen_n > 1) else float(INV_LN2_F32)
+    log_mag = math.log(mag2)
+    if log_mag > 1.0:
+        return float(k + 1.0) - (math.log(0.5 * log_mag) - LN_BAILOUT_LOG) * inv_n
+    return float(k)
+
+
+# Exact Decimal iteration in the reference's operation order: the path for orbits the
+# fixed-point runs cannot certify.
 def _orbit_context(prec_bits):
     ctx = decimal_context()
     ctx.prec = int(prec_bits / 3.32) + 30
@@ -54,7 +201,7 @@ def _step(fractal_type, zx, zy, zx2, zy2, c_x, c_y, two, n, kr, ki):
     return zn_r + kz_r + c_x, zn_i + kz_i + c_y
 
 
-def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
+def decimal_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
                                   julia_cx=0.0, julia_cy=0.0, prec_bits=256,
                                   gen_n=3, gen_kr=0.25, gen_ki=1.0):
     """Reference orbit Z_0..Z_ref_len as float64 arrays of length max_iter + 1.
@@ -98,7 +245,7 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     return ref_re, ref_im, ref_len
 
 
-def compute_highprec_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
+def decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
                                    julia_cx=0.0, julia_cy=0.0, prec_bits=256,
                                    gen_n=3, gen_kr=0.25, gen_ki=1.0):
     """Smooth escape value of one point in Decimal arithmetic (max_iter if it stays bounded)."""

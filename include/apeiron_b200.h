@@ -217,6 +217,25 @@ AP_API int ap_bbsa_coeffs(const double* ref_re, const double* ref_im, int32_t re
                           int32_t fractal_type, double tol, int32_t order, int32_t gen_n,
                           double gen_kr, double gen_ki, int32_t e_scale, double* out);
 
+/* Reference orbit of one point on the HOST, in binary fixed point.  Replaces the
+ * Decimal orbit loop of compute_single_highprec_orbit (math_core/high_precision.py:706-875)
+ * and, with escape_only, of compute_highprec_escape_scalar (:581-703).
+ * seeds: 6 numbers (z0_re, z0_im, c_re, c_im, K_re, K_im), each `limbs` little-endian
+ * uint64 limbs of two's-complement fixed point value * 2^(64 (limbs - int_limbs));
+ * limbs <= 160; int_limbs >= ceil((16 n + 9) / 64) (n = 2 except Multibrot), so that
+ * |Z|^2 of the first escaped Z is representable.
+ * escape_only = 0: ref_re/ref_im (max_iter + 1 float64 each) receive the orbit rounded
+ * to nearest, *ref_len the step at which |Z|^2 > 65536 (max_iter if none; an exactly
+ * repeating Mandelbrot/Julia orbit found at power-of-two checkpoints is copied to the
+ * end).  escape_only = 1: no arrays; *ref_len = escape step, *escape_mag2 = |Z|^2 there.
+ * trace_hash (optional): a hash of the float64 values of every Z_k up to the escape, so
+ * that runs at two precisions can confirm they followed the same float64 trajectory. */
+AP_API int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_limbs,
+                              int32_t fractal_type,
+                              int32_t gen_n, int32_t max_iter, int32_t escape_only,
+                              double* ref_re, double* ref_im, int32_t* ref_len,
+                              double* escape_mag2, uint64_t* trace_hash);
+
 /* Measurement helper (no counterpart in the reference): number of kernels this
  * library has launched in the process so far. */
 AP_API uint64_t ap_launch_counter(void);

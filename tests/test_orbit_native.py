@@ -1,0 +1,97 @@
+"""Reference orbits computed natively (ap_reference_orbit at two fixed-point
+precisions bracketing the reference's Decimal precision, Decimal only when those
+disagree) against the Decimal loop in the reference's operation order.
+
+The reference's own orbits pin the result (tests/test_oracle_pert.py and
+tests/test_oracle_fexp.py compare find_optimal_reference_orbit with them).  Here:
+seeded points of every formula at two precisions give float64 orbits, escape
+steps and escape values equal to the Decimal loop's, including bounded chaotic
+orbits that run through the available precision; interior points whose orbits
+become exactly periodic reach the same cycle and the same ref_len.
+"""
+from decimal import Decimal, localcontext
+
+import numpy as np
+import pytest
+
+from fractura_b200 import high_precision as hp
+
+FORMULAS = [  # fractal_type, julia, gen_n, kr, ki
+    (0, (0.0, 0.0), 3, 0.25, 1.0),
+    (1, (0.0, 0.0), 3, 0.25, 1.0),
+    (2, (-0.8, 0.156), 3, 0.25, 1.0),
+    (3, (-1.755, 0.03), 3, 0.25, 1.0),
+    (4, (0.0, 0.0), 3, 0.1, 0.2),
+    (4, (0.0, 0.0), 5, 0.1, 0.2),
+]
+
+
+def _points(seed, n, ft):
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        if ft in (2, 3):
+            x, y = rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0)
+        else:
+            x, y = rng.uniform(-2.0, 0.6), rng.uniform(-1.2, 1.2)
+        digits = int(rng.integers(20, 120))
+        out.append((Decimal(repr(x)) + Decimal(int(rng.integers(1, 10 ** 9))).scaleb(-digits),
+                    Decimal(repr(y)) - Decimal(int(rng.integers(1, 10 ** 9))).scaleb(-digits)))
+    return out
+
+
+@pytest.mark.parametrize("prec_bits", [256, 700])
+@pytest.mark.parametrize("formula", FORMULAS, ids=lambda f: f"type{f[0]}_n{f[2]}")
+def test_orbits_equal_decimal(formula, prec_bits):
+    ft, (jx, jy), n, kr, ki = formula
+    for cx, cy in _points(prec_bits + 31 * ft + n, 6, ft):
+        a = hp.compute_single_highprec_orbit(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
+        b = hp.decimal_orbit(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
+        assert a[2] == b[2]
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+        ea = hp.compute_highprec_escape_scalar(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
+        eb = hp.decimal_escape_scalar(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
+        assert ea == eb
+
+
+@pytest.mark.parametrize("c", [("0", "0"), ("-1", "0"), ("0", "1"), ("-0.1", "0.1"),
+                               ("-1.3", "0.05"), ("0.25", "0")])
+def test_periodic_interior_orbits(c):
+    cx, cy = Decimal(c[0]), Decimal(c[1])
+    a = hp.compute_single_highprec_orbit(cx, cy, 5000, 0, 0.0, 0.0, 300)
+    b = hp.decimal_orbit(cx, cy, 5000, 0, 0.0, 0.0, 300)
+    assert a[2] == b[2] == 5000
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_uncertified_orbit_takes_the_decimal_path():
+    """A bounded chaotic Burning Ship orbit at 256 bits: the two fixed-point runs part
+    after ~900 steps, and the result is the Decimal loop's."""
+    from test_orbit_native import _points as pts
+    cx, cy = pts(256 + 31, 6, 1)[3]
+    lo, hi = hp.orbit_limbs(256)
+
+    def seeds(L, I):
+        return hp._seeds(1, cx, cy, 0.0, 0.0, 0.25, 1.0, L, I)
+
+    a = hp._native_orbit(seeds, hi, 3000, 1, 3)
+    b = hp._native_orbit(seeds, lo, 3000, 1, 3)
+    assert not np.array_equal(a[0], b[0])
+    got = hp.compute_single_highprec_orbit(cx, cy, 3000, 1, 0.0, 0.0, 256)
+    ref = hp.decimal_orbit(cx, cy, 3000, 1, 0.0, 0.0, 256)
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+
+
+def test_fixed_point_conversion():
+    L = 4
+    for v in ("0", "1", "-1", "0.5", "-0.75", "255.125", "-3.14159265358979323846264338327950288"):
+        limbs = hp.to_fixed(Decimal(v), L)
+        q = int.from_bytes(limbs.tobytes(), "little")
+        if q >= 1 << (64 * L - 1):
+            q -= 1 << (64 * L)
+        with localcontext() as ctx:
+            ctx.prec = 200
+            assert abs(Decimal(q) / Decimal(2) ** (64 * (L - 1)) - Decimal(v)) <= Decimal(2) ** -(64 * (L - 1))
+    with pytest.raises(OverflowError):
+        hp.to_fixed(Decimal(2) ** 70, 2)
+    assert [hp.orbit_int_limbs(t, n) for t, n in ((0, 3), (1, 3), (4, 3), (4, 4), (4, 8))] == [1, 1, 1, 2, 3]
