@@ -109,6 +109,28 @@ __global__ void __launch_bounds__(256) colour_kernel(const ApFrameParams p, cons
     store_rgb(b.rgb, p.is_hdr, idx, r, g, bb);
 }
 
+// ----------------------------------------------------------- rebase bins
+// Glitched pixels per cell of the 16 x 16 grid the rebase loop picks its next
+// reference from (math_core/engine.py:1923-1935: row bin (16 j) / H, column bin
+// (16 i) / W).  One block per 256 x 16 pixel slab; shared-memory counts, then
+// one atomic per non-empty cell.
+__global__ void __launch_bounds__(256) glitch_bins_kernel(const uint8_t* __restrict__ g, int W, int H,
+                                                          int* __restrict__ counts) {
+    __shared__ int c[256];
+    c[threadIdx.x] = 0;
+    __syncthreads();
+    const int i = blockIdx.x * 256 + threadIdx.x;
+    if (i < W) {
+        const int bc = min(15, (i * 16) / W);
+        const int j0 = blockIdx.y * 16, j1 = min(H, j0 + 16);
+        for (int j = j0; j < j1; ++j) {
+            if (g[(size_t)j * W + i]) atomicAdd(&c[min(15, (j * 16) / H) * 16 + bc], 1);
+        }
+    }
+    __syncthreads();
+    if (c[threadIdx.x]) atomicAdd(counts + threadIdx.x, c[threadIdx.x]);
+}
+
 }  // namespace ap
 
 extern "C" int ap_edge_detect(const float* iter_map, uint8_t* edge_mask, int32_t width,
@@ -161,4 +183,22 @@ extern "C" int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* 
     dim3 grid((p->width + 15) / 16, (p->height + 15) / 16);
     ap::colour_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(*p, *b, hist);
     return ap::check_launch("colour_kernel");
+}
+
+extern "C" int ap_glitch_bins(const uint8_t* glitch_map, int32_t width, int32_t height,
+                              int32_t* counts, void* stream) {
+    if (!glitch_map || !counts || width <= 0 || height <= 0 || width > (1 << 26) / 16 ||
+        height > (1 << 26) / 16) {
+        ap::set_error("ap_glitch_bins: bad arguments");
+        return AP_E_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(counts, 0, 256 * sizeof(int32_t), st);
+    if (e != cudaSuccess) {
+        ap::set_error("ap_glitch_bins: memset: %s", cudaGetErrorString(e));
+        return AP_E_CUDA;
+    }
+    dim3 grid((width + 255) / 256, (height + 15) / 16);
+    ap::glitch_bins_kernel<<<grid, 256, 0, st>>>(glitch_map, width, height, counts);
+    return ap::check_launch("glitch_bins_kernel");
 }

@@ -85,7 +85,8 @@ __global__ void __launch_bounds__(256) pack_fe32_kernel(const double4* __restric
     if (t < n) {
         const double4 Z = orb[t];
         // .w = 1 marks a close approach (|Z|^2 < 2^-100) that takes the FP64 slow path
-        orb32[t] = make_float4((float)Z.x, (float)Z.y, (float)Z.w, Z.w < 0x1p-100 ? 1.0f : 0.0f);
+        const double r2 = Z.x * Z.x + Z.y * Z.y;
+        orb32[t] = make_float4((float)Z.x, (float)Z.y, (float)r2, r2 < 0x1p-100 ? 1.0f : 0.0f);
     }
     if (T == nullptr || Rs == nullptr || t >= ref_len * 16) return;
     const int k = t >> 4, d = t & 15;

@@ -14,7 +14,16 @@ __global__ void __launch_bounds__(256) pack_orbit_kernel(const double* __restric
     const double rx = re[k], ry = im[k];
     const double r_mag2 = rx * rx + ry * ry;
     const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;
-    out[k] = make_double4(rx, ry, thr, r_mag2);
+    // Safe radius s: for |dz| < s the rounded |Z + dz|^2 is neither above the
+    // bailout 65536 (|Z| + s <= 256 (1 - 1e-12)) nor below the Pauldelbrot
+    // threshold 1e-6 |Z|^2 (|Z| - s >= 1e-3 |Z| (1 + 1e-7)); the 1e-12 margins
+    // cover the roundings of |Z|, of Z + dz and of both squares.  Stored as
+    // s^2 (1 - 1e-12) to be compared with the rounded |dz|^2.
+    const double rz = sqrt(r_mag2);
+    double s = 256.0 * (1.0 - 1e-12) - rz * (1.0 + 1e-12);
+    if (thr >= 0.0) s = fmin(s, rz * (1.0 - 1e-12) * (1.0 - 1.0000001e-3));
+    s = s > 0.0 ? s : 0.0;
+    out[k] = make_double4(rx, ry, thr, s * s * (1.0 - 1e-12));
 }
 
 __global__ void __launch_bounds__(256) pack_bla_kernel(const double* __restrict__ T, int levels,

@@ -5,8 +5,11 @@
 // by ap_render_pass when the buffers carry the packed orbit (ap_pack_orbit)
 // and, with BLA, the packed table (ap_pack_bla).  What changes is only how the
 // loop gets its inputs:
-//   * one 32-byte read per step: Z_k, the Pauldelbrot threshold and |Z_k|^2
-//     precomputed exactly as the step would compute them;
+//   * one 32-byte read per step: Z_k, the Pauldelbrot threshold precomputed
+//     exactly as the step would compute it, and a safe radius: while |dz| is
+//     below it neither the escape test nor the Pauldelbrot test can fire, so
+//     |Z + dz|^2 is not formed (the rounded |dz|^2 decides, and the BLA test
+//     reuses it);
 //   * the 16 BLA radii of step k in one 128-byte row.  Radii never increase
 //     with the level (each level's radius is the min of its first half's), and
 //     levels past the end of the orbit hold 0, so the largest admissible level
@@ -84,16 +87,18 @@ __global__ void __launch_bounds__(256, 4) perturb_coarse_kernel(const ApFramePar
         const double4 Z = ldg4(orb + k);
         const double rx = Z.x, ry = Z.y;
         const double zx = rx + dzx, zy = ry + dzy;
-        const double mag2 = zx * zx + zy * zy;
-        if (mag2 > kBailout) {
-            if (esc_glitch && strict && k > 15 && Z.w < 4.0) glitch = 1;
-            o = escaped_sample(k, mag2, inv_ln);
-            finished = true;
-            break;
+        const double dz_mag2 = dzx * dzx + dzy * dzy;
+        if (!(dz_mag2 < Z.w)) {  // outside the safe radius: the tests may fire
+            const double mag2 = zx * zx + zy * zy;
+            if (mag2 > kBailout) {
+                if (esc_glitch && strict && k > 15 && (rx * rx + ry * ry) < 4.0) glitch = 1;
+                o = escaped_sample(k, mag2, inv_ln);
+                finished = true;
+                break;
+            }
+            if (strict && k > 15 && mag2 < Z.z) glitch = 1;
         }
-        if (strict && k > 15 && mag2 < Z.z) glitch = 1;
         if (BLA && k < ref_len - 1) {
-            const double dz_mag2 = dzx * dzx + dzy * dzy;
             const double* row = R + (size_t)k * 16;
             if (dz_mag2 < __ldg(row)) {
                 int hi = max_level;

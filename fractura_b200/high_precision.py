@@ -87,6 +87,20 @@ def _native():
     return _lib.load()
 
 
+_PAIR_POOL = None
+_PAIR_LOCK = threading.Lock()
+
+
+def _pair_pool():
+    """Threads that run the higher-precision orbit beside the lower one (the native
+    call releases the GIL)."""
+    global _PAIR_POOL
+    with _PAIR_LOCK:
+        if _PAIR_POOL is None:
+            _PAIR_POOL = ThreadPoolExecutor(max_workers=4, thread_name_prefix="orbit")
+        return _PAIR_POOL
+
+
 def _native_orbit(seeds_fn, L, max_iter, fractal_type, gen_n):
     import ctypes as C
     from . import _lib
@@ -124,8 +138,9 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     def seeds(L, I):
         return _seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki, L, I)
 
-    a = _native_orbit(seeds, hi, max_iter, fractal_type, gen_n)
+    fa = _pair_pool().submit(_native_orbit, seeds, hi, max_iter, fractal_type, gen_n)
     b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
+    a = fa.result()
     if a[2] == b[2] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]):
         return a
     return decimal_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,

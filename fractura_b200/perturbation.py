@@ -30,6 +30,34 @@ def _ptr(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
+def _pick_in_cluster(cluster, its, max_iter, visited):
+    """The reference's choice inside one grid cell (math_core/engine.py:1943-1985):
+    cluster = glitched (row, col) in row-major order, its = their smooth values."""
+    cr = np.median(cluster[:, 0])
+    cc = np.median(cluster[:, 1])
+    interior = (its < 0) | (its >= max_iter)
+    if np.any(interior):
+        pts = cluster[interior]
+        dists = (pts[:, 0] - cr) ** 2 + (pts[:, 1] - cc) ** 2
+        for d in np.argsort(dists):
+            cand = (int(pts[d, 0]), int(pts[d, 1]))
+            if cand not in visited:
+                return cand
+    escaped = (its > 0) & (its < max_iter)
+    cands = cluster[escaped]
+    if len(cands) > 0:
+        for c in np.argsort(-its[escaped]):
+            cand = (int(cands[c, 0]), int(cands[c, 1]))
+            if cand not in visited:
+                return cand
+    dists = (cluster[:, 0] - cr) ** 2 + (cluster[:, 1] - cc) ** 2
+    for d in np.argsort(dists):
+        cand = (int(cluster[d, 0]), int(cluster[d, 1]))
+        if cand not in visited:
+            return cand
+    return None
+
+
 def select_rebase_pixel(glitch_map, iter_map, max_iter, visited, W, H):
     """Next reference pixel (row, col) for a rebase pass, or None.
 
@@ -50,31 +78,47 @@ def select_rebase_pixel(glitch_map, iter_map, max_iter, visited, W, H):
         if counts[b] == 0:
             break
         cluster = gi[bin_idx == b]
-        its = iter_map[cluster[:, 0], cluster[:, 1]]
-        cr = np.median(cluster[:, 0])
-        cc = np.median(cluster[:, 1])
-        interior = (its < 0) | (its >= max_iter)
-        if np.any(interior):
-            pts = cluster[interior]
-            dists = (pts[:, 0] - cr) ** 2 + (pts[:, 1] - cc) ** 2
-            for d in np.argsort(dists):
-                cand = (int(pts[d, 0]), int(pts[d, 1]))
-                if cand not in visited:
-                    return cand
-        escaped = (its > 0) & (its < max_iter)
-        cands = cluster[escaped]
-        if len(cands) > 0:
-            for c in np.argsort(-its[escaped]):
-                cand = (int(cands[c, 0]), int(cands[c, 1]))
-                if cand not in visited:
-                    return cand
-        dists = (cluster[:, 0] - cr) ** 2 + (cluster[:, 1] - cc) ** 2
-        for d in np.argsort(dists):
-            cand = (int(cluster[d, 0]), int(cluster[d, 1]))
-            if cand not in visited:
-                return cand
+        cand = _pick_in_cluster(cluster, iter_map[cluster[:, 0], cluster[:, 1]], max_iter, visited)
+        if cand is not None:
+            return cand
     for g in range(len(gi)):
         cand = (int(gi[g, 0]), int(gi[g, 1]))
+        if cand not in visited:
+            return cand
+    return None
+
+
+def _cell_spans(n):
+    """[start, stop) of the pixels whose cell index min(15, 16 p // n) is 0..15."""
+    cell = np.minimum((np.arange(n) * 16) // n, 15)
+    return [(int(np.searchsorted(cell, q, "left")), int(np.searchsorted(cell, q, "right")))
+            for q in range(16)]
+
+
+def select_rebase_pixel_binned(counts, fetch_cell, fetch_all, max_iter, visited, W, H):
+    """select_rebase_pixel from the grid's cell counts (ap_glitch_bins): only the
+    cells it inspects are fetched (fetch_cell(r0, r1, c0, c1) -> glitch and smooth
+    values of that rectangle), the whole maps only when every cell is exhausted
+    (fetch_all()).  Same result as select_rebase_pixel on the whole maps: a cell's
+    glitched pixels in row-major order are the whole map's, restricted to the cell."""
+    counts = np.asarray(counts, dtype=np.int64)
+    if counts.sum() == 0:
+        return None
+    rows, cols = _cell_spans(H), _cell_spans(W)
+    for b in np.argsort(-counts):
+        if counts[b] == 0:
+            break
+        (r0, r1), (c0, c1) = rows[b // 16], cols[b % 16]
+        g, it = fetch_cell(r0, r1, c0, c1)
+        loc = np.argwhere(g > 0)
+        cluster = loc + np.array([r0, c0])
+        cand = _pick_in_cluster(cluster, it[loc[:, 0], loc[:, 1]], max_iter, visited)
+        if cand is not None:
+            return cand
+    g, _ = fetch_all()
+    gi = np.argwhere(g > 0)
+    for q in range(len(gi)):
+        cand = (int(gi[q, 0]), int(gi[q, 1]))
         if cand not in visited:
             return cand
     return None
@@ -348,18 +392,31 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     state = RebaseState((int(np.clip(p.ref_py / factor, 0, H - 1)), int(np.clip(p.ref_px / factor, 0, W - 1))),
                         exhaustive, strict_limit=128 if cpu_sem else 512)
     bits = compute_required_prec_bits(plot_width_dec)
+    d_counts = torch.empty(256, dtype=torch.int32, device=fr.glitch_out.device)
+
+    def fetch_cell(r0, r1, c0, c1):
+        g = fr.glitch_out[r0:r1, c0:c1].cpu().numpy()
+        it = fr.iter[r0:r1, c0:c1].cpu().numpy()
+        LAST_FRAME_STATS["d2h_bytes"] += g.nbytes + it.nbytes
+        return g, it
+
+    def fetch_all():
+        return fetch_cell(0, H, 0, W)
+
     while state.passes < MAX_REBASE_PASSES:
+        # the glitch map's 16 x 16 cell counts come from the device (1 KB), then
+        # only the cells the choice inspects
+        _lib.launch(L.ap_glitch_bins, _ptr(fr.glitch_out), W, H, _ptr(d_counts), stream_h,
+                    what="ap_glitch_bins")
         st.synchronize()
-        h_glitch = fr.glitch_out.cpu().numpy()
-        LAST_FRAME_STATS["d2h_bytes"] += h_glitch.nbytes
-        n_gl = int(np.count_nonzero(h_glitch))
+        counts = d_counts.cpu().numpy().astype(np.int64)
+        LAST_FRAME_STATS["d2h_bytes"] += counts.size * 4
+        n_gl = int(counts.sum())
         if not state.should_continue(n_gl):
             break
         state.passes += 1
-        h_iter = fr.iter.cpu().numpy()
-        LAST_FRAME_STATS["d2h_bytes"] += h_iter.nbytes
         LAST_FRAME_STATS["rebase_passes"] = state.passes
-        chosen = select_rebase_pixel(h_glitch, h_iter, max_iter, state.visited, W, H)
+        chosen = select_rebase_pixel_binned(counts, fetch_cell, fetch_all, max_iter, state.visited, W, H)
         if chosen is None:
             break
         g_row, g_col = chosen

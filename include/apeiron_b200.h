@@ -144,9 +144,11 @@ AP_API int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height
                      int32_t num_bins, int32_t* hist, float* cdf, void* stream);
 
 /* Reference orbit in the layout the perturbation kernels read: per step the
- * 32-byte record (Z_re, Z_im, Pauldelbrot threshold, |Z|^2), the threshold being
- * 1e-6 |Z|^2 where |Z|^2 > 1e-8 and -1 elsewhere (the glitch test of
- * math_core/cpu_kernels.py:428-431 as one compare).  out: [ref_len + 1, 4] float64. */
+ * 32-byte record (Z_re, Z_im, Pauldelbrot threshold, safe radius^2), the threshold
+ * being 1e-6 |Z|^2 where |Z|^2 > 1e-8 and -1 elsewhere (the glitch test of
+ * math_core/cpu_kernels.py:428-431 as one compare); while the rounded |dz|^2 is below
+ * the safe radius^2 neither the escape nor the glitch test can fire at that step.
+ * out: [ref_len + 1, 4] float64. */
 AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref_len, double* out,
                          void* stream);
 
@@ -188,6 +190,13 @@ AP_API int ap_histogram_cdf_noalloc(const float* iter_map, int32_t width, int32_
  * p->rebase_pass > 0 only pixels whose glitch_in is set are coloured (the pixels a
  * rebase pass re-rendered). */
 AP_API int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stream);
+
+/* Rebase-loop statistics on the device: counts[256] (int32, zeroed here) receives the
+ * number of glitched pixels in each cell of the 16 x 16 grid (row cell 16 j / H, column
+ * cell 16 i / W) from which math_core/engine.py:1923-1992 picks the next reference, so
+ * the host downloads 1 KB and then one cell's pixels instead of the whole maps. */
+AP_API int ap_glitch_bins(const uint8_t* glitch_map, int32_t width, int32_t height, int32_t* counts,
+                          void* stream);
 
 /* Chained-BLA table from a reference orbit, built on the device.
  * Replaces _jit_build_bla_table (math_core/high_precision.py:1101) and its upload

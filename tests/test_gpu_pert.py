@@ -96,8 +96,16 @@ def test_packed_orbit_and_bla_layouts():
     got = po.cpu().numpy()
     r2 = re * re + im * im
     assert np.array_equal(got[:, 0], re) and np.array_equal(got[:, 1], im)
-    assert np.array_equal(got[:, 3], r2)
     assert np.array_equal(got[:, 2], np.where(r2 > 1e-8, 1e-6 * r2, -1.0))
+    # safe radius: inside it neither the bailout nor the Pauldelbrot threshold is reachable
+    safe2 = got[:, 3]
+    s = np.sqrt(safe2)
+    rz = np.sqrt(r2)
+    assert np.all(safe2 >= 0.0)
+    assert np.all((rz + s) ** 2 < 65536.0)
+    glitchable = r2 > 1e-8
+    assert np.all((rz[glitchable] - s[glitchable]) ** 2 > 1e-6 * r2[glitchable])
+    assert np.count_nonzero(safe2) > 0.9 * len(safe2)
     T = oracle.build_bla(re, im, rl, 0, 1e-6, 16, 3, 0.25, 1.0)
     d_T = torch.from_numpy(T).cuda()
     pb = torch.empty(80 * rl, dtype=torch.float64, device="cuda")
@@ -134,3 +142,21 @@ def test_series_started_frame_matches_oracle(name, arith):
         int((it.view(np.uint32) != fr.iter_map.view(np.uint32)).sum())
     n_bad, max_diff = rgb_mismatch(rgb, fr.rgb)
     assert n_bad == 0, (n_bad, max_diff)
+
+
+@pytest.mark.parametrize("shape", [(1080, 1920), (90, 160), (37, 53), (1, 1)])
+def test_glitch_bins_match_numpy(shape):
+    """ap_glitch_bins: glitched pixels per cell of the rebase loop's 16 x 16 grid."""
+    import torch
+    H, W = shape
+    rng = np.random.default_rng(H * 7 + W)
+    g = (rng.random((H, W)) < 0.4).astype(np.uint8)
+    d_g = torch.from_numpy(g).cuda()
+    counts = torch.full((256,), 7, dtype=torch.int32, device="cuda")   # stale contents are cleared
+    L = _lib.load()
+    for _ in range(2):
+        _lib.check(L.ap_glitch_bins(C.c_void_p(d_g.data_ptr()), W, H, C.c_void_p(counts.data_ptr()), None),
+                   "ap_glitch_bins")
+        gi = np.argwhere(g > 0)
+        b = np.clip((gi[:, 0] * 16) // H, 0, 15) * 16 + np.clip((gi[:, 1] * 16) // W, 0, 15)
+        assert np.array_equal(counts.cpu().numpy(), np.bincount(b, minlength=256))
