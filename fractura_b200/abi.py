@@ -5,7 +5,7 @@ compares the sizes against the library's own ``sizeof`` report.
 """
 import ctypes as C
 
-AP_ABI_VERSION = 3
+AP_ABI_VERSION = 4
 
 AP_OK = 0
 AP_E_INVALID = -1
@@ -70,6 +70,15 @@ class ApFrameBuffers(C.Structure):
         ("glitch_out", C.c_void_p), ("kmap", C.c_void_p), ("s64", C.c_void_p),
         ("counters", C.c_void_p),
         ("orbit_packed", C.c_void_p), ("bla_packed", C.c_void_p),
+    ]
+
+
+class ApTileDesc(C.Structure):
+    _fields_ = [
+        ("p", ApFrameParams),
+        ("orbit_packed", C.c_void_p), ("bla_packed", C.c_void_p),
+        ("iter_map", C.c_void_p), ("kmap", C.c_void_p), ("s64", C.c_void_p),
+        ("glitch_out", C.c_void_p), ("counters", C.c_void_p), ("reserved", C.c_int64),
     ]
 
 

@@ -1,0 +1,238 @@
+// ap_coarse.cuh -- one pixel of a coarse FP64-delta perturbation pass on packed inputs.
+//
+// Same results as the generic render pass (ap_perturb.cuh) for tier
+// AP_TIER_PERTURB in AP_MODE_COARSE without in-kernel colouring; it is picked
+// by ap_render_pass when the buffers carry the packed orbit (ap_pack_orbit)
+// and, with BLA, the packed table (ap_pack_bla).  What changes is only how the
+// loop gets its inputs:
+//   * one 32-byte read per step: Z_k, the Pauldelbrot threshold precomputed
+//     exactly as the step would compute it, and a safe radius: while |dz| is
+//     below it neither the escape test nor the Pauldelbrot test can fire, so
+//     |Z + dz|^2 is not formed (the rounded |dz|^2 decides, and the BLA test
+//     reuses it);
+//   * the 16 BLA radii of step k in one 128-byte row.  Radii never increase
+//     with the level (each level's radius is the min of its first half's), and
+//     levels past the end of the orbit hold 0, so the largest admissible level
+//     -- the reference's top-down scan -- is found by a 4-probe binary search;
+//   * formula, BLA presence and arithmetic profile are template parameters;
+//   * no colouring (ap_colour runs afterwards), keeping registers low.
+#pragma once
+
+#include "ap_common.cuh"
+
+namespace ap {
+
+constexpr int kFtQuad = 0;   // Mandelbrot (0) and its Julia set (2)
+constexpr int kFtShip = 1;   // Burning Ship (1) and its Julia set (3)
+constexpr int kFtMulti = 4;  // Multibrot z^n + k z + c
+
+// 32-byte record through the read-only path (two 16-byte loads).
+__device__ __forceinline__ double4 ldg4(const double4* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldg(q), c = __ldg(q + 1);
+    return make_double4(a.x, a.y, c.x, c.y);
+}
+
+// One pixel (i, j) of a coarse pass: the whole stage-1 / stage-2 loop and the
+// output writes.  Shared by the per-frame kernel below and the persistent
+// batch kernel (ap_batch.cu), so both give identical values.
+template <int ARITH, int FT, bool BLA>
+__device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFrameBuffers& b, int i,
+                                             int j) {
+    constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
+    const int idx = j * p.width + i;
+    if (p.rebase_pass > 0 && b.glitch_in[idx] == 0) return;
+
+    const double sub_offset = ((double)p.factor - 1.0) * 0.5;
+    const double sub_i = (double)(i * p.factor) + sub_offset;
+    const double sub_j = (double)(j * p.factor) + sub_offset;
+    const double dcy = (p.ref_py - sub_j) * p.dy_hi;
+    const double dcx = (sub_i - p.ref_px) * p.dx_hi;
+    const bool julia = (p.fractal_type == 2 || p.fractal_type == 3);
+    const int ref_len = p.ref_len, max_iter = p.max_iter;
+    const double4* __restrict__ orb = reinterpret_cast<const double4*>(b.orbit_packed);
+
+    double dzx = julia ? dcx : 0.0, dzy = julia ? dcy : 0.0;
+    int k = 0;
+    if (p.bbsa_skip > 0 && FT != kFtShip) {
+        const double ux = dcx * p.bbsa_inv_r, uy = dcy * p.bbsa_inv_r;
+        if (ux * ux + uy * uy <= 1.0) {
+            bool eight = false;
+            for (int q = 8; q < 16; ++q) eight |= (p.bbsa[q] != 0.0);
+            const int top = eight ? 7 : 3;
+            double tr = ux * p.bbsa[2 * top] - uy * p.bbsa[2 * top + 1];
+            double ti = ux * p.bbsa[2 * top + 1] + uy * p.bbsa[2 * top];
+            for (int q = top - 1; q >= 0; --q) {
+                const double ar = p.bbsa[2 * q] + tr, ai = p.bbsa[2 * q + 1] + ti;
+                tr = ux * ar - uy * ai;
+                ti = ux * ai + uy * ar;
+            }
+            dzx = tr;
+            dzy = ti;
+            k = p.bbsa_skip;
+        }
+    }
+    const double dcpx = julia ? 0.0 : dcx, dcpy = julia ? 0.0 : dcy;
+    const bool strict = p.strict_glitch > 0;
+    const bool esc_glitch = (p.flags & AP_FLAG_ESCAPE_GLITCH) != 0;
+    const int k0 = k;
+    int glitch = 0, leaps = 0, skipped = 0, k2 = -1;
+    const double inv_ln = inv_ln_for(p.fractal_type, p.gen_n);
+    const double* __restrict__ R = b.bla_packed;
+    const double4* __restrict__ AB =
+        reinterpret_cast<const double4*>(b.bla_packed + (size_t)ref_len * 16);
+    const int max_level = p.bla_levels - 1;
+
+    SampleOut o;
+    bool finished = false;
+    while (k < ref_len) {
+        const double4 Z = ldg4(orb + k);
+        const double rx = Z.x, ry = Z.y;
+        const double zx = rx + dzx, zy = ry + dzy;
+        const double dz_mag2 = dzx * dzx + dzy * dzy;
+        if (!(dz_mag2 < Z.w)) {  // outside the safe radius: the tests may fire
+            const double mag2 = zx * zx + zy * zy;
+            if (mag2 > kBailout) {
+                if (esc_glitch && strict && k > 15 && (rx * rx + ry * ry) < 4.0) glitch = 1;
+                o = escaped_sample(k, mag2, inv_ln);
+                finished = true;
+                break;
+            }
+            if (strict && k > 15 && mag2 < Z.z) glitch = 1;
+        }
+        if (BLA && k < ref_len - 1) {
+            const double* row = R + (size_t)k * 16;
+            if (dz_mag2 < __ldg(row)) {
+                int hi = max_level;
+                if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
+                int lo = 0;  // row[lo] admissible
+#pragma unroll 4
+                for (int it = 0; it < 4; ++it) {
+                    if (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (dz_mag2 < __ldg(row + mid)) lo = mid;
+                        else hi = mid - 1;
+                    }
+                }
+                const double4 e = ldg4(AB + (size_t)k * 16 + lo);
+                double nx, ny;
+                if (kCpu) {
+                    nx = (e.x * dzx - e.y * dzy) + (e.z * dcpx - e.w * dcpy);
+                    ny = (e.x * dzy + e.y * dzx) + (e.z * dcpy + e.w * dcpx);
+                } else {
+                    nx = fma(e.x, dzx, fma(-e.y, dzy, fma(e.z, dcpx, -e.w * dcpy)));
+                    ny = fma(e.x, dzy, fma(e.y, dzx, fma(e.z, dcpy, e.w * dcpx)));
+                }
+                dzx = nx;
+                dzy = ny;
+                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) {
+                    o = interior_sample();
+                    o.s = (float)k;
+                    o.s64 = (double)k;
+                    o.k = k;
+                    glitch = 1;
+                    finished = true;
+                    break;
+                }
+                k += 1 << lo;
+                ++leaps;
+                skipped += 1 << lo;
+                continue;
+            }
+        }
+        if (FT == kFtQuad) {
+            double nx, ny;
+            if (kCpu) {
+                nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+                ny = 2.0 * (zx * dzy + ry * dzx) + dcpy;
+            } else {
+                nx = fma(2.0 * rx + dzx, dzx, fma(-(2.0 * ry + dzy), dzy, dcpx));
+                ny = fma(2.0, fma(zx, dzy, ry * dzx), dcpy);
+            }
+            dzx = nx;
+            dzy = ny;
+        } else if (FT == kFtShip) {
+            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+            const double ddx = zx * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+            const double ddy = zy * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcpy;
+            dzx = nx;
+        } else {
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p.gen_n - 1; ++t) {
+                const double t1r = pr * rx - pi * ry, t1i = pr * ry + pi * rx;
+                const double sr = pr + qr, si = pi + qi;
+                const double t2r = sr * dzx - si * dzy, t2i = sr * dzy + si * dzx;
+                pr = t1r + t2r;
+                pi = t1i + t2i;
+                const double nqr = qr * rx - qi * ry, nqi = qr * ry + qi * rx;
+                qr = nqr;
+                qi = nqi;
+            }
+            const double kzr = p.gen_kr * dzx - p.gen_ki * dzy;
+            const double kzi = p.gen_kr * dzy + p.gen_ki * dzx;
+            dzx = pr + kzr + dcpx;
+            dzy = pi + kzi + dcpy;
+        }
+        ++k;
+    }
+
+    if (!finished) {
+        // Stage 2: past the end of the reference orbit, iterate z directly.
+        const double4 Zend = ldg4(orb + ref_len);
+        double zx = Zend.x + dzx, zy = Zend.y + dzy;
+        const double cx = julia ? p.julia_cx_hi : p.ref_cx + dcx;
+        const double cy = julia ? p.julia_cy_hi : p.ref_cy + dcy;
+        if (ref_len < max_iter) glitch = 1;
+        k2 = k;
+        const bool nan_guard = (p.flags & AP_FLAG_NAN_GUARD) != 0;
+        o = interior_sample();
+        while (k < max_iter) {
+            const double zx2 = zx * zx, zy2 = zy * zy;
+            const double mag2 = zx2 + zy2;
+            if (nan_guard && (isnan(mag2) || isinf(mag2))) {
+                o.s = (float)k;
+                o.s64 = (double)k;
+                o.k = k;
+                glitch = 1;
+                break;
+            }
+            if (mag2 > kBailout) {
+                o = escaped_sample(k, mag2, inv_ln);
+                break;
+            }
+            if (FT == kFtQuad) {
+                zy = 2.0 * zx * zy + cy;
+                zx = zx2 - zy2 + cx;
+            } else if (FT == kFtShip) {
+                zy = 2.0 * fabs(zx) * fabs(zy) - cy;
+                zx = zx2 - zy2 + cx;
+            } else {
+                double zr = zx, zi = zy;
+                for (int t = 0; t < p.gen_n - 1; ++t) {
+                    const double nr = zr * zx - zi * zy, ni = zr * zy + zi * zx;
+                    zr = nr;
+                    zi = ni;
+                }
+                const double kzr = p.gen_kr * zx - p.gen_ki * zy;
+                const double kzi = p.gen_kr * zy + p.gen_ki * zx;
+                zx = zr + kzr + cx;
+                zy = zi + kzi + cy;
+            }
+            ++k;
+        }
+    }
+    const int k_end = (o.k == -1) ? max_iter : k;
+    b.iter_map[idx] = o.s;
+    if (b.kmap) b.kmap[idx] = o.k;
+    if (b.s64) b.s64[idx] = o.s64;
+    if (b.glitch_out) b.glitch_out[idx] = glitch ? 1 : 0;
+    if (b.counters) {
+        const int it1 = (k2 < 0 ? k_end - k0 : k2 - k0) - skipped;
+        const int it2 = k2 < 0 ? 0 : k_end - k2;
+        reinterpret_cast<int4*>(b.counters)[idx] = make_int4(it1, leaps, it2, 0);
+    }
+}
+
+}  // namespace ap

@@ -26,7 +26,7 @@ extern "C" {
 #define AP_API
 #endif
 
-#define AP_ABI_VERSION 3
+#define AP_ABI_VERSION 4
 
 /* Return codes. */
 #define AP_OK 0
@@ -115,6 +115,21 @@ typedef struct ApFrameBuffers {
     const double* orbit_packed; /* optional [ref_len + 1, 4] from ap_pack_orbit */
     const double* bla_packed;   /* optional, from ap_pack_bla (needs orbit_packed) */
 } ApFrameBuffers;
+
+/* One tile of a batch (ap_render_batch): a coarse AP_TIER_PERTURB pass on packed
+ * inputs, without in-kernel colour (p.flags has AP_FLAG_NO_RGB), with its own
+ * parameters, reference orbit and outputs.  448 bytes. */
+typedef struct ApTileDesc {
+    ApFrameParams p;
+    const double* orbit_packed; /* ap_pack_orbit records of the tile's reference */
+    const double* bla_packed;   /* ap_pack_bla rows when p.bla_levels > 1, else NULL */
+    float* iter_map;            /* [H, W] smooth values (required) */
+    int32_t* kmap;              /* optional [H, W] escape steps */
+    double* s64;                /* optional [H, W] float64 smooth values */
+    uint8_t* glitch_out;        /* optional [H, W] glitch flags */
+    int32_t* counters;          /* optional [H, W, 4] work counters, 16-byte aligned */
+    int64_t reserved;
+} ApTileDesc;
 
 /* Library identity. */
 AP_API int ap_abi_version(void);
@@ -244,6 +259,22 @@ AP_API int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_
                               int32_t gen_n, int32_t max_iter, int32_t escape_only,
                               double* ref_re, double* ref_im, int32_t* ref_len,
                               double* escape_mag2, uint64_t* trace_hash);
+
+/* Batches (no single counterpart: the reference renders tile by tile, e.g.
+ * workers/image_workers.py:428-601 calling render_frame_ssaa per tile).
+ * ap_batch_plan (HOST): checks every tile of host_tiles[n] and writes first_patch[n + 1],
+ * the number of each tile's first 256-pixel patch (patch_w x patch_h == 256) and the total;
+ * tiles should come in decreasing order of expected cost.
+ * ap_render_batch: renders all tiles with one persistent kernel of blocks_per_sm blocks per
+ * SM that take patches from a shared counter (device word *queue_head, reset here);
+ * tiles and first_patch are device copies of the planned arrays.  min_blocks (4 or 6) picks
+ * the register budget the kernel is compiled for; arith is the tiles' common profile.
+ * Values equal ap_render_pass's for each tile. */
+AP_API int ap_batch_plan(const ApTileDesc* host_tiles, int32_t n, int32_t patch_w, int32_t patch_h,
+                         int64_t* first_patch);
+AP_API int ap_render_batch(const ApTileDesc* tiles, const int64_t* first_patch, int32_t n,
+                           int32_t arith, int32_t patch_w, int32_t patch_h, int32_t blocks_per_sm,
+                           int32_t min_blocks, unsigned long long* queue_head, void* stream);
 
 /* Measurement helper (no counterpart in the reference): number of kernels this
  * library has launched in the process so far. */

@@ -102,8 +102,10 @@ def test_packed_orbit_and_bla_layouts():
     s = np.sqrt(safe2)
     rz = np.sqrt(r2)
     assert np.all(safe2 >= 0.0)
-    assert np.all((rz + s) ** 2 < 65536.0)
-    glitchable = r2 > 1e-8
+    inside = safe2 > 0.0          # zero where |Z| >= 256 (no step is safe there)
+    assert np.all((rz[inside] + s[inside]) ** 2 < 65536.0)
+    assert np.all(safe2[rz >= 256.0] == 0.0)
+    glitchable = inside & (r2 > 1e-8)
     assert np.all((rz[glitchable] - s[glitchable]) ** 2 > 1e-6 * r2[glitchable])
     assert np.count_nonzero(safe2) > 0.9 * len(safe2)
     T = oracle.build_bla(re, im, rl, 0, 1e-6, 16, 3, 0.25, 1.0)
