@@ -1,0 +1,296 @@
+"""Many perturbation tiles in one persistent kernel (ap_render_batch).
+
+The reference renders tiles one call at a time (its mosaic exporter,
+workers/image_workers.py:428-601, calls render_frame_ssaa per tile).  Here a
+batch of tiles of any size, formula and max_iter is prepared on the host
+(reference orbit, device BLA table, packed inputs, one descriptor per tile) and
+rendered by a single persistent kernel whose blocks take 256-pixel patches from
+a shared counter.  Each tile's values equal the per-frame coarse pass
+(ap_render_pass) for the same parameters.
+
+    tiles = [Tile(cx, cy, width, W, H, max_iter, fractal_type=...), ...]
+    batch = prepare_batch(tiles)            # orbits, tables, descriptors
+    cfg = tune(batch)                       # autotuned patch shape and occupancy
+    batch.render(cfg)                       # or: g = batch.capture(cfg); g.replay()
+    batch.tiles_out[t]["iter"]              # [H, W] float32 smooth values on the device
+"""
+import ctypes as C
+import threading
+from concurrent.futures import ThreadPoolExecutor
+from dataclasses import dataclass
+from decimal import Decimal, localcontext
+
+import numpy as np
+
+from . import _lib, abi
+from . import high_precision as hp
+from .config import ACCURATE_BLA_EPS, decimal_context
+
+BLA_LEVELS = 16
+
+
+@dataclass
+class Tile:
+    """One coarse perturbation-tier view: centre, width, size, depth and formula."""
+    cx: Decimal
+    cy: Decimal
+    width: Decimal
+    W: int
+    H: int
+    max_iter: int
+    fractal_type: int = 0
+    julia_cx: float = 0.0
+    julia_cy: float = 0.0
+    gen_n: int = 3
+    gen_kr: float = 0.25
+    gen_ki: float = 1.0
+    bla: bool = True           # chained-BLA leaps (Mandelbrot, Julia, Multibrot)
+    strict_glitch: bool = True  # Pauldelbrot glitch flags
+
+
+@dataclass(frozen=True)
+class BatchConfig:
+    """Launch shape of the persistent kernel: patch_w x patch_h = 256 pixels per work
+    item, blocks_per_sm resident blocks, min_blocks = the register budget (4 or 6)."""
+    patch_w: int = 16
+    patch_h: int = 16
+    blocks_per_sm: int = 4
+    min_blocks: int = 4
+
+
+CANDIDATES = tuple(BatchConfig(pw, 256 // pw, bps, mb)
+                   for pw in (16, 32, 64, 8)
+                   for (bps, mb) in ((4, 4), (8, 4), (6, 6)))
+
+
+def _ptr(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+class PreparedBatch:
+    """Device inputs, outputs and descriptors of a batch."""
+
+    def __init__(self, tiles, arith_code, stream):
+        self.tiles = tiles
+        self.arith = arith_code
+        self.stream = stream
+        self.tiles_out = []
+        self.keep = []          # device tensors the descriptors point into
+        self.order = []         # descriptor order (tile indices, largest cost first)
+        self.desc_dev = None
+        self.first_dev = None
+        self.head = None
+        self.n = len(tiles)
+        self.total_patches = {}
+
+    # -- launch ------------------------------------------------------------
+    def _plan(self, cfg):
+        key = (cfg.patch_w, cfg.patch_h)
+        if key not in self.total_patches:
+            import torch
+            L = _lib.load()
+            first = np.zeros(self.n + 1, np.int64)
+            _lib.check(L.ap_batch_plan(C.byref(self.desc_host), self.n, cfg.patch_w, cfg.patch_h,
+                                       first.ctypes.data_as(C.c_void_p)), "ap_batch_plan")
+            dev = torch.from_numpy(first).cuda()
+            self.total_patches[key] = (int(first[-1]), dev)
+        return self.total_patches[key][1]
+
+    def render(self, cfg=BatchConfig()):
+        """Render every tile (one persistent launch on the batch's stream)."""
+        import torch
+        first = self._plan(cfg)
+        L = _lib.load()
+        with torch.cuda.stream(self.stream):
+            _lib.launch(L.ap_render_batch, _ptr(self.desc_dev), _ptr(first), self.n, self.arith,
+                        cfg.patch_w, cfg.patch_h, cfg.blocks_per_sm, cfg.min_blocks,
+                        _ptr(self.head), C.c_void_p(self.stream.cuda_stream), what="ap_render_batch")
+
+    def capture(self, cfg=BatchConfig()):
+        """A CUDA graph of the batch's launch (queue reset + persistent kernel); replaying
+        it renders the batch again from the same device inputs."""
+        import torch
+        self._plan(cfg)
+        self.render(cfg)                       # warm-up outside the capture
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=self.stream):
+            first = self._plan(cfg)
+            L = _lib.load()
+            _lib.check(L.ap_render_batch(_ptr(self.desc_dev), _ptr(first), self.n, self.arith,
+                                         cfg.patch_w, cfg.patch_h, cfg.blocks_per_sm, cfg.min_blocks,
+                                         _ptr(self.head), C.c_void_p(self.stream.cuda_stream)),
+                       "ap_render_batch")
+        return g
+
+    def nominal_iterations(self):
+        """Sum over tiles of their escape steps (max_iter for pixels that never escape)."""
+        tot = 0
+        for t, out in zip(self.tiles, self.tiles_out):
+            k = out["kmap"].cpu().numpy()
+            tot += int(k[k >= 0].astype(np.int64).sum()) + t.max_iter * int(np.count_nonzero(k == -1))
+        return tot
+
+
+def _tile_inputs(t, cpu_sem, bla_form, torch, stream, L, scratch):
+    """Orbit, packed records, BLA rows, outputs and parameters of one tile, as the
+    coarse pass of render_perturbation_frame sets them (factor 1, one reference)."""
+    from .perturbation import max_delta_c
+    pw = Decimal(t.width)
+    with localcontext(decimal_context(pw)):
+        ph = pw * (Decimal(t.H) / Decimal(t.W))
+        dx = float(pw / Decimal(max(1, t.W - 1)))
+        dy = float(ph / Decimal(max(1, t.H - 1)))
+    bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
+        Decimal(t.cx), Decimal(t.cy), pw, ph, t.max_iter, t.W, t.H, fractal_type=t.fractal_type,
+        julia_cx=t.julia_cx, julia_cy=t.julia_cy, gen_n=t.gen_n, gen_kr=t.gen_kr, gen_ki=t.gen_ki)
+    n = rl + 1
+    d_re = torch.from_numpy(np.ascontiguousarray(re[:n])).to("cuda", non_blocking=False)
+    d_im = torch.from_numpy(np.ascontiguousarray(im[:n])).to("cuda", non_blocking=False)
+    orbit = torch.empty(6 * n, dtype=torch.float64, device="cuda")
+    s = C.c_void_p(stream.cuda_stream)
+    _lib.check(L.ap_pack_orbit(_ptr(d_re), _ptr(d_im), int(rl), _ptr(orbit), s), "ap_pack_orbit")
+    use_bla = t.bla and t.fractal_type in (0, 2, 4) and rl > 0
+    ref_px, ref_py = float(t.W - 1) * float(bu), float(t.H - 1) * float(bv)
+    bla_packed = None
+    if use_bla:
+        table = scratch(BLA_LEVELS * rl * 5)
+        if bla_form == "accurate":
+            dcm = max_delta_c(ref_px, ref_py, t.W, t.H, dx, dy)
+            _lib.check(L.ap_build_bla_dc(_ptr(d_re), _ptr(d_im), int(rl), int(t.fractal_type),
+                                         ACCURATE_BLA_EPS, float(dcm), BLA_LEVELS, int(t.gen_n),
+                                         float(t.gen_kr), float(t.gen_ki), _ptr(table), s), "ap_build_bla_dc")
+        else:
+            _lib.check(L.ap_build_bla(_ptr(d_re), _ptr(d_im), int(rl), int(t.fractal_type), 1e-6,
+                                      BLA_LEVELS, int(t.gen_n), float(t.gen_kr), float(t.gen_ki),
+                                      _ptr(table), s), "ap_build_bla")
+        bla_packed = torch.empty(80 * rl, dtype=torch.float64, device="cuda")
+        _lib.check(L.ap_pack_bla(_ptr(table), BLA_LEVELS, int(rl), _ptr(bla_packed), s), "ap_pack_bla")
+        stream.synchronize()  # the table scratch is reused by the next tile
+    flags = abi.AP_FLAG_NO_RGB | ((abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem
+                                  else abi.AP_FLAG_NAN_GUARD)
+    p = abi.new_params(width=t.W, height=t.H, factor=1, max_iter=int(t.max_iter),
+                       fractal_type=int(t.fractal_type), tier=abi.AP_TIER_PERTURB,
+                       arith=abi.AP_ARITH_REF_CPU if cpu_sem else abi.AP_ARITH_REF_CUDA,
+                       mode=abi.AP_MODE_COARSE, flags=flags, gen_n=int(t.gen_n),
+                       gen_kr=float(t.gen_kr), gen_ki=float(t.gen_ki), dx_hi=dx, dy_hi=dy,
+                       ref_px=ref_px, ref_py=ref_py, ref_cx=float(bcx), ref_cy=float(bcy),
+                       julia_cx_hi=float(t.julia_cx), julia_cy_hi=float(t.julia_cy), ref_len=int(rl),
+                       bla_levels=BLA_LEVELS if use_bla else 0,
+                       strict_glitch=1 if t.strict_glitch else 0)
+    out = dict(iter=torch.empty((t.H, t.W), dtype=torch.float32, device="cuda"),
+               kmap=torch.empty((t.H, t.W), dtype=torch.int32, device="cuda"),
+               glitch=torch.empty((t.H, t.W), dtype=torch.uint8, device="cuda"))
+    return p, orbit, bla_packed, out, (d_re, d_im), rl
+
+
+def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, workers=8):
+    """Host and device preparation of a batch: reference orbits (in parallel threads;
+    the native orbit code releases the GIL), device BLA tables, packed records,
+    outputs and the descriptor array, ordered by estimated cost (pixels x ref_len)."""
+    import torch
+    if bla_form not in ("reference", "accurate"):
+        raise ValueError("bla_form must be 'reference' or 'accurate'")
+    cpu_sem = arith == "ref_cpu"
+    if arith not in ("ref_cpu", "ref_cuda"):
+        raise ValueError("arith must be 'ref_cpu' or 'ref_cuda'")
+    if not tiles:
+        raise ValueError("a batch needs at least one tile")
+    L = _lib.load()
+    stream = stream or torch.cuda.current_stream()
+    b = PreparedBatch(list(tiles), abi.AP_ARITH_REF_CPU if cpu_sem else abi.AP_ARITH_REF_CUDA, stream)
+    # the orbits first, concurrently (host work)
+    with ThreadPoolExecutor(max_workers=max(1, workers)) as ex:
+        orbits = list(ex.map(lambda t: _warm_orbit(t), b.tiles))
+    del orbits
+    scratch_box = {}
+    lock = threading.Lock()
+
+    def scratch(n):
+        with lock:
+            cur = scratch_box.get("t")
+            if cur is None or cur.numel() < n:
+                scratch_box["t"] = torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
+            return scratch_box["t"]
+
+    recs = []
+    with torch.cuda.stream(stream):
+        for t in b.tiles:
+            recs.append(_tile_inputs(t, cpu_sem, bla_form, torch, stream, L, scratch))
+    stream.synchronize()
+    cost = [t.W * t.H * max(1, r[5]) for t, r in zip(b.tiles, recs)]
+    b.order = sorted(range(len(b.tiles)), key=lambda q: -cost[q])
+    arr = (abi.ApTileDesc * len(b.tiles))()
+    for slot, q in enumerate(b.order):
+        p, orbit, bla_packed, out, ref, _ = recs[q]
+        d = arr[slot]
+        d.p = p
+        d.orbit_packed = _ptr(orbit)
+        d.bla_packed = _ptr(bla_packed)
+        d.iter_map, d.kmap, d.glitch_out = _ptr(out["iter"]), _ptr(out["kmap"]), _ptr(out["glitch"])
+        b.keep.extend([orbit, bla_packed, ref])
+    b.tiles_out = [recs[q][3] for q in range(len(b.tiles))]
+    b.params = [recs[q][0] for q in range(len(b.tiles))]
+    b.desc_host = arr
+    raw = np.frombuffer(bytes(arr), dtype=np.uint8)
+    b.desc_dev = torch.from_numpy(raw.copy()).cuda()
+    b.head = torch.zeros(1, dtype=torch.int64, device="cuda")
+    return b
+
+
+def _warm_orbit(t):
+    """Compute (and cache) a tile's reference orbit on the host."""
+    pw = Decimal(t.width)
+    with localcontext(decimal_context(pw)):
+        ph = pw * (Decimal(t.H) / Decimal(t.W))
+    return hp.find_optimal_reference_orbit(
+        Decimal(t.cx), Decimal(t.cy), pw, ph, t.max_iter, t.W, t.H, fractal_type=t.fractal_type,
+        julia_cx=t.julia_cx, julia_cy=t.julia_cy, gen_n=t.gen_n, gen_kr=t.gen_kr, gen_ki=t.gen_ki)
+
+
+# ------------------------------------------------------------------ tuner
+_TUNED = {}
+_TUNED_LOCK = threading.Lock()
+
+
+def tuning_key(batch):
+    """Batches with the same device, profile, tile count and (log2-bucketed) pixel and
+    iteration scales share a tuned configuration."""
+    import torch
+    px = sum(t.W * t.H for t in batch.tiles)
+    it = sum(t.max_iter for t in batch.tiles)
+    return (torch.cuda.get_device_name(), batch.arith, len(batch.tiles),
+            int(np.log2(max(px, 1))), int(np.log2(max(it, 1))))
+
+
+def tune(batch, candidates=CANDIDATES, reps=2):
+    """Time every candidate launch shape on the batch itself (CUDA events on the batch's
+    stream, after one warm-up) and keep the fastest; cached per tuning_key."""
+    import torch
+    key = tuning_key(batch)
+    with _TUNED_LOCK:
+        if key in _TUNED:
+            return _TUNED[key][0]
+    timings = []
+    for cfg in candidates:
+        batch.render(cfg)
+        best = None
+        for _ in range(reps):
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(batch.stream)
+            batch.render(cfg)
+            e.record(batch.stream)
+            e.synchronize()
+            ms = a.elapsed_time(e)
+            best = ms if best is None else min(best, ms)
+        timings.append((best, cfg))
+    timings.sort(key=lambda x: x[0])
+    with _TUNED_LOCK:
+        _TUNED[key] = (timings[0][1], timings)
+    return timings[0][1]
+
+
+def tuned_timings(batch):
+    """(ms, config) of every candidate the tuner measured for this batch's key."""
+    with _TUNED_LOCK:
+        return list(_TUNED.get(tuning_key(batch), (None, []))[1])

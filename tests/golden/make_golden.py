@@ -219,7 +219,9 @@ def config3_centre(seed=SEED, digits=600):
 def write_workloads():
     cx3, cy3 = config3_centre()
     cx2, cy2 = config2_centre()
-    wl = {"seed": SEED, "config2_centre": [cx2, cy2], "config3_centre": [cx3, cy3]}
+    path = os.path.join(HERE, "workloads.json")
+    wl = json.load(open(path)) if os.path.exists(path) else {}
+    wl.update({"seed": SEED, "config2_centre": [cx2, cy2], "config3_centre": [cx3, cy3]})
     with open(os.path.join(HERE, "workloads.json"), "w") as f:
         json.dump(wl, f, indent=1)
     print("  wrote workloads.json")
@@ -470,6 +472,78 @@ def gen_fexp():
     save("fexp_samples.npz", meta=json.dumps(meta), **out)
 
 
+CONFIG4_FORMULAS = [
+    # fractal_type, julia (jx, jy), gen_n, kr, ki
+    (0, (0.0, 0.0), 3, 0.25, 1.0),
+    (1, (0.0, 0.0), 3, 0.25, 1.0),
+    (2, (-0.8, 0.156), 3, 0.25, 1.0),
+    (3, (-1.755, 0.03), 3, 0.25, 1.0),
+    (4, (0.0, 0.0), 3, 0.1, 0.2),
+    (4, (0.0, 0.0), 4, 0.1, 0.2),
+    (4, (0.0, 0.0), 5, 0.1, 0.2),
+]
+
+
+def _bounded(fx, x, y, n_iter, bits):
+    ft, (jx, jy), n, kr, ki = fx
+    from fractura_b200 import high_precision as hp
+    return hp.compute_highprec_escape_scalar(x, y, n_iter, ft, jx, jy, bits, n, kr, ki) >= n_iter
+
+
+def gen_config4():
+    """Config 4: 64 seeded tiles -- edge U{64..512}, formula uniform over the seven of
+    CONFIG4_FORMULAS, max_iter = floor(10^U(3,5)), width 10^U(-60,-12) -- centred on
+    boundary points: from a point that stays bounded, bisect along a seeded ray towards
+    a point 3 away (which escapes) until the bracket is below a quarter of the width,
+    the test being "stays bounded for min(max_iter, 2000) steps" at the tile's orbit
+    precision (the engine's native escape test).  Written into workloads.json."""
+    from fractura_b200.config import compute_required_prec_bits
+    rng = np.random.default_rng(SEED + 4)
+    path = os.path.join(HERE, "workloads.json")
+    wl = json.load(open(path))
+    tiles = []
+    t0 = time.time()
+    for q in range(64):
+        fx = CONFIG4_FORMULAS[int(rng.integers(0, len(CONFIG4_FORMULAS)))]
+        edge = int(rng.integers(64, 513))
+        aspect = float(rng.uniform(0.5, 1.0))
+        W, H = (edge, max(16, int(edge * aspect))) if rng.random() < 0.5 else (max(16, int(edge * aspect)), edge)
+        max_iter = int(10 ** rng.uniform(3, 5))
+        width = Decimal(repr(float(10 ** rng.uniform(-60, -12)))).normalize()
+        bits = compute_required_prec_bits(width)
+        n_test = min(max_iter, 2000)
+        inside = None
+        for cand in ((0.0, 0.0), (-0.5, 0.0), (-1.0, 0.0), (0.0, 0.3), (0.2, 0.2), (-0.1, -0.6)):
+            if _bounded(fx, Decimal(repr(cand[0])), Decimal(repr(cand[1])), n_test, bits):
+                inside = cand
+                break
+        while inside is None:
+            cand = (float(rng.uniform(-1.5, 1.5)), float(rng.uniform(-1.5, 1.5)))
+            if _bounded(fx, Decimal(repr(cand[0])), Decimal(repr(cand[1])), n_test, bits):
+                inside = cand
+        theta = float(rng.uniform(0.0, 2.0 * math.pi))
+        with __import__("decimal").localcontext() as ctx:
+            ctx.prec = int(-width.adjusted()) + 40
+            lo = (Decimal(repr(inside[0])), Decimal(repr(inside[1])))
+            hi = (lo[0] + Decimal(repr(3.0 * math.cos(theta))), lo[1] + Decimal(repr(3.0 * math.sin(theta))))
+            while max(abs(hi[0] - lo[0]), abs(hi[1] - lo[1])) > width / 4:
+                mid = ((lo[0] + hi[0]) / 2, (lo[1] + hi[1]) / 2)
+                if _bounded(fx, mid[0], mid[1], n_test, bits):
+                    lo = mid
+                else:
+                    hi = mid
+            cx, cy = (lo[0] + hi[0]) / 2, (lo[1] + hi[1]) / 2
+        ft, (jx, jy), n, kr, ki = fx
+        tiles.append(dict(cx=str(cx), cy=str(cy), width=str(width), W=W, H=H, max_iter=max_iter,
+                          fractal_type=ft, julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki))
+    wl["config4_tiles"] = tiles
+    wl["config4_seed"] = SEED + 4
+    with open(path, "w") as f:
+        json.dump(wl, f, indent=1)
+    px = sum(t["W"] * t["H"] for t in tiles)
+    print(f"  config 4: {len(tiles)} tiles, {px} pixels, {time.time() - t0:.0f}s")
+
+
 def render3_cases():
     wl = json.load(open(os.path.join(HERE, "workloads.json")))
     cx3, cy3 = wl["config3_centre"]
@@ -571,7 +645,7 @@ def gen_truth():
 
 
 SECTIONS = {"truth": gen_truth, "fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
-            "fexp": gen_fexp, "bbsa": gen_bbsa, "render_bbsa": gen_render_bbsa,
+            "fexp": gen_fexp, "bbsa": gen_bbsa, "render_bbsa": gen_render_bbsa, "config4": gen_config4,
             "render3": gen_render3}
 
 if __name__ == "__main__":

@@ -76,3 +76,25 @@ def test_invalid_arguments_rejected_without_gpu():
     assert L.ap_render_pass(C.byref(p), C.byref(b), None) == abi.AP_E_INVALID
     assert L.ap_edge_detect(None, None, 4, 4, 0.35, None) == abi.AP_E_INVALID
     assert L.ap_histogram_cdf(None, 4, 4, 10, 65536, None, None, None) == abi.AP_E_INVALID
+
+
+def test_batch_plan_checks_tiles_without_gpu():
+    """ap_batch_plan is host code: it numbers the patches and rejects tiles that are not
+    coarse perturbation passes on packed inputs."""
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("engine library not built")
+    import numpy as np
+    L = _lib.load()
+    arr = (abi.ApTileDesc * 2)()
+    for q, (w, h) in enumerate(((40, 20), (16, 16))):
+        arr[q].p = abi.new_params(width=w, height=h, max_iter=100, tier=abi.AP_TIER_PERTURB,
+                                  mode=abi.AP_MODE_COARSE, flags=abi.AP_FLAG_NO_RGB, ref_len=10)
+        arr[q].orbit_packed = C.c_void_p(64)
+        arr[q].iter_map = C.c_void_p(128)
+    first = np.zeros(3, np.int64)
+    assert L.ap_batch_plan(C.byref(arr), 2, 16, 16, first.ctypes.data_as(C.c_void_p)) == 0
+    assert list(first) == [0, 3 * 2, 3 * 2 + 1]
+    assert L.ap_batch_plan(C.byref(arr), 2, 16, 8, first.ctypes.data_as(C.c_void_p)) != 0  # 128 px
+    arr[1].p.tier = abi.AP_TIER_FP64
+    assert L.ap_batch_plan(C.byref(arr), 2, 16, 16, first.ctypes.data_as(C.c_void_p)) != 0
+    assert b"tile 1" in L.ap_last_error()
