@@ -85,7 +85,21 @@ def workload_cfg1():
                 form="FP64 direct iteration, histogram colouring")
 
 
-WORKLOADS = {"cfg3": workload_cfg3, "cfg1": workload_cfg1}
+def workload_cfg4():
+    tiles = _centres().get("config4_tiles")
+    if not tiles:
+        raise SystemExit("workloads.json holds no config4_tiles (python tests/golden/make_golden.py config4)")
+    return dict(name="batch64_mixed_formulas_perturb_w1e-60_1e-12", kind="batch", tiles=tiles,
+                arith="ref_cpu", bla_form="accurate", dtype="f64", W=0, H=0, factor=1,
+                max_iter=max(t["max_iter"] for t in tiles), width="1e-60..1e-12",
+                bbsa_order=32, glitch_mode="Off (Single-Ref)", precision_mode="1e-300 (Perturbation)",
+                scheme=0, fractal_type=-1,
+                form="one persistent work-stealing kernel over 64 tiles (FP64 deltas, dc-aware "
+                     "chained BLA, Pauldelbrot flags, one reference per tile), CUDA-graph replay, "
+                     "autotuned launch shape")
+
+
+WORKLOADS = {"cfg3": workload_cfg3, "cfg1": workload_cfg1, "cfg4": workload_cfg4}
 DEFAULT_WORKLOAD = "cfg3"
 
 
@@ -195,7 +209,28 @@ def nominal_iterations(kmap, max_iter):
     return float(k[k >= 0].astype(np.int64).sum() + np.int64(max_iter) * np.count_nonzero(k == -1))
 
 
+def batch_tiles(wl):
+    from fractura_b200 import batch as fb
+    return [fb.Tile(cx=Decimal(t["cx"]), cy=Decimal(t["cy"]), width=Decimal(t["width"]), W=t["W"], H=t["H"],
+                    max_iter=t["max_iter"], fractal_type=t["fractal_type"], julia_cx=t["julia_cx"],
+                    julia_cy=t["julia_cy"], gen_n=t["gen_n"], gen_kr=t["gen_kr"], gen_ki=t["gen_ki"],
+                    bla=True, strict_glitch=True) for t in wl["tiles"]]
+
+
 def config_of(wl, n_gpus):
+    if wl.get("kind") == "batch":
+        tiles = wl["tiles"]
+        kinds = {}
+        for t in tiles:
+            key = {0: "mandelbrot", 1: "burning_ship", 2: "julia", 3: "ship_julia"}.get(
+                t["fractal_type"], f"multibrot{t['gen_n']}")
+            kinds[key] = kinds.get(key, 0) + 1
+        return {"workload": wl["name"], "tiles": len(tiles), "pixels": sum(t["W"] * t["H"] for t in tiles),
+                "formulas": kinds, "max_iter_range": [min(t["max_iter"] for t in tiles),
+                                                      max(t["max_iter"] for t in tiles)],
+                "width_range": wl["width"], "arith": wl["arith"], "bla_form": wl["bla_form"],
+                "form": wl["form"], "l2": "flushed between timed steps (512 MiB write)",
+                "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single"}
     return {"workload": wl["name"], "width": wl["W"], "height": wl["H"], "max_iter": wl["max_iter"],
             "view_width": wl["width"], "ssaa": wl["factor"], "bla": wl["bbsa_order"] == 32,
             "glitch_mode": wl["glitch_mode"], "max_rebase_passes": 4, "arith": wl["arith"],
@@ -215,9 +250,89 @@ def max_over_ranks(x, world):
 
 
 # ----------------------------------------------------------- CPU baseline
-def oracle_baseline(wl, budget_s=12.0):
+def oracle_batch_baseline(wl, budget_s=12.0, start=0):
+    """The reference's CPU path, tile by tile (oracle C port, all host cores, chained BLA
+    with the reference's table, one reference per tile), on the first tiles of the
+    batch until budget_s of CPU time is spent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle
+    from helpers import oracle_pert_frame
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    iters, spent, n = 0.0, 0.0, 0
+    order = wl["tiles"][start % len(wl["tiles"]):] + wl["tiles"][:start % len(wl["tiles"])]
+    for t in order:
+        m = dict(W=t["W"], H=t["H"], factor=1, max_iter=t["max_iter"], cx=t["cx"], cy=t["cy"],
+                 width=t["width"], scheme=0, fractal_type=t["fractal_type"], julia_cx=t["julia_cx"],
+                 julia_cy=t["julia_cy"], gen_n=t["gen_n"], gen_kr=t["gen_kr"], gen_ki=t["gen_ki"],
+                 bbsa_order=32 if t["fractal_type"] in (0, 2, 4) else 0, glitch_mode="Off (Single-Ref)")
+        t0 = time.perf_counter()
+        fr, _ = oracle_pert_frame(m)
+        spent += time.perf_counter() - t0
+        iters += nominal_iterations(fr.kmap, t["max_iter"])
+        n += 1
+        if spent > budget_s:
+            break
+    return iters / spent / 1e9, cores, (f"{n} of {len(wl['tiles'])} tiles from tile {start % len(wl['tiles'])}, "
+                                        f"one pass each incl. host orbits, C port of the reference's "
+                                        f"CPU kernels")
+
+
+def oracle_pert_rows(wl, budget_s, start=0):
+    """Rows of a perturbation frame through the oracle (all host cores): the primary
+    reference orbit, the reference's BLA table, Pauldelbrot flags, rows start,
+    start + 17, ... until budget_s is spent.  Returns (G iter/s, cores, sample)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from fractura_b200 import abi
+    from fractura_b200 import high_precision as hp
+    from fractura_b200.config import decimal_context
+    from decimal import localcontext
+    cores = os.cpu_count() or 1
+    oracle.set_threads(cores)
+    W, H, mi = wl["W"], wl["H"], wl["max_iter"]
+    pw = Decimal(wl["width"])
+    with localcontext(decimal_context(pw)):
+        ph = pw * (Decimal(H) / Decimal(W))
+        dx = float(pw / Decimal(W - 1))
+        dy = float(ph / Decimal(H - 1))
+    t0 = time.perf_counter()
+    bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
+        Decimal(wl["cx"]), Decimal(wl["cy"]), pw, ph, mi, W, H)
+    T = oracle.build_bla(re, im, rl, 0, 1e-6, 16, 3, 0.25, 1.0) if wl["bbsa_order"] == 32 else None
+    p = abi.new_params(width=W, height=H, max_iter=mi, tier=abi.AP_TIER_PERTURB,
+                       arith=abi.AP_ARITH_REF_CPU, dx_hi=dx, dy_hi=dy, ref_px=(W - 1) * float(bu),
+                       ref_py=(H - 1) * float(bv), ref_cx=float(bcx), ref_cy=float(bcy), ref_len=rl,
+                       bla_levels=16 if T is not None else 0, strict_glitch=1,
+                       flags=abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD)
+    xs = np.arange(W, dtype=np.float64)
+    iters, rows = 0.0, 0
+    j = start % 17
+    while True:
+        _, _, k = oracle.pert_grid(p, re[:rl + 1], im[:rl + 1], T, xs, np.array([float(j)]))
+        iters += nominal_iterations(k, mi)
+        rows += 1
+        j += 17
+        if j >= H:
+            j = (j + 1) % 17
+        if time.perf_counter() - t0 > budget_s:
+            break
+    spent = time.perf_counter() - t0
+    return iters / spent / 1e9, cores, (f"{rows} rows of the {W}x{H} frame incl. the host orbit "
+                                        f"and BLA table, one reference, C port of the reference's "
+                                        f"CPU kernels")
+
+
+def oracle_baseline(wl, budget_s=12.0, sampled=False, start=0):
     """The reference's per-pixel path restated in C (oracle/) on all host cores, on a
-    bounded sample of the workload: every n-th row of the frame, chained BLA, one pass."""
+    bounded sample of the workload: the whole frame (direct tiers; perturbation frames
+    with their rebase passes unless sampled), rows of it (sampled perturbation frames)
+    or whole tiles (batches) until budget_s is spent."""
+    if wl.get("kind") == "batch":
+        return oracle_batch_baseline(wl, budget_s, start=start)
+    if sampled and not wl["precision_mode"].startswith("1e-12"):
+        return oracle_pert_rows(wl, budget_s, start=start)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     from fractura_b200 import abi
@@ -260,8 +375,10 @@ def cpu_reference_arm(args, wl, rank, world):
         return
     vals = []
     sample = cores = None
-    for _ in range(max(1, args.steps)):
-        v, cores, sample = oracle_baseline(wl)
+    # each step a bounded sample, so that the whole run stays within a few minutes
+    budget = min(12.0, max(0.3, 150.0 / max(1, args.steps + args.warmup)))
+    for q in range(max(1, args.steps)):
+        v, cores, sample = oracle_baseline(wl, budget_s=budget, sampled=True, start=q)
         vals.append(v)
     value = float(np.median(vals))
     line = {"metric": "G iter/s", "value": value, "unit": "G iter/s", "n_gpus": args.gpus,
@@ -392,6 +509,92 @@ def summarise_form(form, ms, plain=None, wl=None):
         out["k_identical_vs_plain"] = float(np.mean(form.kmap == plain.kmap))
         out["smooth_diff_vs_plain_p99.9"] = float(np.percentile(np.abs(form.s64 - plain.s64), 99.9))
     return out
+
+
+def batch_arm(args, wl, rank, world, local_rank):
+    """Config 4: every rank renders the whole 64-tile batch (weak scaling)."""
+    import torch
+    from fractura_b200 import _lib
+    from fractura_b200 import batch as fb
+    from fractura_b200 import dist
+    from fractura_b200 import high_precision as hp
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    L = _lib.load()
+    tiles = batch_tiles(wl)
+    hp.clear_reference_orbit_cache()
+    b = fb.prepare_batch(tiles, arith=wl["arith"], bla_form=wl["bla_form"], stream=stream)
+    cfg = fb.tune(b)
+    g = b.capture(cfg)
+    for _ in range(args.warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    iters = b.nominal_iterations()
+
+    barrier(world)
+    c0 = L.ap_launch_counter()
+    step_ms = []
+    with ClockSampler(local_rank) as clocks:
+        time.sleep(0.5)
+        torch.cuda.synchronize()
+        clocks.mark(True)
+        torch.cuda.nvtx.range_push("timed_region")
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            with torch.cuda.stream(stream):
+                g.replay()
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+        torch.cuda.nvtx.range_pop()
+        torch.cuda.synchronize()
+        clocks.mark(False)
+    # a graph replay launches the batch kernel once; the library's counter does not see it
+    launches = (L.ap_launch_counter() - c0) + args.steps
+    barrier(world)
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
+    value = dist.whole_job_rate(iters, args.steps, world, total_ms) / 1e9
+
+    # end to end: orbits (host), tables and records (device), the persistent launch and
+    # the download of every tile's smooth map, per step
+    e2e_steps = max(2, args.steps // 20)
+    barrier(world)
+    t0 = time.perf_counter()
+    h2d = d2h = 0
+    for _ in range(e2e_steps):
+        hp.clear_reference_orbit_cache()
+        bb = fb.prepare_batch(tiles, arith=wl["arith"], bla_form=wl["bla_form"], stream=stream)
+        bb.render(cfg)
+        maps = [o["iter"].cpu() for o in bb.tiles_out]
+        d2h = sum(m.numel() * 4 for m in maps)
+        h2d = sum(16 * (p.ref_len + 1) for p in bb.params) + len(bb.desc_dev)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    barrier(world)
+    e2e = iters * e2e_steps * world / e2e_s / 1e9
+    if rank != 0:
+        return
+    cpu_value, cores, cpu_sample = oracle_baseline(wl)
+    line = {
+        "metric": "G iter/s", "value": value, "unit": "G iter/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl["dtype"],
+        "data": "synthetic", "impl": "ours", "config": config_of(wl, world),
+        "nominal_iterations_per_batch": iters,
+        "e2e": {"value": e2e, "unit": "G iter/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+        "autotuner": {"chosen": vars(cfg) if hasattr(cfg, "__dict__") else cfg.__repr__(),
+                      "candidates_ms": [[round(ms, 4), repr(c)] for ms, c in fb.tuned_timings(b)]},
+        "clocks": clocks.summary(),
+        "gpu_launches": int(launches),
+        "cpu_baseline": {"value": cpu_value, "unit": "G iter/s", "cores": cores, "kind": "port",
+                         "sample": cpu_sample},
+    }
+    print(json.dumps(line), flush=True)
 
 
 def our_arm(args, wl, rank, world, local_rank):
@@ -527,7 +730,10 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     try:
-        our_arm(args, wl, rank, world, local_rank)
+        if wl.get("kind") == "batch":
+            batch_arm(args, wl, rank, world, local_rank)
+        else:
+            our_arm(args, wl, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
