@@ -484,51 +484,57 @@ CONFIG4_FORMULAS = [
 ]
 
 
-def _bounded(fx, x, y, n_iter, bits):
+def _escape_count(fx, x, y, n_iter, bits):
     ft, (jx, jy), n, kr, ki = fx
     from fractura_b200 import high_precision as hp
-    return hp.compute_highprec_escape_scalar(x, y, n_iter, ft, jx, jy, bits, n, kr, ki) >= n_iter
+    return int(hp.compute_highprec_escape_scalar(x, y, n_iter, ft, jx, jy, bits, n, kr, ki))
 
 
 def gen_config4():
-    """Config 4: 64 seeded tiles -- edge U{64..512}, formula uniform over the seven of
+    """Config 4: 64 seeded square tiles -- edge U{64..512}, formula uniform over the seven of
     CONFIG4_FORMULAS, max_iter = floor(10^U(3,5)), width 10^U(-60,-12) -- centred on
-    boundary points: from a point that stays bounded, bisect along a seeded ray towards
-    a point 3 away (which escapes) until the bracket is below a quarter of the width,
-    the test being "stays bounded for min(max_iter, 2000) steps" at the tile's orbit
-    precision (the engine's native escape test).  Written into workloads.json."""
+    boundary points.  Per tile: the point of a 48 x 48 grid over [-2, 2]^2 with the most
+    escape steps (at most N = min(max_iter, 2000)) is the inner end, a point 3 away
+    along a seeded ray the outer end, and the bracket is bisected on "at least as many
+    escape steps as the inner end" (the set's boundary when the inner end stays bounded
+    for N steps, else a level curve of the escape time) until it is below a quarter of
+    the width, with the engine's native escape test at the tile's orbit precision.
+    Written into workloads.json."""
     from fractura_b200.config import compute_required_prec_bits
     rng = np.random.default_rng(SEED + 4)
     path = os.path.join(HERE, "workloads.json")
     wl = json.load(open(path))
     tiles = []
     t0 = time.time()
+    grid = [Decimal(repr(-2.0 + 4.0 * q / 47.0)) for q in range(48)]
+    inner_cache = {}
     for q in range(64):
-        fx = CONFIG4_FORMULAS[int(rng.integers(0, len(CONFIG4_FORMULAS)))]
+        fi = int(rng.integers(0, len(CONFIG4_FORMULAS)))
+        fx = CONFIG4_FORMULAS[fi]
         edge = int(rng.integers(64, 513))
-        aspect = float(rng.uniform(0.5, 1.0))
-        W, H = (edge, max(16, int(edge * aspect))) if rng.random() < 0.5 else (max(16, int(edge * aspect)), edge)
+        W = H = edge
         max_iter = int(10 ** rng.uniform(3, 5))
         width = Decimal(repr(float(10 ** rng.uniform(-60, -12)))).normalize()
+        theta = float(rng.uniform(0.0, 2.0 * math.pi))
         bits = compute_required_prec_bits(width)
         n_test = min(max_iter, 2000)
-        inside = None
-        for cand in ((0.0, 0.0), (-0.5, 0.0), (-1.0, 0.0), (0.0, 0.3), (0.2, 0.2), (-0.1, -0.6)):
-            if _bounded(fx, Decimal(repr(cand[0])), Decimal(repr(cand[1])), n_test, bits):
-                inside = cand
-                break
-        while inside is None:
-            cand = (float(rng.uniform(-1.5, 1.5)), float(rng.uniform(-1.5, 1.5)))
-            if _bounded(fx, Decimal(repr(cand[0])), Decimal(repr(cand[1])), n_test, bits):
-                inside = cand
-        theta = float(rng.uniform(0.0, 2.0 * math.pi))
+        key = (fi, n_test)
+        if key not in inner_cache:
+            best = (-1, None)
+            for y in grid:
+                for x in grid:
+                    e = _escape_count(fx, x, y, n_test, 128)
+                    if e > best[0]:
+                        best = (e, (x, y))
+            inner_cache[key] = best
+        level, inner = inner_cache[key]
         with __import__("decimal").localcontext() as ctx:
             ctx.prec = int(-width.adjusted()) + 40
-            lo = (Decimal(repr(inside[0])), Decimal(repr(inside[1])))
+            lo = inner
             hi = (lo[0] + Decimal(repr(3.0 * math.cos(theta))), lo[1] + Decimal(repr(3.0 * math.sin(theta))))
             while max(abs(hi[0] - lo[0]), abs(hi[1] - lo[1])) > width / 4:
                 mid = ((lo[0] + hi[0]) / 2, (lo[1] + hi[1]) / 2)
-                if _bounded(fx, mid[0], mid[1], n_test, bits):
+                if _escape_count(fx, mid[0], mid[1], n_test, bits) >= level:
                     lo = mid
                 else:
                     hi = mid
@@ -536,6 +542,8 @@ def gen_config4():
         ft, (jx, jy), n, kr, ki = fx
         tiles.append(dict(cx=str(cx), cy=str(cy), width=str(width), W=W, H=H, max_iter=max_iter,
                           fractal_type=ft, julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki))
+        print(f"  tile {q}: type {ft} n {n} {W}x{H} max_iter {max_iter} width {width} "
+              f"(inner level {level}) {time.time() - t0:.0f}s", flush=True)
     wl["config4_tiles"] = tiles
     wl["config4_seed"] = SEED + 4
     with open(path, "w") as f:
