@@ -82,6 +82,15 @@ class ApTileDesc(C.Structure):
     ]
 
 
+class ApGradView(C.Structure):
+    _fields_ = [
+        ("width", C.c_int32), ("height", C.c_int32), ("max_iter", C.c_int32),
+        ("fractal_type", C.c_int32), ("gen_n", C.c_int32), ("ckpt_every", C.c_int32),
+        ("cx", C.c_double), ("cy", C.c_double), ("w", C.c_double), ("pr", C.c_double),
+        ("pi", C.c_double),
+    ]
+
+
 def new_params(**kw):
     """ApFrameParams with neutral defaults (factor 1, density/contrast 1)."""
     p = ApFrameParams()

@@ -134,7 +134,6 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
             pixel_setup(v, i, j, z0, c, dpx_dw, dpy_dw, skip);
             double2 seg[kMaxSegment];
             const int C = v.ckpt_every;
-            // z_K itself: recompute from the checkpoint of its segment
             C2d G = {0.0, 0.0};  // dL/dz_{k+1} during the sweep
             C2d gc = {0.0, 0.0}, gp = {0.0, 0.0};
             bool first = true;
@@ -143,14 +142,12 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
                 const int k1 = min(K, k0 + C);  // this segment's steps z_k -> z_{k+1}, k in [k0, k1)
                 const double2 st = ckpt[idx * n_ck + sg];
                 C2d z = {st.x, st.y}, d;
-                for (int k = k0; k <= k1; ++k) {
+                for (int k = k0; k < k1; ++k) {  // inputs z_k0 .. z_(k1-1): at most C values
                     seg[k - k0] = make_double2(z.r, z.i);
-                    if (k < k1 || (first && k < K)) step_f(v, z, c, z, d);
+                    step_f(v, z, c, z, d);
                 }
-                if (first) {
-                    // z_K is the last recomputed value of the last segment
-                    const double2 zk = seg[K - k0];
-                    const C2d dz = ds_dzK(v, {zk.x, zk.y});
+                if (first) {  // the last segment ends at k1 = K: z is z_K
+                    const C2d dz = ds_dzK(v, z);
                     G = {gs * dz.r, gs * dz.i};
                     first = false;
                 }

@@ -131,6 +131,16 @@ typedef struct ApTileDesc {
     int64_t reserved;
 } ApTileDesc;
 
+/* A view for the derivative entry points (FP64 direct iteration; formulas 0 Mandelbrot,
+ * 2 Julia with z0 = pixel and parameter P = (pr, pi), 4 Multibrot z^n + P z + pixel).
+ * Pixel (i, j) sits at (cx - w/2 + i w/(W-1), cy + h/2 - j h/(H-1)), h = w H / W.
+ * 64 bytes. */
+typedef struct ApGradView {
+    int32_t width, height, max_iter, fractal_type, gen_n;
+    int32_t ckpt_every;        /* checkpoint spacing of the orbit, 1..1024 steps */
+    double cx, cy, w, pr, pi;
+} ApGradView;
+
 /* Library identity. */
 AP_API int ap_abi_version(void);
 AP_API const char* ap_last_error(void);
@@ -275,6 +285,24 @@ AP_API int ap_batch_plan(const ApTileDesc* host_tiles, int32_t n, int32_t patch_
 AP_API int ap_render_batch(const ApTileDesc* tiles, const int64_t* first_patch, int32_t n,
                            int32_t arith, int32_t patch_w, int32_t patch_h, int32_t blocks_per_sm,
                            int32_t min_blocks, unsigned long long* queue_head, void* stream);
+
+/* Derivatives of the smooth escape value (no counterpart in the reference).
+ * theta = (cx, cy, ln w, Re P, Im P).
+ * ap_smooth_forward: s64[H, W] float64 smooth values (-1 interior), kmap[H, W] escape
+ *   steps (-1 bounded, -2 cardioid/bulb), and, when ckpt is given, the orbit at every
+ *   ckpt_every-th step: ckpt[H, W, n_ck] complex float64, n_ck >= ceil(max_iter/ckpt_every)+1.
+ * ap_smooth_adjoint: for grad_s[H, W] = dL/ds, dL/dtheta summed per block of pixels into
+ *   block_sums[ap_smooth_adjoint_blocks(W, H), 5] (the caller sums the rows); the orbit
+ *   is recomputed segment by segment from ckpt, never stored; pix_grads[H, W, 5]
+ *   (optional) receives each pixel's term.
+ * ap_smooth_tangent: forward mode, ds[H, W, 5] = ds/dtheta per pixel. */
+AP_API int ap_smooth_forward(const ApGradView* v, double* s64, int32_t* kmap, double* ckpt,
+                             int32_t n_ck, void* stream);
+AP_API int32_t ap_smooth_adjoint_blocks(int32_t width, int32_t height);
+AP_API int ap_smooth_adjoint(const ApGradView* v, const double* grad_s, const int32_t* kmap,
+                             const double* ckpt, int32_t n_ck, double* pix_grads, double* block_sums,
+                             void* stream);
+AP_API int ap_smooth_tangent(const ApGradView* v, double* ds, void* stream);
 
 /* Measurement helper (no counterpart in the reference): number of kernels this
  * library has launched in the process so far. */
