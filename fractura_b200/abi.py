@@ -91,6 +91,19 @@ class ApGradView(C.Structure):
     ]
 
 
+AP_STRICT_DD = 1
+AP_STRICT_LIMBS = 2
+AP_STRICT_NLIMBS = 34
+
+
+class ApStrictView(C.Structure):
+    _fields_ = [
+        ("tier", C.c_int32), ("jx_sign", C.c_int32), ("jy_sign", C.c_int32),
+        ("reserved", C.c_int32),
+        ("jx_limbs", C.c_uint32 * AP_STRICT_NLIMBS), ("jy_limbs", C.c_uint32 * AP_STRICT_NLIMBS),
+    ]
+
+
 def new_params(**kw):
     """ApFrameParams with neutral defaults (factor 1, density/contrast 1)."""
     p = ApFrameParams()

@@ -109,6 +109,28 @@ __global__ void __launch_bounds__(256) colour_kernel(const ApFrameParams p, cons
     store_rgb(b.rgb, p.is_hdr, idx, r, g, bb);
 }
 
+// ---------------------------------------------------------- listed pixels
+// Values computed elsewhere for a list of pixels (the Strict Metric
+// re-evaluation, math_core/engine.py:191-267): iter_map = float32(value), the
+// colour of the float64 value (black for value < 0 or >= max_iter), glitch
+// flag cleared.
+__global__ void __launch_bounds__(256) set_pixels_kernel(const ApFrameParams p, const ApFrameBuffers b,
+                                                         const int32_t* __restrict__ coords,
+                                                         const double* __restrict__ values, int n,
+                                                         int hist) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int r = coords[2 * q], c = coords[2 * q + 1];
+    if (r < 0 || r >= p.height || c < 0 || c >= p.width) return;
+    const size_t idx = (size_t)r * p.width + c;
+    const double s = values[q];
+    b.iter_map[idx] = (float)s;
+    double cr = 0.0, cg = 0.0, cb = 0.0;
+    if (s >= 0.0 && s < (double)p.max_iter) colour_of(p, b.lut, b.cdf, hist != 0, s, cr, cg, cb);
+    store_rgb(b.rgb, p.is_hdr, idx, cr, cg, cb);
+    if (b.glitch_out) b.glitch_out[idx] = 0;
+}
+
 // ----------------------------------------------------------- rebase bins
 // Glitched pixels per cell of the 16 x 16 grid the rebase loop picks its next
 // reference from (math_core/engine.py:1923-1935: row bin (16 j) / H, column bin
@@ -201,4 +223,18 @@ extern "C" int ap_glitch_bins(const uint8_t* glitch_map, int32_t width, int32_t 
     dim3 grid((width + 255) / 256, (height + 15) / 16);
     ap::glitch_bins_kernel<<<grid, 256, 0, st>>>(glitch_map, width, height, counts);
     return ap::check_launch("glitch_bins_kernel");
+}
+
+extern "C" int ap_set_pixels(const ApFrameParams* p, const ApFrameBuffers* b, const int32_t* coords,
+                             const double* values, int32_t n, void* stream) {
+    if (!p || !b || !b->iter_map || !b->rgb || !b->lut || n < 0 || (n > 0 && (!coords || !values)) ||
+        p->width <= 0 || p->height <= 0) {
+        ap::set_error("ap_set_pixels: bad arguments");
+        return AP_E_INVALID;
+    }
+    if (n == 0) return AP_OK;
+    const int hist = (p->scheme_id == 11 && b->cdf != nullptr) ? 1 : 0;
+    ap::set_pixels_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        *p, *b, coords, values, n, hist);
+    return ap::check_launch("set_pixels_kernel");
 }

@@ -23,7 +23,7 @@ BLA_LEVELS = 16
 MAX_REBASE_PASSES = 4
 
 # Host<->device traffic of the last perturbation frame (bytes), for benchmarking.
-LAST_FRAME_STATS = {"h2d_bytes": 0, "d2h_bytes": 0, "rebase_passes": 0}
+LAST_FRAME_STATS = {"h2d_bytes": 0, "d2h_bytes": 0, "rebase_passes": 0, "strict_pixels": 0, "strict_tier": 0}
 
 
 def _ptr(t):
@@ -302,7 +302,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
                     int(fe_e))
     strict = 1 if ("Auto Rebasing" in glitch_mode or "Strict" in glitch_mode
                    or "Pauldelbrot" in glitch_mode) else 0
-    LAST_FRAME_STATS.update(h2d_bytes=0, d2h_bytes=0, rebase_passes=0)
+    LAST_FRAME_STATS.update(h2d_bytes=0, d2h_bytes=0, rebase_passes=0, strict_pixels=0, strict_tier=0)
 
     bcx, bcy, bu, bv, re, im, ref_len = hp.find_optimal_reference_orbit(
         center_x_dec, center_y_dec, plot_width_dec, plot_height_dec, max_iter, W, H,
@@ -480,9 +480,141 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
             _lib.launch(L.ap_render_pass, C.byref(q), C.byref(b), stream_h, what="ap_render_pass")
     if exhaustive:
         st.synchronize()
-        if int(torch.count_nonzero(fr.glitch_out)) > 0:
-            raise NotImplementedError("Strict Metric exhaustive re-evaluation is not served yet")
+        g_all = fr.glitch_out.cpu().numpy()
+        LAST_FRAME_STATS["d2h_bytes"] += g_all.nbytes
+        coords = np.argwhere(g_all > 0)
+        if len(coords):
+            dev = fr.iter.device
+
+            def upload(a):
+                t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+                LAST_FRAME_STATS["h2d_bytes"] += t.numel() * t.element_size()
+                return t
+
+            d_coords = upload(coords.astype(np.int32))
+            b = _buffers(fr, lut, cdf=cdf if scheme == 11 else None)
+            tier = None if cpu_sem else strict_device_tier(plot_width_dec, fractal_type)
+            LAST_FRAME_STATS.update(strict_pixels=int(len(coords)), strict_tier=int(tier or 0))
+            if tier is None:
+                # host evaluation (the CPU path, and the CUDA path beyond its device
+                # tiers), coloured with the CPU transfer functions
+                values = strict_values(coords, W, H, max_iter, center_x_dec, center_y_dec, plot_width_dec,
+                                       plot_height_dec, fractal_type, julia_cx, julia_cy, gen_n, gen_kr,
+                                       gen_ki)
+                d_vals = upload(values)
+                q = _copy_params(p)
+                q.arith = abi.AP_ARITH_REF_CPU
+                _lib.launch(L.ap_set_pixels, C.byref(q), C.byref(b), _ptr(d_coords), _ptr(d_vals),
+                            int(len(coords)), stream_h, what="ap_set_pixels")
+            else:
+                q, view, signs, limbs = strict_device_inputs(p, coords, tier, W, H, center_x_dec, center_y_dec,
+                                                             plot_width_dec, plot_height_dec, julia_cx,
+                                                             julia_cy)
+                d_signs = upload(signs) if signs is not None else None
+                d_limbs = upload(limbs.view(np.int32)) if limbs is not None else None
+                _lib.launch(L.ap_strict_eval, C.byref(q), C.byref(b), C.byref(view), _ptr(d_coords),
+                            _ptr(d_signs), _ptr(d_limbs), int(len(coords)), stream_h, what="ap_strict_eval")
+            st.synchronize()
     return dict(ref_len=ref_len, passes=state.passes)
+
+
+def strict_device_tier(plot_width_dec, fractal_type):
+    """Device tier of the CUDA path's Strict Metric fallback (math_core/engine.py:285-296,
+    :330): double-double down to 1e-30, 34-limb fixed point down to 1e-315 except for
+    Multibrot, None where the reference evaluates on the host."""
+    if plot_width_dec >= Decimal("1e-30"):
+        return abi.AP_STRICT_DD
+    if plot_width_dec >= Decimal("1e-315") and fractal_type != 4:
+        return abi.AP_STRICT_LIMBS
+    return None
+
+
+def fixed_limbs(d):
+    """(sign, 34 uint32 limbs) of a Decimal: limb 0 the integer part, then 33 fraction
+    limbs of floor(|d| 2^1056), most significant first (decimal_to_limbs,
+    math_core/cuda_kernels.py:2242-2274, whose Decimal steps run at 500+ digits and so
+    reproduce the exact floor)."""
+    sign = 1 if d < 0 else 0
+    t = d.copy_abs().as_tuple()  # exact: abs() would round to the context
+    coeff = int("".join(map(str, t.digits))) if t.digits else 0
+    frac_bits = 32 * (abi.AP_STRICT_NLIMBS - 1)
+    if t.exponent >= 0:
+        f = (coeff * 10 ** t.exponent) << frac_bits
+    else:
+        f = (coeff << frac_bits) // (10 ** (-t.exponent))
+    f &= (1 << (32 * abi.AP_STRICT_NLIMBS)) - 1
+    return sign, np.frombuffer(f.to_bytes(4 * abi.AP_STRICT_NLIMBS, "big"), dtype=">u4").astype(np.uint32)
+
+
+def strict_device_inputs(p, coords, tier, W, H, center_x_dec, center_y_dec, plot_width_dec, plot_height_dec,
+                         julia_cx, julia_cy):
+    """Parameters of ap_strict_eval as eval_glitched_pixels_fallback_cuda prepares them
+    (math_core/engine.py:298-375): x_min, y_max and the pixel steps W-1, H-1 apart in
+    Decimal at the view's precision; double-double views of them, or every pixel's c in
+    fixed point."""
+    from .engine import to_dd
+    ctx = decimal_context(plot_width_dec)
+    view = abi.ApStrictView()
+    view.tier = tier
+    q = _copy_params(p)
+    q.arith = abi.AP_ARITH_REF_CUDA
+    with localcontext(ctx):
+        x_min = center_x_dec - (plot_width_dec / Decimal(2))
+        y_max = center_y_dec + (plot_height_dec / Decimal(2))
+        dx = plot_width_dec / Decimal(max(1, W - 1))
+        dy = plot_height_dec / Decimal(max(1, H - 1))
+        if tier == abi.AP_STRICT_DD:
+            q.x_min_hi, q.x_min_lo = to_dd(x_min, ctx)
+            q.y_max_hi, q.y_max_lo = to_dd(y_max, ctx)
+            q.dx_hi, q.dx_lo = to_dd(dx, ctx)
+            q.dy_hi, q.dy_lo = to_dd(dy, ctx)
+            q.julia_cx_hi, q.julia_cx_lo = to_dd(julia_cx, ctx)
+            q.julia_cy_hi, q.julia_cy_lo = to_dd(julia_cy, ctx)
+            return q, view, None, None
+        n = len(coords)
+        signs = np.empty((n, 2), np.int32)
+        limbs = np.empty((n, 2, abi.AP_STRICT_NLIMBS), np.uint32)
+        for t in range(n):
+            signs[t, 0], limbs[t, 0] = fixed_limbs(x_min + Decimal(int(coords[t, 1])) * dx)
+            signs[t, 1], limbs[t, 1] = fixed_limbs(y_max - Decimal(int(coords[t, 0])) * dy)
+        view.jx_sign, jx = fixed_limbs(Decimal(str(julia_cx)))
+        view.jy_sign, jy = fixed_limbs(Decimal(str(julia_cy)))
+        view.jx_limbs[:] = [int(x) for x in jx]
+        view.jy_limbs[:] = [int(x) for x in jy]
+    return q, view, signs, limbs
+
+
+def strict_values(coords, W, H, max_iter, center_x_dec, center_y_dec, plot_width_dec, plot_height_dec,
+                  fractal_type, julia_cx, julia_cy, gen_n, gen_kr, gen_ki, workers=None, scalar=None):
+    """Smooth values of the listed (row, col) pixels, each from its own orbit at the
+    view's precision: the Strict Metric re-evaluation of math_core/engine.py:191-267
+    (its Decimal branch; gmpy2 is not used).  Pixel c is x_min + col dx, y_max - row dy
+    in Decimal at int(bits / 3.32) + 30 digits.  ``scalar`` replaces the certified
+    native escape evaluation (the exact Decimal one, for instance)."""
+    scalar = scalar or hp.compute_highprec_escape_scalar
+    from concurrent.futures import ThreadPoolExecutor
+    import os
+    ctx = decimal_context(plot_width_dec)
+    bits = compute_required_prec_bits(plot_width_dec)
+    with localcontext(ctx):
+        x_min = center_x_dec - (plot_width_dec / Decimal(2))
+        y_max = center_y_dec + (plot_height_dec / Decimal(2))
+        dx = plot_width_dec * (Decimal(1) / Decimal(max(1, W - 1)))
+        dy = plot_height_dec * (Decimal(1) / Decimal(max(1, H - 1)))
+    px_ctx = decimal_context()
+    px_ctx.prec = int(bits / 3.32) + 30
+
+    def one(rc):
+        r, c = int(rc[0]), int(rc[1])
+        with localcontext(px_ctx):
+            cx = x_min + Decimal(c) * dx
+            cy = y_max - Decimal(r) * dy
+        return scalar(cx, cy, max_iter, fractal_type, julia_cx, julia_cy, bits,
+                      gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki)
+
+    n = workers or min(32, os.cpu_count() or 4)
+    with ThreadPoolExecutor(max_workers=n) as ex:
+        return np.fromiter(ex.map(one, list(coords)), dtype=np.float64, count=len(coords))
 
 
 def _copy_params(p):

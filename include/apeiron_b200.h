@@ -216,6 +216,42 @@ AP_API int ap_histogram_cdf_noalloc(const float* iter_map, int32_t width, int32_
  * rebase pass re-rendered). */
 AP_API int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stream);
 
+/* Write values computed elsewhere into the listed pixels: coords[n, 2] = (row, col),
+ * values[n] float64 smooth values; iter_map = float32(value), RGB = the colour of the
+ * float64 value (black below 0 or at or above max_iter; CDF colouring for scheme 11
+ * when b->cdf is set), glitch flag cleared.  The Strict Metric re-evaluation's output
+ * step (math_core/engine.py:249-266). */
+AP_API int ap_set_pixels(const ApFrameParams* p, const ApFrameBuffers* b, const int32_t* coords,
+                         const double* values, int32_t n, void* stream);
+
+/* Strict Metric re-evaluation on the device (eval_glitched_pixels_cuda_kernel and
+ * eval_glitched_pixels_hist_cuda_kernel, math_core/cuda_kernels.py:2450-2569; host side
+ * math_core/engine.py:270-410).  Each listed pixel (coords[n, 2] = (row, col)) is
+ * iterated on its own, then written like ap_set_pixels (iter_map = the float32 value,
+ * RGB black for a value below 0, glitch flag cleared).
+ *   AP_STRICT_DD: double-double; pixel c = x_min + col dx, y_max - row dy with the
+ *     double-double view of p (x_min_hi/lo, y_max_hi/lo, dx_hi/lo, dy_hi/lo) and the
+ *     Julia constant in p->julia_c{x,y}_{hi,lo}; fractal types 0-4.
+ *   AP_STRICT_LIMBS: AP_STRICT_NLIMBS x 32-bit sign-magnitude fixed point (limb 0 the
+ *     integer part, most significant first); signs[n, 2] (1 = negative) and
+ *     limbs[n, 2, AP_STRICT_NLIMBS] give each pixel's c (x then y), v the Julia
+ *     constant; fractal types 0-3 (type 4 evaluates as interior, as the reference).
+ * Colours use p->arith's transfer functions and, for scheme 11, b->cdf. */
+#define AP_STRICT_DD 1
+#define AP_STRICT_LIMBS 2
+#define AP_STRICT_NLIMBS 34
+typedef struct ApStrictView {
+    int32_t tier;
+    int32_t jx_sign, jy_sign;
+    int32_t reserved;
+    uint32_t jx_limbs[AP_STRICT_NLIMBS];
+    uint32_t jy_limbs[AP_STRICT_NLIMBS];
+} ApStrictView;
+
+AP_API int ap_strict_eval(const ApFrameParams* p, const ApFrameBuffers* b, const ApStrictView* v,
+                          const int32_t* coords, const int32_t* signs, const uint32_t* limbs,
+                          int32_t n, void* stream);
+
 /* Rebase-loop statistics on the device: counts[256] (int32, zeroed here) receives the
  * number of glitched pixels in each cell of the 16 x 16 grid (row cell 16 j / H, column
  * cell 16 i / W) from which math_core/engine.py:1923-1992 picks the next reference, so

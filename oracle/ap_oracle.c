@@ -1246,6 +1246,170 @@ APO_EXPORT int apo_colour(const ApFrameParams* p, const ApFrameBuffers* b) {
     return AP_OK;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Strict Metric fallback on the device: 34 x 32-bit fixed point              */
+/* (compute_ml_sample and ml_*, math_core/cuda_kernels.py:2239-2446).         */
+/* ------------------------------------------------------------------------- */
+#define ML_N AP_STRICT_NLIMBS
+
+static void ml_add_mag(const uint32_t* a, const uint32_t* b, uint32_t* o) {
+    uint64_t carry = 0;
+    for (int i = ML_N - 1; i >= 0; i--) {
+        uint64_t s = (uint64_t)a[i] + (uint64_t)b[i] + carry;
+        o[i] = (uint32_t)(s & 0xFFFFFFFFu);
+        carry = s >> 32;
+    }
+}
+
+static void ml_sub_mag(const uint32_t* a, const uint32_t* b, uint32_t* o) {
+    int64_t borrow = 0;
+    for (int i = ML_N - 1; i >= 0; i--) {
+        int64_t diff = (int64_t)a[i] - (int64_t)b[i] - borrow;
+        if (diff < 0) {
+            diff += 4294967296LL;
+            borrow = 1;
+        } else {
+            borrow = 0;
+        }
+        o[i] = (uint32_t)(diff & 0xFFFFFFFF);
+    }
+}
+
+static int ml_cmp_mag(const uint32_t* a, const uint32_t* b) {
+    for (int i = 0; i < ML_N; i++) {
+        if (a[i] > b[i]) return 1;
+        if (a[i] < b[i]) return -1;
+    }
+    return 0;
+}
+
+static int ml_add_signed(int as, const uint32_t* a, int bs, const uint32_t* b, uint32_t* o) {
+    if (as == bs) {
+        ml_add_mag(a, b, o);
+        return as;
+    }
+    if (ml_cmp_mag(a, b) >= 0) {
+        ml_sub_mag(a, b, o);
+        return as;
+    }
+    ml_sub_mag(b, a, o);
+    return bs;
+}
+
+static int ml_sub_signed(int as, const uint32_t* a, int bs, const uint32_t* b, uint32_t* o) {
+    return ml_add_signed(as, a, bs == 0 ? 1 : 0, b, o);
+}
+
+static void ml_mul_mag(const uint32_t* a, const uint32_t* b, uint32_t* o) {
+    uint64_t carry = 0;
+    for (int k = ML_N - 1; k >= 0; k--) {
+        uint64_t sum = carry;
+        for (int i = 0; i <= k; i++) sum += ((uint64_t)a[i] * (uint64_t)b[k - i]) & 0xFFFFFFFFu;
+        if (k + 1 < ML_N) {
+            for (int i = 0; i <= k + 1; i++) sum += ((uint64_t)a[i] * (uint64_t)b[k + 1 - i]) >> 32;
+        } else {
+            for (int i = 1; i < ML_N; i++) sum += ((uint64_t)a[i] * (uint64_t)b[ML_N - i]) >> 32;
+        }
+        o[k] = (uint32_t)(sum & 0xFFFFFFFFu);
+        carry = sum >> 32;
+    }
+}
+
+static float ml_sample(int cxs, const uint32_t* cxl, int cys, const uint32_t* cyl, int max_iter, int ft,
+                       int jxs, const uint32_t* jxl, int jys, const uint32_t* jyl) {
+    uint32_t zx[ML_N], zy[ML_N], zx2[ML_N], zy2[ML_N], zxy[ML_N], two_zxy[ML_N], sub_xy[ML_N], tmp[ML_N];
+    const uint32_t *cx, *cy;
+    int zxs = 0, zys = 0, c_xs, c_ys;
+    memset(zx, 0, sizeof zx);
+    memset(zy, 0, sizeof zy);
+    if (ft == 4) return -1.0f;
+    if (ft == 2 || ft == 3) {
+        memcpy(zx, cxl, sizeof zx);
+        memcpy(zy, cyl, sizeof zy);
+        zxs = cxs;
+        zys = cys;
+        c_xs = jxs;
+        c_ys = jys;
+        cx = jxl;
+        cy = jyl;
+    } else {
+        c_xs = cxs;
+        c_ys = cys;
+        cx = cxl;
+        cy = cyl;
+    }
+    for (int k = 0; k < max_iter; k++) {
+        if (ft == 1 || ft == 3) zxs = zys = 0;
+        ml_mul_mag(zx, zx, zx2);
+        ml_mul_mag(zy, zy, zy2);
+        if (zx2[0] >= 65536u || zy2[0] >= 65536u || (uint64_t)zx2[0] + (uint64_t)zy2[0] >= 65536u) {
+            double mag2 = (double)zx2[0] + (double)zy2[0] + ((double)zx2[1] + (double)zy2[1]) * 2.3283064365386963e-10;
+            return escaped(k, mag2, INV_LN2).s;
+        }
+        int zxys = zxs == zys ? 0 : 1;
+        ml_mul_mag(zx, zy, zxy);
+        ml_add_mag(zxy, zxy, two_zxy);
+        int subs = ml_sub_signed(0, zx2, 0, zy2, sub_xy);
+        zxs = ml_add_signed(subs, sub_xy, c_xs, cx, tmp);
+        memcpy(zx, tmp, sizeof zx);
+        if (ft == 1 || ft == 3)
+            zys = ml_sub_signed(0, two_zxy, c_ys, cy, tmp);
+        else
+            zys = ml_add_signed(zxys, two_zxy, c_ys, cy, tmp);
+        memcpy(zy, tmp, sizeof zy);
+    }
+    return -1.0f;
+}
+
+/* eval_glitched_pixels_cuda_kernel / _hist_ (math_core/cuda_kernels.py:2450-2569):
+   each listed pixel iterated on its own in double-double or in fixed point, then the
+   float32 value, its colour (black below 0) and a cleared glitch flag written. */
+APO_EXPORT int apo_strict_eval(const ApFrameParams* p, const ApFrameBuffers* b, const ApStrictView* v,
+                               const int32_t* coords, const int32_t* signs, const uint32_t* limbs, int n) {
+    const int hist = p->scheme_id == 11 && b->cdf != NULL;
+    ApFrameParams q = *p;
+    q.arith = AP_ARITH_REF_CUDA;
+    for (int t = 0; t < n; t++) {
+        int r = coords[2 * t], c = coords[2 * t + 1];
+        if (r < 0 || r >= p->height || c < 0 || c >= p->width) continue;
+        float s;
+        if (v->tier == AP_STRICT_DD) {
+            s = dd_sample_at(&q, (double)c, (double)r).s;
+        } else {
+            const uint32_t* l = limbs + (size_t)t * 2 * ML_N;
+            s = ml_sample(signs[2 * t], l, signs[2 * t + 1], l + ML_N, p->max_iter, p->fractal_type,
+                          v->jx_sign, v->jx_limbs, v->jy_sign, v->jy_limbs);
+        }
+        size_t idx = (size_t)r * p->width + c;
+        b->iter_map[idx] = s;
+        double cr = 0, cg = 0, cb = 0;
+        if (s >= 0.0f) lut_lerp(b->lut, colour_norm(p, b, (double)s, hist), &cr, &cg, &cb);
+        put_rgb(p, b->rgb, idx, cr, cg, cb);
+        if (b->glitch_out) b->glitch_out[idx] = 0;
+    }
+    return AP_OK;
+}
+
+/* Strict Metric write-back (math_core/engine.py:252-266): iter_map = float32 of the
+   value, the float64 value's colour unless it is < 0 or >= max_iter (then black),
+   glitch flag cleared. */
+APO_EXPORT int apo_set_pixels(const ApFrameParams* p, const ApFrameBuffers* b, const int32_t* coords,
+                              const double* values, int n) {
+    const int hist = p->scheme_id == 11 && b->cdf != NULL;
+    for (int q = 0; q < n; q++) {
+        int r = coords[2 * q], c = coords[2 * q + 1];
+        if (r < 0 || r >= p->height || c < 0 || c >= p->width) continue;
+        size_t idx = (size_t)r * p->width + c;
+        double s = values[q];
+        b->iter_map[idx] = (float)s;
+        double cr = 0, cg = 0, cb = 0;
+        if (s >= 0.0 && s < (double)p->max_iter) lut_lerp(b->lut, colour_norm(p, b, s, hist), &cr, &cg, &cb);
+        put_rgb(p, b->rgb, idx, cr, cg, cb);
+        if (b->glitch_out) b->glitch_out[idx] = 0;
+    }
+    return AP_OK;
+}
+
 /* Per-sample FP64 values on an explicit coordinate grid (x per column, y per row). */
 typedef struct {
     const ApFrameParams* p;

@@ -41,6 +41,8 @@ def lib():
         L.apo_render_pass.argtypes = [P, B]
         L.apo_resolve_hist_pass.argtypes = [P, B]
         L.apo_colour.argtypes = [P, B]
+        L.apo_set_pixels.argtypes = [P, B, C.c_void_p, C.c_void_p, C.c_int]
+        L.apo_strict_eval.argtypes = [P, B, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
         L.apo_edge_detect.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float]
         L.apo_histogram_cdf.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                         C.c_void_p, C.c_void_p]
@@ -165,6 +167,24 @@ def resolve_hist_pass(params, fr):
 
 def colour(params, fr):
     _check(lib().apo_colour(C.byref(params), C.byref(fr.buffers())), "colour")
+
+
+def strict_eval(params, fr, view, coords, signs=None, limbs=None):
+    """Device-tier Strict Metric re-evaluation of the listed pixels (apo_strict_eval);
+    ``view`` is an abi.ApStrictView."""
+    coords = np.ascontiguousarray(coords, np.int32)
+    signs = None if signs is None else np.ascontiguousarray(signs, np.int32)
+    limbs = None if limbs is None else np.ascontiguousarray(limbs, np.uint32)
+    _check(lib().apo_strict_eval(C.byref(params), C.byref(fr.buffers()), C.byref(view), ptr(coords),
+                                 ptr(signs), ptr(limbs), int(len(coords))), "strict_eval")
+
+
+def set_pixels(params, fr, coords, values):
+    """Strict Metric write-back of the listed (row, col) pixels (apo_set_pixels)."""
+    coords = np.ascontiguousarray(coords, np.int32)
+    values = np.ascontiguousarray(values, np.float64)
+    _check(lib().apo_set_pixels(C.byref(params), C.byref(fr.buffers()), ptr(coords), ptr(values),
+                                int(len(values))), "set_pixels")
 
 
 def edge_detect(fr, threshold):

@@ -596,6 +596,48 @@ def gen_render3():
     save("render_pert.npz", meta=json.dumps(meta), **out)
 
 
+def strict_cases():
+    pc = {c[0]: c for c in pert_cases()}
+    cases = []
+    # name, source case, W, H, max_iter, scheme
+    for (name, src, W, H, mi, sid) in (("strict_ship", "ship", 48, 27, 1500, 0),
+                                       ("strict_julia_hist", "julia", 48, 27, 1500, 11),
+                                       ("strict_ship_julia", "ship_julia", 48, 27, 1500, 5),
+                                       ("strict_multibrot3", "multibrot3", 48, 27, 1500, 0)):
+        c = pc[src]
+        cases.append((name, W, H, mi, c[2], c[3], c[4], sid, 1, 32, "Strict Metric",
+                      c[1], c[9], c[10], c[11], c[12], c[13]))
+    return cases
+
+
+def gen_strict():
+    """Strict Metric frames through render_frame_cpu: rebasing stops at 128 glitched
+    pixels or after 4 passes, then every pixel still flagged is evaluated on its own
+    high-precision orbit (math_core/engine.py:191-267, :1033-1046)."""
+    out = {}
+    meta = []
+    for c in strict_cases():
+        (name, W, H, mi, cx, cy, w, sid, fac, order, gm, ft, jx, jy, n, kr, ki) = c
+        R.hp.clear_reference_orbit_cache()
+        it = np.zeros((H, W), np.float32)
+        t0 = time.time()
+        rgb = R.engine.render_frame_cpu(
+            W, H, mi, Decimal(cx), Decimal(cy), Decimal(w), "synthetic",
+            ssaa_factor=fac, edge_threshold=0.35, color_scheme_id=sid,
+            precision_mode="1e-300 (Perturbation)", fractal_type=ft, julia_cx=jx, julia_cy=jy,
+            bbsa_tol=1e-6, bbsa_order=order, glitch_mode=gm,
+            gen_n=n, gen_kr=kr, gen_ki=ki, cpu_threads=8, palette_offset=0.0,
+            color_density=1.0, color_contrast=1.0, h_iter_buf=it)
+        print(f"  {name}: {time.time() - t0:.2f}s escaped {np.mean(it >= 0):.3f}")
+        out[name + "__rgb"] = rgb
+        out[name + "__iter"] = it
+        meta.append(dict(name=name, W=W, H=H, max_iter=mi, cx=cx, cy=cy, width=w, scheme=sid,
+                         factor=fac, bbsa_order=order, glitch_mode=gm, fractal_type=ft,
+                         julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki,
+                         offset=0.0, density=1.0, contrast=1.0))
+    save("render_strict.npz", meta=json.dumps(meta), **out)
+
+
 # ---------------------------------------------------------------------------
 # Ground truth for precision checks: direct iteration in 700-bit arithmetic
 # (mpmath), independent of the reference and of perturbation theory.
@@ -654,7 +696,7 @@ def gen_truth():
 
 SECTIONS = {"truth": gen_truth, "fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
             "fexp": gen_fexp, "bbsa": gen_bbsa, "render_bbsa": gen_render_bbsa, "config4": gen_config4,
-            "render3": gen_render3}
+            "render3": gen_render3, "strict": gen_strict}
 
 if __name__ == "__main__":
     wanted = sys.argv[1:] or list(SECTIONS)

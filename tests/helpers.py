@@ -210,4 +210,21 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
         else:
             q.mode, q.flags = abi.AP_MODE_FULL, uf | abi.AP_FLAG_ITER_LAST_SUB
             oracle.render_pass(q, fr)
+    if "Strict" in m["glitch_mode"]:
+        # every pixel still flagged: its own orbit, on the host in exact Decimal
+        # arithmetic (CPU path; CUDA path beyond its device tiers) or in the CUDA
+        # path's double-double / fixed-point tier
+        from fractura_b200.perturbation import strict_device_inputs, strict_device_tier, strict_values
+        coords = np.argwhere(fr.glitch_out > 0)
+        tier = None if cpu_sem else strict_device_tier(pw, ft)
+        if len(coords) and tier is None:
+            vals = strict_values(coords, W, H, mi, cxd, cyd, pw, ph, ft, m["julia_cx"], m["julia_cy"],
+                                 m["gen_n"], m["gen_kr"], m["gen_ki"], scalar=hp.decimal_escape_scalar)
+            q = abi.ApFrameParams.from_buffer_copy(p)
+            q.arith = abi.AP_ARITH_REF_CPU
+            oracle.set_pixels(q, fr, coords, vals)
+        elif len(coords):
+            q, view, signs, limbs = strict_device_inputs(p, coords, tier, W, H, cxd, cyd, pw, ph, m["julia_cx"],
+                                                         m["julia_cy"])
+            oracle.strict_eval(q, fr, view, coords, signs, limbs)
     return fr, state.passes

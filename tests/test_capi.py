@@ -38,8 +38,8 @@ def test_abi_version_and_struct_layout():
         pytest.skip("engine library not built")
     L = _lib.load()
     assert L.ap_abi_version() == abi.AP_ABI_VERSION
-    assert (C.sizeof(abi.ApFrameParams), C.sizeof(abi.ApFrameBuffers),
-            C.sizeof(abi.ApTileDesc)) == c_struct_sizes()
+    assert (C.sizeof(abi.ApFrameParams), C.sizeof(abi.ApFrameBuffers), C.sizeof(abi.ApTileDesc),
+            C.sizeof(abi.ApGradView), C.sizeof(abi.ApStrictView)) == c_struct_sizes()
 
 
 def c_struct_sizes(tmp_dir=None):
@@ -51,11 +51,11 @@ def c_struct_sizes(tmp_dir=None):
     exe = os.path.join(d, "sz")
     with open(src, "w") as f:
         f.write('#include <stdio.h>\n#include "apeiron_b200.h"\n'
-                'int main(void){printf("%zu %zu %zu", sizeof(ApFrameParams), sizeof(ApFrameBuffers),'
-                ' sizeof(ApTileDesc)); return 0;}\n')
+                'int main(void){printf("%zu %zu %zu %zu %zu", sizeof(ApFrameParams), sizeof(ApFrameBuffers),'
+                ' sizeof(ApTileDesc), sizeof(ApGradView), sizeof(ApStrictView)); return 0;}\n')
     subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
     out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
-    return int(out[0]), int(out[1]), int(out[2])
+    return tuple(int(x) for x in out)
 
 
 def test_oracle_sees_same_layout():

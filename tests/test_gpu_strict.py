@@ -1,0 +1,113 @@
+"""Strict Metric fallback on the device (ap_strict_eval) and through the engine.
+
+* ap_strict_eval equals the oracle on the reference-kernel fixtures (34-limb points,
+  double-double and fixed-point frames) value for value, colour for colour.
+* Whole Strict Metric frames through render_frame_ssaa equal the oracle's in both
+  profiles: the CPU path evaluates the remaining glitched pixels on the host, the CUDA
+  path in its device tiers (double-double at 2e-14, fixed point at 1e-160).
+"""
+import ctypes as C
+from decimal import Decimal
+
+import numpy as np
+import pytest
+
+import oracle
+from fractura_b200 import _lib, abi, engine
+from fractura_b200 import high_precision as hp
+from helpers import load_golden, oracle_pert_frame, rgb_mismatch
+from test_oracle_strict import ML_POINTS, SIM, SIM_FRAMES, ml_point_inputs, sim_frame_inputs
+
+pytestmark = pytest.mark.gpu
+
+
+def device_strict_eval(fr, q, view, coords, signs, limbs):
+    """ap_strict_eval on device copies of an oracle frame's buffers; returns (iter, rgb, glitch)."""
+    import torch
+    dev = "cuda"
+
+    def d(a):
+        return None if a is None else torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    it, rgb, gl = d(fr.iter_map), d(fr.rgb), d(fr.glitch_out)
+    lut, cdf = d(fr.lut), d(fr.cdf)
+    b = abi.ApFrameBuffers()
+    for name, t in (("iter_map", it), ("rgb", rgb), ("glitch_out", gl), ("lut", lut), ("cdf", cdf)):
+        setattr(b, name, None if t is None else t.data_ptr())
+    d_coords = d(np.asarray(coords, np.int32))
+    d_signs = d(signs)
+    d_limbs = None if limbs is None else d(np.asarray(limbs, np.uint32).view(np.int32))
+    L = _lib.load()
+    ptr = (lambda t: None if t is None else C.c_void_p(t.data_ptr()))
+    _lib.check(L.ap_strict_eval(C.byref(q), C.byref(b), C.byref(view), ptr(d_coords), ptr(d_signs),
+                                ptr(d_limbs), int(len(coords)), None), "ap_strict_eval")
+    torch.cuda.synchronize()
+    return it.cpu().numpy(), rgb.cpu().numpy(), gl.cpu().numpy()
+
+
+@pytest.mark.parametrize("ft", [0, 1, 2, 3])
+def test_fixed_point_points_device_equals_reference(ft):
+    pts = [p for p in ML_POINTS if p["ft"] == ft]
+    p, view, coords, signs, limbs = ml_point_inputs(pts)
+    fr = oracle.Frame(len(pts), 1, lut=np.zeros(2048 * 3, np.float32))
+    it, _, _ = device_strict_eval(fr, p, view, coords, signs, limbs)
+    want = np.array([q["s"] for q in pts], np.float32)
+    assert np.array_equal(it[0].view(np.uint32), want.view(np.uint32)), (it[0], want)
+
+
+@pytest.mark.parametrize("name", [m["name"] for m in SIM_FRAMES])
+def test_device_tier_frames_device_equals_oracle(name):
+    m = next(x for x in SIM_FRAMES if x["name"] == name)
+    fr, q, view, coords, signs, limbs = sim_frame_inputs(m)
+    it, rgb, gl = device_strict_eval(fr, q, view, coords, signs, limbs)
+    oracle.strict_eval(q, fr, view, coords, signs, limbs)
+    assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32))
+    assert np.array_equal(it.view(np.uint32), SIM[f"frame_{name}__iter"].view(np.uint32))
+    assert rgb_mismatch(rgb, fr.rgb)[0] == 0
+    assert not gl.any()
+
+
+STRICT, STRICT_META = load_golden("render_strict.npz")
+
+
+def engine_frame(m, arith, glitch_mode=None, width=None, W=None, H=None, max_iter=None):
+    W = W or m["W"]
+    H = H or m["H"]
+    hp.clear_reference_orbit_cache()
+    it = np.zeros((H, W), np.float32)
+    rgb = engine.render_frame_ssaa(
+        W, H, max_iter or m["max_iter"], Decimal(m["cx"]), Decimal(m["cy"]), Decimal(width or m["width"]), None,
+        color_scheme_id=m["scheme"], precision_mode="1e-300 (Perturbation)", fractal_type=m["fractal_type"],
+        julia_cx=m["julia_cx"], julia_cy=m["julia_cy"], bbsa_tol=1e-6, bbsa_order=m["bbsa_order"],
+        glitch_mode=glitch_mode or m["glitch_mode"], gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"],
+        h_iter_buf=it, arith=arith)
+    return it, rgb
+
+
+@pytest.mark.parametrize("name", [m["name"] for m in STRICT_META])
+@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda"])
+def test_strict_frame_engine_equals_oracle(name, arith):
+    m = next(x for x in STRICT_META if x["name"] == name)
+    it, rgb = engine_frame(m, arith)
+    from fractura_b200.perturbation import LAST_FRAME_STATS
+    assert LAST_FRAME_STATS["strict_pixels"] > 0
+    fr, _ = oracle_pert_frame(m, arith=0 if arith == "ref_cpu" else 1)
+    assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32)), \
+        int((it.view(np.uint32) != fr.iter_map.view(np.uint32)).sum())
+    assert rgb_mismatch(rgb, fr.rgb)[0] == 0
+    if arith == "ref_cpu":
+        assert np.array_equal(it.view(np.uint32), STRICT[name + "__iter"].view(np.uint32))
+
+
+def test_strict_frame_fixed_point_tier_through_engine():
+    """The CUDA path at 1e-160 (the deep view of the 1920x1080 workload, here 64x36):
+    pixels left after rebasing go through the 34-limb device tier."""
+    G, META = load_golden("render_pert.npz")
+    m = dict(next(x for x in META if x["name"] == "cfg3_bla_pauldelbrot"))
+    m.update(W=64, H=36, glitch_mode="Strict Metric", max_iter=4000)
+    it, rgb = engine_frame(m, "ref_cuda")
+    from fractura_b200.perturbation import LAST_FRAME_STATS
+    assert LAST_FRAME_STATS["strict_pixels"] > 0 and LAST_FRAME_STATS["strict_tier"] == abi.AP_STRICT_LIMBS
+    fr, _ = oracle_pert_frame(m, arith=1)
+    assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32))
+    assert rgb_mismatch(rgb, fr.rgb)[0] == 0
