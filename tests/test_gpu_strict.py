@@ -90,7 +90,9 @@ def test_strict_frame_engine_equals_oracle(name, arith):
     m = next(x for x in STRICT_META if x["name"] == name)
     it, rgb = engine_frame(m, arith)
     from fractura_b200.perturbation import LAST_FRAME_STATS
-    assert LAST_FRAME_STATS["strict_pixels"] > 0
+    # the CPU path stops rebasing at 128 glitched pixels and always leaves some here;
+    # the CUDA path may clear them all by rebasing
+    assert arith == "ref_cuda" or LAST_FRAME_STATS["strict_pixels"] > 0
     fr, _ = oracle_pert_frame(m, arith=0 if arith == "ref_cpu" else 1)
     assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32)), \
         int((it.view(np.uint32) != fr.iter_map.view(np.uint32)).sum())
@@ -104,7 +106,7 @@ def test_strict_frame_fixed_point_tier_through_engine():
     pixels left after rebasing go through the 34-limb device tier."""
     G, META = load_golden("render_pert.npz")
     m = dict(next(x for x in META if x["name"] == "cfg3_bla_pauldelbrot"))
-    m.update(W=64, H=36, glitch_mode="Strict Metric", max_iter=4000)
+    m.update(W=64, H=36, glitch_mode="Strict Metric", max_iter=20000)
     it, rgb = engine_frame(m, "ref_cuda")
     from fractura_b200.perturbation import LAST_FRAME_STATS
     assert LAST_FRAME_STATS["strict_pixels"] > 0 and LAST_FRAME_STATS["strict_tier"] == abi.AP_STRICT_LIMBS
