@@ -59,6 +59,13 @@ FLOPS_STEP1 = 25.0
 FLOPS_LEAP = 26.0
 FLOPS_STEP2 = 8.0
 FLOPS_DIRECT = 8.0  # FP64 direct Mandelbrot step
+# Double-double Burning Ship step, CPU profile (csrc/ap_dd.cuh with the Dekker
+# product): two squares (2 x 26), |Z|^2 (1), dd_sub (14), dd_mul of |zx|,|zy| (27),
+# doubling (2), dd_add (14), dd_sub (14)                                           -> 124
+FLOPS_DD_SHIP = 124.0
+# FloatExp perturbation step (FP64 mantissa): the FP64-delta step (25) plus the
+# exponent-scaled Z terms and the renormalisation test (10)                          -> 35
+FLOPS_STEP1_FEXP = 35.0
 
 
 # --------------------------------------------------------------- workloads
@@ -85,6 +92,23 @@ def workload_cfg1():
                 form="FP64 direct iteration, histogram colouring")
 
 
+def workload_cfg2():
+    cx, cy = _centres()["config2_centre"]
+    return dict(name="burning_ship_dd_1280x720_w1e-20_ssaa2", W=1280, H=720, max_iter=20000, cx=cx, cy=cy,
+                width="1e-20", scheme=0, factor=2, fractal_type=1, precision_mode="1e-24 (DD)",
+                bbsa_order=0, bbsa_tol=0.0, glitch_mode="Off (Single-Ref)", arith="ref_cpu", dtype="f64",
+                flops_per_iter=FLOPS_DD_SHIP,
+                form="double-double direct iteration, 2x adaptive SSAA (coarse, edge mask, edge pass)")
+
+
+def workload_cfg3b():
+    wl = workload_cfg3()
+    wl.update(name="mandelbrot_floatexp_bla_pauldelbrot_1920x1080_w1e-1000", width="1e-1000",
+              form="FloatExp deltas (FP64 mantissa, int exponent), dc-aware chained BLA (eps 1e-14), "
+                   "Pauldelbrot with up to 4 rebase passes")
+    return wl
+
+
 def workload_cfg4():
     tiles = _centres().get("config4_tiles")
     if not tiles:
@@ -99,7 +123,8 @@ def workload_cfg4():
                      "autotuned launch shape")
 
 
-WORKLOADS = {"cfg3": workload_cfg3, "cfg1": workload_cfg1, "cfg4": workload_cfg4}
+WORKLOADS = {"cfg3": workload_cfg3, "cfg1": workload_cfg1, "cfg2": workload_cfg2, "cfg3b": workload_cfg3b,
+             "cfg4": workload_cfg4}
 DEFAULT_WORKLOAD = "cfg3"
 
 
@@ -287,21 +312,25 @@ def oracle_pert_rows(wl, budget_s, start=0):
     import oracle
     from fractura_b200 import abi
     from fractura_b200 import high_precision as hp
-    from fractura_b200.config import decimal_context
+    from fractura_b200.config import compute_floatexp_scale, decimal_context
     from decimal import localcontext
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
     W, H, mi = wl["W"], wl["H"], wl["max_iter"]
     pw = Decimal(wl["width"])
+    floatexp = pw < Decimal("1e-300")
+    e_scale = compute_floatexp_scale(pw) if floatexp else 0
     with localcontext(decimal_context(pw)):
         ph = pw * (Decimal(H) / Decimal(W))
-        dx = float(pw / Decimal(W - 1))
-        dy = float(ph / Decimal(H - 1))
+        two_e = Decimal(2) ** e_scale
+        dx = float(pw * two_e / Decimal(W - 1))
+        dy = float(ph * two_e / Decimal(H - 1))
     t0 = time.perf_counter()
     bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
-        Decimal(wl["cx"]), Decimal(wl["cy"]), pw, ph, mi, W, H)
+        Decimal(wl["cx"]), Decimal(wl["cy"]), pw, ph, mi, W, H, is_floatexp=floatexp)
     T = oracle.build_bla(re, im, rl, 0, 1e-6, 16, 3, 0.25, 1.0) if wl["bbsa_order"] == 32 else None
-    p = abi.new_params(width=W, height=H, max_iter=mi, tier=abi.AP_TIER_PERTURB,
+    p = abi.new_params(width=W, height=H, max_iter=mi,
+                       tier=abi.AP_TIER_FLOATEXP if floatexp else abi.AP_TIER_PERTURB, e_scale=e_scale,
                        arith=abi.AP_ARITH_REF_CPU, dx_hi=dx, dy_hi=dy, ref_px=(W - 1) * float(bu),
                        ref_py=(H - 1) * float(bv), ref_cx=float(bcx), ref_cy=float(bcy), ref_len=rl,
                        bla_levels=16 if T is not None else 0, strict_glitch=1,
@@ -331,7 +360,8 @@ def oracle_baseline(wl, budget_s=12.0, sampled=False, start=0):
     or whole tiles (batches) until budget_s is spent."""
     if wl.get("kind") == "batch":
         return oracle_batch_baseline(wl, budget_s, start=start)
-    if sampled and not wl["precision_mode"].startswith("1e-12"):
+    direct = wl["precision_mode"].startswith(("1e-12", "1e-24"))
+    if sampled and not direct:
         return oracle_pert_rows(wl, budget_s, start=start)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -342,18 +372,25 @@ def oracle_baseline(wl, budget_s=12.0, sampled=False, start=0):
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
     W, H, mi = wl["W"], wl["H"], wl["max_iter"]
-    if wl["precision_mode"].startswith("1e-12"):
+    if direct:
         sys.path.insert(0, os.path.join(ROOT, "tests"))
-        from helpers import direct_params
-        m = dict(W=W, H=H, factor=1, max_iter=mi, cx=wl["cx"], cy=wl["cy"], width=wl["width"],
+        from helpers import direct_params, oracle_direct_frame
+        m = dict(W=W, H=H, factor=wl["factor"], max_iter=mi, cx=wl["cx"], cy=wl["cy"], width=wl["width"],
                  scheme=wl["scheme"], fractal_type=wl["fractal_type"])
-        p = direct_params(m, abi.AP_TIER_FP64, abi.AP_ARITH_REF_CPU)
-        p.flags = abi.AP_FLAG_NO_RGB
-        fr = oracle.Frame(W, H)
+        tier = abi.AP_TIER_FP64 if wl["precision_mode"].startswith("1e-12") else abi.AP_TIER_DD
+        if wl["factor"] == 1:
+            p = direct_params(m, tier, abi.AP_ARITH_REF_CPU)
+            p.flags = abi.AP_FLAG_NO_RGB
+            fr = oracle.Frame(W, H)
+            t0 = time.perf_counter()
+            oracle.render_pass(p, fr)
+            t = time.perf_counter() - t0
+            return nominal_iterations(fr.kmap, mi) / t / 1e9, cores, f"full {W}x{H} frame, one pass"
         t0 = time.perf_counter()
-        oracle.render_pass(p, fr)
+        fr = oracle_direct_frame(m, tier=tier, arith=abi.AP_ARITH_REF_CPU)
         t = time.perf_counter() - t0
-        return nominal_iterations(fr.kmap, mi) / t / 1e9, cores, f"full {W}x{H} frame, one pass"
+        return (nominal_iterations(fr.kmap, mi) / t / 1e9, cores,
+                f"full {W}x{H} frame with its {wl['factor']}x adaptive SSAA passes")
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from helpers import oracle_pert_frame
     m = dict(W=W, H=H, factor=wl["factor"], max_iter=mi, cx=wl["cx"], cy=wl["cy"],
@@ -431,7 +468,7 @@ def timed_replay(torch, _lib, ops, stream, steps, flush, record_pass=False):
     return step_ms, pass_ev
 
 
-def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla):
+def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla, direct_flops=FLOPS_DIRECT):
     """Executed FP64 operations of every render pass in one replay, from the work counters."""
     counters = torch.zeros((H, W, 4), dtype=torch.int32, device="cuda")
     f1 = 18.0 + (4.0 if strict else 0.0) + (3.0 if has_bla else 0.0)
@@ -450,8 +487,11 @@ def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla):
                 _lib.check(fn(args[0], C.byref(q), args[2]), what)
                 c = counters.view(-1, 4).sum(dim=0, dtype=torch.int64).cpu().numpy()
                 p = args[0]._obj
-                if p.tier == abi.AP_TIER_FP64:
-                    total += FLOPS_DIRECT * float(c[0])
+                if p.tier in (abi.AP_TIER_FP64, abi.AP_TIER_DD):
+                    total += direct_flops * float(c[0])
+                elif p.tier == abi.AP_TIER_FLOATEXP:
+                    total += (f1 - 25.0 + FLOPS_STEP1_FEXP) * float(c[0]) + FLOPS_LEAP * float(c[1]) + \
+                        FLOPS_STEP2 * float(c[2])
                 else:
                     total += f1 * float(c[0]) + FLOPS_LEAP * float(c[1]) + FLOPS_STEP2 * float(c[2])
                 launches += 1
@@ -679,7 +719,8 @@ def our_arm(args, wl, rank, world, local_rank):
                       "speedup_vs_plain_single_reference": single_ratio, "forms": forms}
 
     strict = "Pauldelbrot" in wl["glitch_mode"] or "Strict" in wl["glitch_mode"]
-    flops, n_pass = pass_flops(torch, _lib, abi, chosen.ops, stream, H, W, strict, perturb)
+    flops, n_pass = pass_flops(torch, _lib, abi, chosen.ops, stream, H, W, strict, perturb,
+                               wl.get("flops_per_iter", FLOPS_DIRECT))
     pass_ms = float(np.sum([a.elapsed_time(b) for a, b in pass_ev])) / args.steps
     peak64 = fma_peak_tflops(64, torch)
     achieved = flops / (pass_ms * 1e-3) / 1e12 if pass_ms > 0 else None
