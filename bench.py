@@ -677,7 +677,9 @@ def our_arm(args, wl, rank, world, local_rank):
     h_rgb = torch.empty((H, W, 3), dtype=torch.uint8).pin_memory().numpy()
     barrier(world)
     t0 = time.perf_counter()
+    from fractura_b200 import high_precision as hp
     for _ in range(e2e_steps):
+        hp.clear_reference_orbit_cache()  # every step computes its orbits: a cold frame
         render_call(engine, wl, stream, h_rgb_buf=h_rgb, **chosen.over)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     barrier(world)

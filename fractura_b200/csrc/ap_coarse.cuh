@@ -90,19 +90,25 @@ __device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFra
         const double rx = Z.x, ry = Z.y;
         const double zx = rx + dzx, zy = ry + dzy;
         const double dz_mag2 = dzx * dzx + dzy * dzy;
-        if (!(dz_mag2 < Z.w)) {  // outside the safe radius: the tests may fire
-            const double mag2 = zx * zx + zy * zy;
-            if (mag2 > kBailout) {
-                if (esc_glitch && strict && k > 15 && (rx * rx + ry * ry) < 4.0) glitch = 1;
-                o = escaped_sample(k, mag2, inv_ln);
-                finished = true;
-                break;
+        // One branch on the common path: inside the safe radius (no test can fire)
+        // and outside the level-0 BLA radius (no leap), the step runs straight
+        // through.  The packed rows hold 0 wherever k + 2^d >= ref_len, so no level
+        // is admissible at the last step without a separate bound check.
+        const double* row = R + (size_t)k * 16;
+        const bool unsafe = !(dz_mag2 < Z.w);
+        const bool leap = BLA && (dz_mag2 < __ldg(row));
+        if (unsafe || leap) {
+            if (unsafe) {
+                const double mag2 = zx * zx + zy * zy;
+                if (mag2 > kBailout) {
+                    if (esc_glitch && strict && k > 15 && (rx * rx + ry * ry) < 4.0) glitch = 1;
+                    o = escaped_sample(k, mag2, inv_ln);
+                    finished = true;
+                    break;
+                }
+                if (strict && k > 15 && mag2 < Z.z) glitch = 1;
             }
-            if (strict && k > 15 && mag2 < Z.z) glitch = 1;
-        }
-        if (BLA && k < ref_len - 1) {
-            const double* row = R + (size_t)k * 16;
-            if (dz_mag2 < __ldg(row)) {
+            if (leap) {
                 int hi = max_level;
                 if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
                 int lo = 0;  // row[lo] admissible

@@ -84,35 +84,69 @@ inline void add_s(Fx& r, const Fx& a, int an, const Fx& b, int bn, int L) {
 inline void add(Fx& r, const Fx& a, const Fx& b, int L) { add_s(r, a, a.neg, b, b.neg, L); }
 inline void sub(Fx& r, const Fx& a, const Fx& b, int L) { add_s(r, a, a.neg, b, !b.neg, L); }
 
+// 192-bit column accumulator of the product-scanning (Comba) products below.
+struct Acc3 {
+    u64 c0 = 0, c1 = 0, c2 = 0;
+    inline void add(u128 p) {
+        const u128 s0 = (u128)c0 + (u64)p;
+        c0 = (u64)s0;
+        const u128 s1 = (u128)c1 + (u64)(p >> 64) + (u64)(s0 >> 64);
+        c1 = (u64)s1;
+        c2 += (u64)(s1 >> 64);
+    }
+    inline void add_twice(const Acc3& o) {  // += 2 * o (o below 2^191)
+        const u64 d0 = o.c0 << 1, d1 = (o.c1 << 1) | (o.c0 >> 63), d2 = (o.c2 << 1) | (o.c1 >> 63);
+        const u128 s0 = (u128)c0 + d0;
+        c0 = (u64)s0;
+        const u128 s1 = (u128)c1 + d1 + (u64)(s0 >> 64);
+        c1 = (u64)s1;
+        c2 += d2 + (u64)(s1 >> 64);
+    }
+    inline u64 shift() {  // take the finished column, move the carries down
+        const u64 out = c0;
+        c0 = c1;
+        c1 = c2;
+        c2 = 0;
+        return out;
+    }
+};
+
 // r = a * b (fixed point, truncated).  Product limb k (of 2L) has weight
 // 2^(64 k - 2F); the result keeps limbs [L - I, 2L - I).  Partial products with
 // index i + j < L - I - 2 are not formed: together they are worth less than one
-// unit of the last kept limb.
+// unit of the last kept limb.  The kept pairs are summed column by column, so the
+// result is the exact sum of the same partial products in any order of
+// evaluation; columns above the kept range are not formed (nothing carries down).
 inline void mul(Fx& r, const Fx& a, const Fx& b, int L, int I) {
-    u64 acc[2 * kMaxLimbs + 2];
-    std::memset(acc, 0, sizeof(u64) * (2 * L + 2));
     const int lo = L - I - 2 > 0 ? L - I - 2 : 0;
-    for (int i = 0; i < L; ++i) {
-        const u64 ai = a.m[i];
-        if (!ai) continue;
-        const int j0 = lo - i > 0 ? lo - i : 0;
-        u64 carry = 0;
-        int j = j0;
-        for (; j < L; ++j) {
-            const u128 p = (u128)ai * b.m[j] + acc[i + j] + carry;
-            acc[i + j] = (u64)p;
-            carry = (u64)(p >> 64);
-        }
-        int k = i + j;
-        while (carry) {
-            const u128 s = (u128)acc[k] + carry;
-            acc[k] = (u64)s;
-            carry = (u64)(s >> 64);
-            ++k;
-        }
+    const int keep = L - I, top = 2 * L - I - 1;
+    Acc3 acc;
+    for (int col = lo; col <= top; ++col) {
+        const int i0 = col - (L - 1) > 0 ? col - (L - 1) : 0;
+        const int i1 = col < L - 1 ? col : L - 1;
+        for (int i = i0; i <= i1; ++i) acc.add((u128)a.m[i] * b.m[col - i]);
+        const u64 limb = acc.shift();
+        if (col >= keep) r.m[col - keep] = limb;
     }
-    std::memcpy(r.m, acc + (L - I), sizeof(u64) * L);
     r.neg = (a.neg ^ b.neg) && !is_zero(r.m, L);
+}
+
+// r = a * a: the same column sums as mul(r, a, a), each symmetric pair formed once
+// (summed apart, then added twice).
+inline void sqr(Fx& r, const Fx& a, int L, int I) {
+    const int lo = L - I - 2 > 0 ? L - I - 2 : 0;
+    const int keep = L - I, top = 2 * L - I - 1;
+    Acc3 acc;
+    for (int col = lo; col <= top; ++col) {
+        const int i0 = col - (L - 1) > 0 ? col - (L - 1) : 0;
+        Acc3 off;
+        for (int i = i0; 2 * i < col; ++i) off.add((u128)a.m[i] * a.m[col - i]);
+        acc.add_twice(off);
+        if ((col & 1) == 0 && col / 2 < L) acc.add((u128)a.m[col / 2] * a.m[col / 2]);
+        const u64 limb = acc.shift();
+        if (col >= keep) r.m[col - keep] = limb;
+    }
+    r.neg = 0;
 }
 
 inline void twice(Fx& r, const Fx& a, int L) {
@@ -229,16 +263,16 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
     sx = zx;
     sy = zy;
     int len = max_iter;
-    // FNV-1a over the float64 bits of every Z_k: lets two runs at different
+    // A multiplicative hash over the float64 bits of every Z_k (xor, then multiply
+    // by an odd constant: each step is a bijection of the state, so a single
+    // differing value always changes the state): lets two runs at different
     // precisions confirm they followed the same float64 trajectory.
     u64 hash = 1469598103934665603ULL;
     auto mix = [&](double d) {
         u64 b;
         std::memcpy(&b, &d, 8);
-        for (int q = 0; q < 8; ++q) {
-            hash ^= (b >> (8 * q)) & 0xff;
-            hash *= 1099511628211ULL;
-        }
+        hash = (hash ^ b) * 0x9E3779B97F4A7C15ULL;
+        hash ^= hash >> 29;
     };
     for (int k = 0; k < max_iter; ++k) {
         if (!escape_only || trace_hash) {
@@ -252,8 +286,8 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
                 mix(im);
             }
         }
-        mul(zx2, zx, zx, L, I);
-        mul(zy2, zy, zy, L, I);
+        sqr(zx2, zx, L, I);
+        sqr(zy2, zy, L, I);
         add(mag, zx2, zy2, L);
         if (!mag.neg && cmp_mag(mag.m, bail.m, L) > 0) {
             len = k;

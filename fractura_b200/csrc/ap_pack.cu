@@ -34,7 +34,9 @@ __global__ void __launch_bounds__(256) pack_bla_kernel(const double* __restrict_
     const int k = t >> 4, d = t & 15;
     if (d < levels) {
         const double* e = T + ((size_t)d * ref_len + k) * 5;
-        R[t] = e[4];
+        // a level is admissible only if its leap ends before the orbit does
+        // (k + 2^d < ref_len); the coarse loop relies on 0 radii elsewhere
+        R[t] = (k + (1 << d) < ref_len) ? e[4] : 0.0;
         AB[t] = make_double4(e[0], e[1], e[2], e[3]);
     } else {
         R[t] = 0.0;

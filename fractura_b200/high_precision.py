@@ -141,7 +141,8 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     fa = _pair_pool().submit(_native_orbit, seeds, hi, max_iter, fractal_type, gen_n)
     b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
     a = fa.result()
-    if a[2] == b[2] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]):
+    n = a[2] + 1  # past ref_len both hold zeros, or the same copied cycle
+    if a[2] == b[2] and np.array_equal(a[0][:n], b[0][:n]) and np.array_equal(a[1][:n], b[1][:n]):
         return a
     return decimal_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,
                          prec_bits, gen_n, gen_kr, gen_ki)

@@ -180,7 +180,8 @@ AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref
 /* Chained-BLA table in the layout the perturbation kernels read: the 16 radii of
  * step k in one 128-byte row ([ref_len, 16] float64), then the coefficients
  * (A_re, A_im, B_re, B_im) per step and level ([ref_len, 16, 4] float64); levels
- * at or above `levels` hold radius 0.  table: the [levels, ref_len, 5] layout of
+ * at or above `levels`, and leaps that would reach the end of the orbit
+ * (k + 2^d >= ref_len), hold radius 0.  table: the [levels, ref_len, 5] layout of
  * ap_build_bla.  out: 80 * ref_len float64. */
 AP_API int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len, double* out,
                        void* stream);
