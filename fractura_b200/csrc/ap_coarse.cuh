@@ -111,14 +111,18 @@ __device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFra
             if (leap) {
                 int hi = max_level;
                 if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
-                int lo = 0;  // row[lo] admissible
-#pragma unroll 4
-                for (int it = 0; it < 4; ++it) {
-                    if (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (dz_mag2 < __ldg(row + mid)) lo = mid;
-                        else hi = mid - 1;
-                    }
+                // The admissible levels are a prefix 0..lo (radii never increase
+                // with the level), so lo is a count.  Two rounds of three
+                // independent loads: the quarter of the row, then the level in it.
+                int q = 0;
+#pragma unroll
+                for (int t = 1; t <= 3; ++t)
+                    q += (4 * t <= hi && dz_mag2 < __ldg(row + 4 * t)) ? 1 : 0;
+                int lo = 4 * q;
+#pragma unroll
+                for (int t = 1; t <= 3; ++t) {
+                    const int d = 4 * q + t;
+                    lo += (d <= hi && dz_mag2 < __ldg(row + d)) ? 1 : 0;
                 }
                 const double4 e = ldg4(AB + (size_t)k * 16 + lo);
                 double nx, ny;
