@@ -72,7 +72,7 @@ def load():
     L.ap_histogram_cdf_noalloc.argtypes = [vp, i32, i32, i32, i32, vp, vp]
     L.ap_launch_counter.restype = C.c_uint64
     L.ap_pack_orbit.argtypes = [vp, vp, i32, vp, vp]
-    L.ap_pack_bla.argtypes = [vp, i32, i32, vp, vp]
+    L.ap_pack_bla.argtypes = [vp, i32, i32, vp, vp, vp]
     L.ap_pack_fe32.argtypes = [vp, i32, vp, i32, vp, vp, vp]
     for name in EXPORTS:
         fn = getattr(L, name)

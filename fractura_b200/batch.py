@@ -165,7 +165,8 @@ def _tile_inputs(t, cpu_sem, bla_form, torch, stream, L, scratch):
                                       BLA_LEVELS, int(t.gen_n), float(t.gen_kr), float(t.gen_ki),
                                       _ptr(table), s), "ap_build_bla")
         bla_packed = torch.empty(80 * rl, dtype=torch.float64, device="cuda")
-        _lib.check(L.ap_pack_bla(_ptr(table), BLA_LEVELS, int(rl), _ptr(bla_packed), s), "ap_pack_bla")
+        _lib.check(L.ap_pack_bla(_ptr(table), BLA_LEVELS, int(rl), _ptr(bla_packed), _ptr(orbit), s),
+                   "ap_pack_bla")
         stream.synchronize()  # the table scratch is reused by the next tile
     flags = abi.AP_FLAG_NO_RGB | ((abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem
                                   else abi.AP_FLAG_NAN_GUARD)

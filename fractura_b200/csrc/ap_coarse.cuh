@@ -5,11 +5,10 @@
 // by ap_render_pass when the buffers carry the packed orbit (ap_pack_orbit)
 // and, with BLA, the packed table (ap_pack_bla).  What changes is only how the
 // loop gets its inputs:
-//   * one 32-byte read per step: Z_k, the Pauldelbrot threshold precomputed
-//     exactly as the step would compute it, and a safe radius: while |dz| is
-//     below it neither the escape test nor the Pauldelbrot test can fire, so
-//     |Z + dz|^2 is not formed (the rounded |dz|^2 decides, and the BLA test
-//     reuses it);
+//   * one 32-byte read per step: Z_k, a safe radius and the level-0 BLA
+//     radius.  While |dz| is below the safe radius neither the escape test nor
+//     the Pauldelbrot test can fire, so |Z + dz|^2 and the threshold are not
+//     formed (the rounded |dz|^2 decides, and the BLA test reuses it);
 //   * the 16 BLA radii of step k in one 128-byte row.  Radii never increase
 //     with the level (each level's radius is the min of its first half's), and
 //     levels past the end of the orbit hold 0, so the largest admissible level
@@ -92,23 +91,26 @@ __device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFra
         const double dz_mag2 = dzx * dzx + dzy * dzy;
         // One branch on the common path: inside the safe radius (no test can fire)
         // and outside the level-0 BLA radius (no leap), the step runs straight
-        // through.  The packed rows hold 0 wherever k + 2^d >= ref_len, so no level
+        // through.  The packed radii are 0 wherever k + 2^d >= ref_len, so no level
         // is admissible at the last step without a separate bound check.
-        const double* row = R + (size_t)k * 16;
-        const bool unsafe = !(dz_mag2 < Z.w);
-        const bool leap = BLA && (dz_mag2 < __ldg(row));
+        const bool unsafe = !(dz_mag2 < Z.z);
+        const bool leap = BLA && (dz_mag2 < Z.w);
         if (unsafe || leap) {
             if (unsafe) {
                 const double mag2 = zx * zx + zy * zy;
+                const double r_mag2 = rx * rx + ry * ry;
                 if (mag2 > kBailout) {
-                    if (esc_glitch && strict && k > 15 && (rx * rx + ry * ry) < 4.0) glitch = 1;
+                    if (esc_glitch && strict && k > 15 && r_mag2 < 4.0) glitch = 1;
                     o = escaped_sample(k, mag2, inv_ln);
                     finished = true;
                     break;
                 }
-                if (strict && k > 15 && mag2 < Z.z) glitch = 1;
+                // the Pauldelbrot threshold, as the reference forms it
+                const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;
+                if (strict && k > 15 && mag2 < thr) glitch = 1;
             }
             if (leap) {
+                const double* row = R + (size_t)k * 16;
                 int hi = max_level;
                 if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
                 // The admissible levels are a prefix 0..lo (radii never increase

@@ -197,7 +197,8 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
                     break;
                 }
                 if (near_glitch) {
-                    const double thr = __ldg(reinterpret_cast<const double*>(orb + k) + 2);
+                    const double r2 = Z64.x * Z64.x + Z64.y * Z64.y;
+                    const double thr = r2 > 1e-8 ? 1e-6 * r2 : -1.0;  // as the reference forms it
                     if (mag2 < thr) glitch = 1;
                 }
             }

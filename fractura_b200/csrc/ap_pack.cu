@@ -13,7 +13,7 @@ __global__ void __launch_bounds__(256) pack_orbit_kernel(const double* __restric
     if (k >= n) return;
     const double rx = re[k], ry = im[k];
     const double r_mag2 = rx * rx + ry * ry;
-    const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;
+    const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;  // the Pauldelbrot threshold
     // Safe radius s: for |dz| < s the rounded |Z + dz|^2 is neither above the
     // bailout 65536 (|Z| + s <= 256 (1 - 1e-12)) nor below the Pauldelbrot
     // threshold 1e-6 |Z|^2 (|Z| - s >= 1e-3 |Z| (1 + 1e-7)); the 1e-12 margins
@@ -23,12 +23,14 @@ __global__ void __launch_bounds__(256) pack_orbit_kernel(const double* __restric
     double s = 256.0 * (1.0 - 1e-12) - rz * (1.0 + 1e-12);
     if (thr >= 0.0) s = fmin(s, rz * (1.0 - 1e-12) * (1.0 - 1.0000001e-3));
     s = s > 0.0 ? s : 0.0;
-    out[k] = make_double4(rx, ry, thr, s * s * (1.0 - 1e-12));
+    // slot 3: the level-0 BLA radius, written by ap_pack_bla (0: no leap)
+    out[k] = make_double4(rx, ry, s * s * (1.0 - 1e-12), 0.0);
 }
 
 __global__ void __launch_bounds__(256) pack_bla_kernel(const double* __restrict__ T, int levels,
                                                        int ref_len, double* __restrict__ R,
-                                                       double4* __restrict__ AB) {
+                                                       double4* __restrict__ AB,
+                                                       double* __restrict__ orb) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;  // one (k, d) pair per thread
     if (t >= ref_len * 16) return;
     const int k = t >> 4, d = t & 15;
@@ -37,6 +39,7 @@ __global__ void __launch_bounds__(256) pack_bla_kernel(const double* __restrict_
         // a level is admissible only if its leap ends before the orbit does
         // (k + 2^d < ref_len); the coarse loop relies on 0 radii elsewhere
         R[t] = (k + (1 << d) < ref_len) ? e[4] : 0.0;
+        if (d == 0 && orb) orb[4 * (size_t)k + 3] = R[t];  // the orbit record's level-0 radius
         AB[t] = make_double4(e[0], e[1], e[2], e[3]);
     } else {
         R[t] = 0.0;
@@ -59,7 +62,7 @@ extern "C" int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t
 }
 
 extern "C" int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len, double* out,
-                           void* stream) {
+                           double* orbit_packed, void* stream) {
     if (!table || !out || levels < 1 || levels > 16 || ref_len < 1 ||
         (reinterpret_cast<uintptr_t>(out) & 31u)) {
         ap::set_error("ap_pack_bla: bad arguments (1 <= levels <= 16, out 32-byte aligned)");
@@ -69,6 +72,6 @@ extern "C" int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len,
     double4* AB = reinterpret_cast<double4*>(out + (size_t)ref_len * 16);
     const int n = ref_len * 16;
     ap::pack_bla_kernel<<<(n + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        table, levels, ref_len, R, AB);
+        table, levels, ref_len, R, AB, orbit_packed);
     return ap::check_launch("pack_bla_kernel");
 }

@@ -219,12 +219,13 @@ def _pack_orbit(L, d_re, d_im, ref_len, slot, tag, stream_h):
     return packed
 
 
-def _pack_bla(L, table, ref_len, slot, tag, stream_h):
+def _pack_bla(L, table, ref_len, slot, tag, stream_h, orbit_packed):
+    """Packed BLA rows; also fills the level-0 radius of the packed orbit records."""
     from .engine import get_scratch_device_array_1d
     n = 80 * max(ref_len, 1)
     packed = get_scratch_device_array_1d(n, np.float64, f"bla_packed_{tag}_{slot}")[:n]
-    _lib.launch(L.ap_pack_bla, _ptr(table), BLA_LEVELS, int(ref_len), _ptr(packed), stream_h,
-                what="ap_pack_bla")
+    _lib.launch(L.ap_pack_bla, _ptr(table), BLA_LEVELS, int(ref_len), _ptr(packed), _ptr(orbit_packed),
+                stream_h, what="ap_pack_bla")
     return packed
 
 
@@ -233,7 +234,7 @@ def _inputs(L, d_re, d_im, ref_len, bla, slot, tag, stream_h, fp32=False):
     FP32 FloatExp tier, the FP32 orbit copy and BLA records."""
     from .engine import get_scratch_device_array_1d
     po = _pack_orbit(L, d_re, d_im, ref_len, slot, tag, stream_h)
-    pb = _pack_bla(L, bla, ref_len, slot, tag, stream_h) if (bla is not None and ref_len > 0) else None
+    pb = _pack_bla(L, bla, ref_len, slot, tag, stream_h, po) if (bla is not None and ref_len > 0) else None
     pf = None
     if fp32:
         n4 = 4 * (ref_len + 1)

@@ -26,7 +26,7 @@ extern "C" {
 #define AP_API
 #endif
 
-#define AP_ABI_VERSION 4
+#define AP_ABI_VERSION 5
 
 /* Return codes. */
 #define AP_OK 0
@@ -169,11 +169,11 @@ AP_API int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height
                      int32_t num_bins, int32_t* hist, float* cdf, void* stream);
 
 /* Reference orbit in the layout the perturbation kernels read: per step the
- * 32-byte record (Z_re, Z_im, Pauldelbrot threshold, safe radius^2), the threshold
- * being 1e-6 |Z|^2 where |Z|^2 > 1e-8 and -1 elsewhere (the glitch test of
- * math_core/cpu_kernels.py:428-431 as one compare); while the rounded |dz|^2 is below
- * the safe radius^2 neither the escape nor the glitch test can fire at that step.
- * out: [ref_len + 1, 4] float64. */
+ * 32-byte record (Z_re, Z_im, safe radius^2, level-0 BLA radius^2).  While the
+ * rounded |dz|^2 is below the safe radius^2 neither the escape test nor the glitch
+ * test (|Z + dz|^2 < 1e-6 |Z|^2 where |Z|^2 > 1e-8, math_core/cpu_kernels.py:428-431)
+ * can fire at that step.  The level-0 radius is written by ap_pack_bla; this call
+ * leaves it 0 (no leap).  out: [ref_len + 1, 4] float64. */
 AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref_len, double* out,
                          void* stream);
 
@@ -182,9 +182,11 @@ AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref
  * (A_re, A_im, B_re, B_im) per step and level ([ref_len, 16, 4] float64); levels
  * at or above `levels`, and leaps that would reach the end of the orbit
  * (k + 2^d >= ref_len), hold radius 0.  table: the [levels, ref_len, 5] layout of
- * ap_build_bla.  out: 80 * ref_len float64. */
+ * ap_build_bla.  out: 80 * ref_len float64.  orbit_packed: the ap_pack_orbit
+ * records of the same orbit, whose level-0 radius slot is filled here (the coarse
+ * pass tests that slot before each step; NULL leaves it 0, and no leap is taken). */
 AP_API int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len, double* out,
-                       void* stream);
+                       double* orbit_packed, void* stream);
 
 /* Inputs of AP_TIER_FLOATEXP32 (the FP32-mantissa FloatExp fast form).
  * orbit_packed: the ap_pack_orbit records; orbit32_out: [ref_len + 1] float4 (Z_re,

@@ -96,9 +96,9 @@ def test_packed_orbit_and_bla_layouts():
     got = po.cpu().numpy()
     r2 = re * re + im * im
     assert np.array_equal(got[:, 0], re) and np.array_equal(got[:, 1], im)
-    assert np.array_equal(got[:, 2], np.where(r2 > 1e-8, 1e-6 * r2, -1.0))
+    assert not got[:, 3].any()  # level-0 radius: filled by ap_pack_bla
     # safe radius: inside it neither the bailout nor the Pauldelbrot threshold is reachable
-    safe2 = got[:, 3]
+    safe2 = got[:, 2]
     s = np.sqrt(safe2)
     rz = np.sqrt(r2)
     assert np.all(safe2 >= 0.0)
@@ -111,10 +111,13 @@ def test_packed_orbit_and_bla_layouts():
     T = oracle.build_bla(re, im, rl, 0, 1e-6, 16, 3, 0.25, 1.0)
     d_T = torch.from_numpy(T).cuda()
     pb = torch.empty(80 * rl, dtype=torch.float64, device="cuda")
-    _lib.check(L.ap_pack_bla(C.c_void_p(d_T.data_ptr()), 16, rl, C.c_void_p(pb.data_ptr()), None),
-               "ap_pack_bla")
+    _lib.check(L.ap_pack_bla(C.c_void_p(d_T.data_ptr()), 16, rl, C.c_void_p(pb.data_ptr()),
+                             C.c_void_p(po.data_ptr()), None), "ap_pack_bla")
     pb = pb.cpu().numpy()
     R = pb[:16 * rl].reshape(rl, 16)
+    rec = po.cpu().numpy()
+    assert np.array_equal(rec[:rl, 3], R[:, 0]) and rec[rl, 3] == 0.0
+    assert np.array_equal(rec[:, :3], got[:, :3])
     AB = pb[16 * rl:].reshape(rl, 16, 4)
     assert np.array_equal(R, T[:, :, 4].T)
     assert np.array_equal(AB, np.transpose(T[:, :, :4], (1, 0, 2)))
