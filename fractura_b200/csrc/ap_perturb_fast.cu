@@ -1,5 +1,5 @@
 // ap_perturb_fast.cu -- the per-frame coarse-pass kernel over coarse_pixel
-// (ap_coarse.cuh): one thread per pixel on 16 x 16 tiles.  Picked by
+// (ap_coarse.cuh): one thread per pixel on 16 x 16 tiles, 8 x 4 pixels per warp.  Picked by
 // ap_render_pass for AP_TIER_PERTURB coarse passes without in-kernel colour
 // when the buffers carry the packed orbit and, with BLA, the packed table.
 #include "ap_coarse.cuh"
@@ -9,8 +9,11 @@ namespace ap {
 template <int ARITH, int FT, bool BLA>
 __global__ void __launch_bounds__(256, 4) perturb_coarse_kernel(const ApFrameParams p,
                                                                 const ApFrameBuffers b) {
-    const int i = blockIdx.x * 16 + (threadIdx.x & 15);
-    const int j = blockIdx.y * 16 + (threadIdx.x >> 4);
+    // each warp takes an 8 x 4 patch of its block's 16 x 16 pixels: neighbours
+    // follow similar paths through the loop, so compact warps diverge less
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int i = blockIdx.x * 16 + (w & 1) * 8 + (l & 7);
+    const int j = blockIdx.y * 16 + (w >> 1) * 4 + (l >> 3);
     if (i >= p.width || j >= p.height) return;
     coarse_pixel<ARITH, FT, BLA>(p, b, i, j);
 }
