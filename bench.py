@@ -176,11 +176,19 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
+        out = self._summary(t0, t1 + 0.05)
+        if out["samples"] == 0:
+            # a timed region shorter than the sampling interval: the samples nearest to it
+            out = self._summary(t0 - 0.1, t1 + 0.1)
+            out["window"] = "timed region +-100 ms (shorter than the sampling interval)"
+        return out
+
+    def _summary(self, t0, t1):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        t0, t1 = getattr(self, "t0", 0.0), getattr(self, "t1", float("inf"))
         for ts, ln in self.lines:
-            if not (t0 <= ts <= t1 + 0.05):
+            if not (t0 <= ts <= t1):
                 continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
