@@ -244,9 +244,11 @@ def _warm_orbit(t):
     pw = Decimal(t.width)
     with localcontext(decimal_context(pw)):
         ph = pw * (Decimal(t.H) / Decimal(t.W))
+    # tiles run in parallel already: no speculative probe beside each centre orbit
     return hp.find_optimal_reference_orbit(
         Decimal(t.cx), Decimal(t.cy), pw, ph, t.max_iter, t.W, t.H, fractal_type=t.fractal_type,
-        julia_cx=t.julia_cx, julia_cy=t.julia_cy, gen_n=t.gen_n, gen_kr=t.gen_kr, gen_ki=t.gen_ki)
+        julia_cx=t.julia_cx, julia_cy=t.julia_cy, gen_n=t.gen_n, gen_kr=t.gen_kr, gen_ki=t.gen_ki,
+        speculate=False)
 
 
 # ------------------------------------------------------------------ tuner

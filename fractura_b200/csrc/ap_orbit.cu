@@ -291,7 +291,7 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
         add(mag, zx2, zy2, L);
         if (!mag.neg && cmp_mag(mag.m, bail.m, L) > 0) {
             len = k;
-            if (escape_only && escape_mag2) *escape_mag2 = to_double(mag, L, I);
+            if (escape_mag2) *escape_mag2 = to_double(mag, L, I);
             break;
         }
         if (periodic) {

@@ -88,7 +88,20 @@ def _native():
 
 
 _PAIR_POOL = None
+_PROBE_POOL = None
 _PAIR_LOCK = threading.Lock()
+
+
+def _probe_pool():
+    """Threads for the centre orbit and the probe candidates of
+    find_optimal_reference_orbit (one task per orbit pair; the native runs release
+    the GIL)."""
+    global _PROBE_POOL
+    with _PAIR_LOCK:
+        if _PROBE_POOL is None:
+            _PROBE_POOL = ThreadPoolExecutor(max_workers=max(2, os.cpu_count() or 4),
+                                             thread_name_prefix="probe")
+        return _PROBE_POOL
 
 
 def _pair_pool():
@@ -101,7 +114,7 @@ def _pair_pool():
         return _PAIR_POOL
 
 
-def _native_orbit(seeds_fn, L, max_iter, fractal_type, gen_n):
+def _native_orbit(seeds_fn, L, max_iter, fractal_type, gen_n, with_mag2=False):
     import ctypes as C
     from . import _lib
     I = orbit_int_limbs(fractal_type, gen_n)
@@ -109,10 +122,13 @@ def _native_orbit(seeds_fn, L, max_iter, fractal_type, gen_n):
     ref_re = np.zeros(max_iter + 1, dtype=np.float64)
     ref_im = np.zeros(max_iter + 1, dtype=np.float64)
     ref_len = C.c_int32(0)
+    mag2 = C.c_double(0.0)
     _lib.check(_native().ap_reference_orbit(
         seeds.ctypes.data_as(C.c_void_p), L, I, int(fractal_type), int(gen_n), int(max_iter), 0,
         ref_re.ctypes.data_as(C.c_void_p), ref_im.ctypes.data_as(C.c_void_p), C.byref(ref_len),
-        None, None), "ap_reference_orbit")
+        C.byref(mag2), None), "ap_reference_orbit")
+    if with_mag2:
+        return ref_re, ref_im, int(ref_len.value), float(mag2.value)
     return ref_re, ref_im, int(ref_len.value)
 
 
@@ -180,6 +196,12 @@ def compute_highprec_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
         return decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy,
                                      prec_bits, gen_n, gen_kr, gen_ki)
     k, mag2, _ = a
+    return _smooth_escape(k, mag2, max_iter, fractal_type, gen_n)
+
+
+def _smooth_escape(k, mag2, max_iter, fractal_type, gen_n):
+    """The escape scalar of math_core/high_precision.py:581-703 from the escape step
+    and |Z|^2 there (max_iter when the orbit stays bounded)."""
     if k >= max_iter:
         return float(max_iter)
     inv_n = (1.0 / math.log(float(gen_n))) if (fractal_type == 4 and gen_n > 1) else float(INV_LN2_F32)
@@ -187,6 +209,27 @@ def compute_highprec_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
     if log_mag > 1.0:
         return float(k + 1.0) - (math.log(0.5 * log_mag) - LN_BAILOUT_LOG) * inv_n
     return float(k)
+
+
+def probe_candidate(cand_cx, cand_cy, max_iter, fractal_type=0, julia_cx=0.0, julia_cy=0.0,
+                    prec_bits=256, gen_n=3, gen_kr=0.25, gen_ki=1.0):
+    """(escape scalar, orbit) of one probe candidate: the value
+    compute_highprec_escape_scalar returns and the orbit compute_single_highprec_orbit
+    returns, from one pair of certified native runs (orbit None when the runs
+    disagree; the escape scalar is then the exact Decimal one)."""
+    lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+
+    def seeds(L, I):
+        return _seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki, L, I)
+
+    a = _native_orbit(seeds, hi, max_iter, fractal_type, gen_n, with_mag2=True)
+    b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n, with_mag2=True)
+    n = a[2] + 1
+    if (a[2] == b[2] and (a[2] >= max_iter or a[3] == b[3]) and np.array_equal(a[0][:n], b[0][:n])
+            and np.array_equal(a[1][:n], b[1][:n])):
+        return _smooth_escape(a[2], a[3], max_iter, fractal_type, gen_n), a[:3]
+    return decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
+                                 gen_n, gen_kr, gen_ki), None
 
 
 # Exact Decimal iteration in the reference's operation order: the path for orbits the
@@ -313,12 +356,14 @@ PROBE_UV = [
 
 def find_optimal_reference_orbit(cx_dec, cy_dec, pw_dec, ph_dec, max_iter, screen_w, screen_h,
                                  fractal_type=0, julia_cx=0.0, julia_cy=0.0,
-                                 gen_n=3, gen_kr=0.25, gen_ki=1.0, is_floatexp=False):
+                                 gen_n=3, gen_kr=0.25, gen_ki=1.0, is_floatexp=False, speculate=True):
     """Reference orbit for a view: cached, at the centre, or at the best of 16 probes.
 
     Returns (cx_dec, cy_dec, u, v, ref_re, ref_im, ref_len) where (u, v) is the
     reference's position in the view as fractions of its width and height
-    (math_core/high_precision.py:919-1097).
+    (math_core/high_precision.py:919-1097).  With ``speculate`` the probe runs beside
+    the centre's orbit (its work is wasted when the centre's orbit is long enough);
+    without, only after it, as the reference does.  The result is the same.
     """
     ctx = decimal_context(pw_dec)
     with localcontext(ctx):
@@ -363,37 +408,52 @@ def find_optimal_reference_orbit(cx_dec, cy_dec, pw_dec, ph_dec, max_iter, scree
                         best_entry["ref_im"], min(best_entry["ref_len"], max_iter))
 
         bits = compute_required_prec_bits(pw_dec)
-        ref_re, ref_im, ref_len = compute_single_highprec_orbit(
-            cx_dec, cy_dec, max_iter, fractal_type, julia_cx, julia_cy, bits,
-            gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki)
-        best_cx, best_cy, best_u, best_v = cx_dec, cy_dec, 0.5, 0.5
+        # The probe of 16 candidates (needed when the centre's orbit escapes before
+        # 0.6 max_iter, the usual case deep in a zoom) runs beside the centre's orbit,
+        # and each candidate keeps its certified orbit, so the winner is not iterated
+        # twice.  Results and choice are those of the sequential reference.
+        pool = _probe_pool()
+        centre = pool.submit(compute_single_highprec_orbit, cx_dec, cy_dec, max_iter, fractal_type,
+                             julia_cx, julia_cy, bits, gen_n, gen_kr, gen_ki)
+        probes = []
 
-        if ref_len < int(max_iter * 0.6) and pw_dec >= Decimal("1e-10000"):
-            def probe(uv):
-                u, v = uv
+        def submit_probes():
+            for (u, v) in PROBE_UV:
                 with localcontext(ctx):
                     cand_x = x_min_dec + Decimal(str(u)) * pw_dec
                     cand_y = y_max_dec - Decimal(str(v)) * ph_dec
-                esc = compute_highprec_escape_scalar(cand_x, cand_y, max_iter, fractal_type,
-                                                     julia_cx, julia_cy, bits, gen_n, gen_kr, gen_ki)
-                return esc, cand_x, cand_y, u, v
+                probes.append((pool.submit(probe_candidate, cand_x, cand_y, max_iter, fractal_type,
+                                           julia_cx, julia_cy, bits, gen_n, gen_kr, gen_ki),
+                               cand_x, cand_y, u, v))
 
-            workers = min(len(PROBE_UV), os.cpu_count() or 4)
-            with ThreadPoolExecutor(max_workers=workers) as ex:
-                results = list(ex.map(probe, PROBE_UV))
+        may_probe = pw_dec >= Decimal("1e-10000")
+        if may_probe and speculate:
+            submit_probes()
+        ref_re, ref_im, ref_len = centre.result()
+        best_cx, best_cy, best_u, best_v = cx_dec, cy_dec, 0.5, 0.5
+
+        if ref_len < int(max_iter * 0.6) and may_probe:
+            if not probes:
+                submit_probes()
             best_esc = max(int(ref_len * 1.2), ref_len + 32)
-            cand = (cx_dec, cy_dec, 0.5, 0.5)
-            for esc, cand_x, cand_y, u, v in results:
+            cand, cand_orbit = (cx_dec, cy_dec, 0.5, 0.5), None
+            for fut, cand_x, cand_y, u, v in probes:
+                esc, orbit = fut.result()
                 if esc > best_esc:
                     best_esc = esc
-                    cand = (cand_x, cand_y, u, v)
+                    cand, cand_orbit = (cand_x, cand_y, u, v), orbit
             if cand[0] != cx_dec or cand[1] != cy_dec:
-                c_re, c_im, c_len = compute_single_highprec_orbit(
-                    cand[0], cand[1], max_iter, fractal_type, julia_cx, julia_cy, bits,
-                    gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki)
+                if cand_orbit is None:
+                    cand_orbit = compute_single_highprec_orbit(
+                        cand[0], cand[1], max_iter, fractal_type, julia_cx, julia_cy, bits,
+                        gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki)
+                c_re, c_im, c_len = cand_orbit
                 if c_len > ref_len:
                     ref_re, ref_im, ref_len = c_re, c_im, c_len
                     best_cx, best_cy, best_u, best_v = cand
+        else:
+            for fut, *_ in probes:
+                fut.cancel()  # not needed: drop those not started
 
         if can_reuse and best_entry is not None and best_entry["ref_len"] > ref_len:
             u = float((best_entry["cx_dec"] - x_min_dec) / pw_dec)

@@ -300,7 +300,8 @@ AP_API int ap_bbsa_coeffs(const double* ref_re, const double* ref_im, int32_t re
  * escape_only = 0: ref_re/ref_im (max_iter + 1 float64 each) receive the orbit rounded
  * to nearest, *ref_len the step at which |Z|^2 > 65536 (max_iter if none; an exactly
  * repeating Mandelbrot/Julia orbit found at power-of-two checkpoints is copied to the
- * end).  escape_only = 1: no arrays; *ref_len = escape step, *escape_mag2 = |Z|^2 there.
+ * end).  escape_only = 1: no arrays, *ref_len = escape step.  escape_mag2 (optional):
+ * |Z|^2 at the escape step, rounded to float64 (left as is when the orbit never escapes).
  * trace_hash (optional): a hash of the float64 values of every Z_k up to the escape, so
  * that runs at two precisions can confirm they followed the same float64 trajectory. */
 AP_API int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_limbs,
