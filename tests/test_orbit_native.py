@@ -52,6 +52,12 @@ def test_orbits_equal_decimal(formula, prec_bits):
         ea = hp.compute_highprec_escape_scalar(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
         eb = hp.decimal_escape_scalar(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
         assert ea == eb
+        # the probe's single pair of runs gives the same value and, when certified,
+        # the same orbit
+        ep, orbit = hp.probe_candidate(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
+        assert ep == eb
+        if orbit is not None:
+            assert orbit[2] == b[2] and np.array_equal(orbit[0], b[0]) and np.array_equal(orbit[1], b[1])
 
 
 @pytest.mark.parametrize("c", [("0", "0"), ("-1", "0"), ("0", "1"), ("-0.1", "0.1"),
@@ -80,6 +86,47 @@ def test_uncertified_orbit_takes_the_decimal_path():
     got = hp.compute_single_highprec_orbit(cx, cy, 3000, 1, 0.0, 0.0, 256)
     ref = hp.decimal_orbit(cx, cy, 3000, 1, 0.0, 0.0, 256)
     assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+    esc, orbit = hp.probe_candidate(cx, cy, 3000, 1, 0.0, 0.0, 256)
+    assert orbit is None and esc == hp.decimal_escape_scalar(cx, cy, 3000, 1, 0.0, 0.0, 256)
+
+
+SEARCH_VIEWS = {  # centre kept / a probe candidate wins (its orbit is reused)
+    "mandelbrot": ("-0.7436438870371587", "0.1318259042053119", "1e-12", 0, 20000),
+    "ship": ("-1.7692733407791943", "0.01796380726768093", "2e-14", 1, 6000),
+}
+
+
+@pytest.mark.parametrize("view", sorted(SEARCH_VIEWS))
+@pytest.mark.parametrize("speculate", [False, True])
+def test_reference_search_is_the_sequential_one(view, speculate):
+    """find_optimal_reference_orbit, with the probe beside the centre orbit or after
+    it, picks the reference the sequential Decimal search picks, with its orbit."""
+    cxs, cys, ws, ft, mi = SEARCH_VIEWS[view]
+    cx, cy, pw = Decimal(cxs), Decimal(cys), Decimal(ws)
+    ph = pw * Decimal(9) / Decimal(16)
+    hp.clear_reference_orbit_cache()
+    got = hp.find_optimal_reference_orbit(cx, cy, pw, ph, mi, 160, 90, fractal_type=ft, speculate=speculate)
+    hp.clear_reference_orbit_cache()
+    bits = hp.compute_required_prec_bits(pw)
+    centre = hp.decimal_orbit(cx, cy, mi, ft, 0.0, 0.0, bits)
+    assert centre[2] < int(0.6 * mi)  # the probe decides
+    best_esc, best = max(int(centre[2] * 1.2), centre[2] + 32), None
+    x_min, y_max = cx - pw / 2, cy + ph / 2
+    for u, v in hp.PROBE_UV:
+        x, y = x_min + Decimal(str(u)) * pw, y_max - Decimal(str(v)) * ph
+        e = hp.decimal_escape_scalar(x, y, mi, ft, 0.0, 0.0, bits)
+        if e > best_esc:
+            best_esc, best = e, (x, y, u, v)
+    want = centre
+    if best is not None:
+        cand = hp.decimal_orbit(best[0], best[1], mi, ft, 0.0, 0.0, bits)
+        if cand[2] > centre[2]:
+            want = cand
+            assert (got[0], got[1], got[2], got[3]) == best
+    assert (best is not None) == (view == "ship")
+    assert got[6] == want[2]
+    assert np.array_equal(got[4][:want[2] + 1], want[0][:want[2] + 1])
+    assert np.array_equal(got[5][:want[2] + 1], want[1][:want[2] + 1])
 
 
 def test_fixed_point_conversion():
