@@ -15,6 +15,7 @@ a shared counter.  Each tile's values equal the per-frame coarse pass
     batch.tiles_out[t]["iter"]              # [H, W] float32 smooth values on the device
 """
 import ctypes as C
+import os
 import threading
 from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
@@ -132,18 +133,17 @@ class PreparedBatch:
         return tot
 
 
-def _tile_inputs(t, cpu_sem, bla_form, torch, stream, L, scratch):
-    """Orbit, packed records, BLA rows, outputs and parameters of one tile, as the
-    coarse pass of render_perturbation_frame sets them (factor 1, one reference)."""
+def _tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch):
+    """Packed records, BLA rows, outputs and parameters of one tile around its
+    reference `ref` (find_optimal_reference_orbit's result), as the coarse pass of
+    render_perturbation_frame sets them (factor 1, one reference)."""
     from .perturbation import max_delta_c
     pw = Decimal(t.width)
     with localcontext(decimal_context(pw)):
         ph = pw * (Decimal(t.H) / Decimal(t.W))
         dx = float(pw / Decimal(max(1, t.W - 1)))
         dy = float(ph / Decimal(max(1, t.H - 1)))
-    bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
-        Decimal(t.cx), Decimal(t.cy), pw, ph, t.max_iter, t.W, t.H, fractal_type=t.fractal_type,
-        julia_cx=t.julia_cx, julia_cy=t.julia_cy, gen_n=t.gen_n, gen_kr=t.gen_kr, gen_ki=t.gen_ki)
+    bcx, bcy, bu, bv, re, im, rl = ref
     n = rl + 1
     d_re = torch.from_numpy(np.ascontiguousarray(re[:n])).to("cuda", non_blocking=False)
     d_im = torch.from_numpy(np.ascontiguousarray(im[:n])).to("cuda", non_blocking=False)
@@ -185,7 +185,7 @@ def _tile_inputs(t, cpu_sem, bla_form, torch, stream, L, scratch):
     return p, orbit, bla_packed, out, (d_re, d_im), rl
 
 
-def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, workers=8):
+def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, workers=None):
     """Host and device preparation of a batch: reference orbits (in parallel threads;
     the native orbit code releases the GIL), device BLA tables, packed records,
     outputs and the descriptor array, ordered by estimated cost (pixels x ref_len)."""
@@ -200,10 +200,10 @@ def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, wor
     L = _lib.load()
     stream = stream or torch.cuda.current_stream()
     b = PreparedBatch(list(tiles), abi.AP_ARITH_REF_CPU if cpu_sem else abi.AP_ARITH_REF_CUDA, stream)
-    # the orbits first, concurrently (host work)
-    with ThreadPoolExecutor(max_workers=max(1, workers)) as ex:
-        orbits = list(ex.map(lambda t: _warm_orbit(t), b.tiles))
-    del orbits
+    # the orbits first, concurrently (host work), each once: a batch can hold more
+    # tiles than the orbit cache keeps
+    with ThreadPoolExecutor(max_workers=max(1, workers or os.cpu_count() or 8)) as ex:
+        refs = list(ex.map(_warm_orbit, b.tiles))
     scratch_box = {}
     lock = threading.Lock()
 
@@ -216,8 +216,8 @@ def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, wor
 
     recs = []
     with torch.cuda.stream(stream):
-        for t in b.tiles:
-            recs.append(_tile_inputs(t, cpu_sem, bla_form, torch, stream, L, scratch))
+        for t, ref in zip(b.tiles, refs):
+            recs.append(_tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch))
     stream.synchronize()
     cost = [t.W * t.H * max(1, r[5]) for t, r in zip(b.tiles, recs)]
     b.order = sorted(range(len(b.tiles)), key=lambda q: -cost[q])
@@ -240,7 +240,7 @@ def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, wor
 
 
 def _warm_orbit(t):
-    """Compute (and cache) a tile's reference orbit on the host."""
+    """A tile's reference orbit (find_optimal_reference_orbit), computed on the host."""
     pw = Decimal(t.width)
     with localcontext(decimal_context(pw)):
         ph = pw * (Decimal(t.H) / Decimal(t.W))
