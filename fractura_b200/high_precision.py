@@ -304,10 +304,59 @@ def decimal_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
     return ref_re, ref_im, ref_len
 
 
+def _dec_parts(d):
+    """(sign, exponent, base-1e8 limbs, little-endian) of a finite Decimal."""
+    t = d.as_tuple()
+    digits = "".join(map(str, t.digits)) or "0"
+    return t.sign, int(t.exponent), [int(digits[max(0, i - 8):i]) for i in range(len(digits), 0, -8)]
+
+
 def decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
-                                   julia_cx=0.0, julia_cy=0.0, prec_bits=256,
-                                   gen_n=3, gen_kr=0.25, gen_ki=1.0):
-    """Smooth escape value of one point in Decimal arithmetic (max_iter if it stays bounded)."""
+                          julia_cx=0.0, julia_cy=0.0, prec_bits=256,
+                          gen_n=3, gen_kr=0.25, gen_ki=1.0):
+    """Smooth escape value of one point in Decimal arithmetic (max_iter if it stays
+    bounded): the loop of math_core/high_precision.py:581-703, run natively
+    (ap_decimal_escape, the decimal module's arithmetic without the Python lock) and
+    in Python only for operands longer than the native code holds."""
+    import ctypes as C
+    from . import _lib
+    ctx = _orbit_context(prec_bits)
+    zx, zy, c_x, c_y = _start(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy)
+    seeds = [zx, zy, c_x, c_y, Decimal(str(gen_kr)), Decimal(str(gen_ki))]
+    parts = [_dec_parts(v) for v in seeds]
+    stride = max(len(p[2]) for p in parts)
+    if stride <= 200:
+        meta = np.array([[p[0], p[1], len(p[2])] for p in parts], dtype=np.int64)
+        limbs = np.zeros((6, stride), dtype=np.uint64)
+        for q, p in enumerate(parts):
+            limbs[q, :len(p[2])] = p[2]
+        k = C.c_int32(0)
+        mag_meta = np.zeros(3, dtype=np.int64)
+        mag_limbs = np.zeros(400, dtype=np.uint64)
+        rc = _native().ap_decimal_escape(
+            meta.ctypes.data_as(C.c_void_p), limbs.ctypes.data_as(C.c_void_p), int(stride), int(ctx.prec),
+            int(fractal_type), int(gen_n), int(max_iter), C.byref(k), mag_meta.ctypes.data_as(C.c_void_p),
+            mag_limbs.ctypes.data_as(C.c_void_p))
+        if rc == 0:
+            if k.value >= max_iter:
+                return float(max_iter)
+            n = int(mag_meta[2])
+            coef = "".join(f"{int(x):08d}" for x in mag_limbs[:n][::-1]).lstrip("0") or "0"
+            mag2 = Decimal((int(mag_meta[0]), tuple(int(ch) for ch in coef), int(mag_meta[1])))
+            inv_n = (1.0 / math.log(float(gen_n))) if (fractal_type == 4 and gen_n > 1) else float(INV_LN2_F32)
+            log_mag = math.log(float(mag2))
+            if log_mag > 1.0:
+                return float(k.value + 1.0) - (math.log(0.5 * log_mag) - LN_BAILOUT_LOG) * inv_n
+            return float(k.value)
+        _lib.last_error()  # clear: the Python loop below serves the call
+    return decimal_escape_scalar_py(cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
+                                    gen_n, gen_kr, gen_ki)
+
+
+def decimal_escape_scalar_py(cand_cx, cand_cy, max_iter, fractal_type=0,
+                             julia_cx=0.0, julia_cy=0.0, prec_bits=256,
+                             gen_n=3, gen_kr=0.25, gen_ki=1.0):
+    """The same loop in Python's decimal module (operands of any length)."""
     with localcontext(_orbit_context(prec_bits)):
         bailout = Decimal(65536)
         two = Decimal(2)

@@ -310,6 +310,24 @@ AP_API int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_
                               double* ref_re, double* ref_im, int32_t* ref_len,
                               double* escape_mag2, uint64_t* trace_hash);
 
+/* The escape iteration of compute_highprec_escape_scalar in Decimal arithmetic
+ * (math_core/high_precision.py:581-703, its decimal-module branch), on the host: for
+ * the points whose fixed-point runs disagree.  Values are (-1)^neg coef 10^exp with
+ * coef in base-1e8 limbs, little-endian, one per uint64.  meta: 6 x (neg, exp, n) for
+ * z0_re, z0_im, c_re, c_im, K_re, K_im (any number of digits up to 1600); limbs: 6 x
+ * limb_stride (<= 200).  Every +, - and * is exact, then rounded to prec significant
+ * digits, half to even; abs() rounds too.  *k_out = the escape step (|Z|^2 > 65536)
+ * or max_iter; mag2_meta/mag2_limbs (3 and 400 entries) = |Z|^2 there. */
+AP_API int ap_decimal_escape(const int64_t* meta, const uint64_t* limbs, int32_t limb_stride,
+                             int32_t prec, int32_t fractal_type, int32_t gen_n, int32_t max_iter,
+                             int32_t* k_out, int64_t* mag2_meta, uint64_t* mag2_limbs);
+
+/* One operation of that arithmetic (op 0 add, 1 subtract, 2 multiply, 3 compare into
+ * *cmp_out), for checking it against the decimal module; out: 3 + 400 entries. */
+AP_API int ap_decimal_arith(int32_t op, const int64_t* a_meta, const uint64_t* a_limbs,
+                            const int64_t* b_meta, const uint64_t* b_limbs, int32_t prec,
+                            int64_t* out_meta, uint64_t* out_limbs, int32_t* cmp_out);
+
 /* Batches (no single counterpart: the reference renders tile by tile, e.g.
  * workers/image_workers.py:428-601 calling render_frame_ssaa per tile).
  * ap_batch_plan (HOST): checks every tile of host_tiles[n] and writes first_patch[n + 1],
