@@ -5,12 +5,12 @@
 // BLA rows, no in-kernel colour) with its own parameters and outputs.  Each
 // tile is cut into patches of patch_w x patch_h = 256 pixels; patches are
 // numbered tile after tile (the host orders tiles by estimated cost, largest
-// first).  The grid holds blocks_per_sm blocks per SM for the whole batch; a
-// block takes the next patch number from one global counter (atomicAdd), looks
-// its tile up by binary search over the tiles' first patch numbers, evaluates
-// the patch with coarse_pixel (the per-frame kernel's code, so values are
-// identical) and takes the next, until the counter passes the last patch.
-// Nothing waits on anything: a block that finds the queue empty exits.
+// first).  The grid holds blocks_per_sm blocks per SM for the whole batch; each
+// warp takes the next eighth of a patch (32 pixels) from one global counter
+// (atomicAdd), looks its tile up by binary search over the tiles' first patch
+// numbers, evaluates its pixels with coarse_pixel (the per-frame kernel's code, so
+// values are identical) and takes the next, until the counter passes the end.
+// Nothing waits on anything: a warp that finds the queue empty exits.
 #include "ap_coarse.cuh"
 
 namespace ap {
@@ -54,15 +54,18 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const ApTileDesc* __re
                                                           const int64_t* __restrict__ first,
                                                           int n, int patch_w, int patch_h,
                                                           unsigned long long* head) {
-    __shared__ long long item_s;
-    const long long total = first[n];
-    const int tx = threadIdx.x % patch_w, ty = threadIdx.x / patch_w;
+    // Each warp takes the next eighth of a patch (32 of its 256 pixels) on its own:
+    // a warp that finishes early does not wait for the slow warps of its block.
+    const long long total = first[n] * 8;
+    const int lane = threadIdx.x & 31;
     for (;;) {
-        if (threadIdx.x == 0) item_s = (long long)atomicAdd(head, 1ULL);
-        __syncthreads();
-        const long long item = item_s;
-        __syncthreads();
-        if (item >= total) break;
+        unsigned long long got = 0;
+        if (lane == 0) got = atomicAdd(head, 1ULL);
+        const long long unit = (long long)__shfl_sync(0xffffffffu, got, 0);
+        if (unit >= total) break;
+        const long long item = unit >> 3;  // the patch
+        const int q = (int)(unit & 7) * 32 + lane;  // pixel of the patch, row-major
+        const int tx = q % patch_w, ty = q / patch_w;
         int lo = 0, hi = n - 1;  // last tile whose first patch <= item
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
