@@ -12,6 +12,7 @@
 // uint64, little-endian).  Every operation forms the exact result, then rounds it;
 // operands keep all their digits (inputs may carry more than P), as Decimal's do.
 // Results only depend on values, never on the representation's trailing zeros.
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 
@@ -285,6 +286,242 @@ void load(Dec& a, const int64_t* meta, const uint64_t* limbs) {  // meta: neg, e
     trim(a);
 }
 
+// The iteration state of one point: z, c, K and the scratch of a step.
+struct Orbit {
+    Dec zx, zy, cx, cy, kr, ki, zx2, zy2, mag, t0, t1, t2, nr, ni, two, bail;
+};
+
+bool load_seeds(Orbit& o, const int64_t* meta, const uint64_t* limbs, int stride) {
+    for (int q = 0; q < 6; ++q)
+        if (meta[3 * q + 2] < 1 || meta[3 * q + 2] > stride) {
+            ap::set_error("decimal iteration: operand %d has %lld limbs (1..%d)", q, (long long)meta[3 * q + 2],
+                          stride);
+            return false;
+        }
+    load(o.zx, meta, limbs);
+    load(o.zy, meta + 3, limbs + stride);
+    load(o.cx, meta + 6, limbs + 2 * stride);
+    load(o.cy, meta + 9, limbs + 3 * stride);
+    load(o.kr, meta + 12, limbs + 4 * stride);
+    load(o.ki, meta + 15, limbs + 5 * stride);
+    o.two.neg = 0; o.two.exp = 0; o.two.n = 1; o.two.d[0] = 2;
+    o.bail.neg = 0; o.bail.exp = 0; o.bail.n = 1; o.bail.d[0] = 65536;
+    return true;
+}
+
+// zx2, zy2 = zx^2, zy^2 and mag = zx2 + zy2 (the bailout test's operand)
+bool squares(Orbit& o, int P) {
+    return mul(o.zx2, o.zx, o.zx, P) && mul(o.zy2, o.zy, o.zy, P) && add(o.mag, o.zx2, o.zy2, false, P);
+}
+
+// z <- f(z) in the reference's operation order (math_core/high_precision.py:660-700),
+// from z and its squares
+bool step(Orbit& o, int fractal_type, int gen_n, int P) {
+    bool ok = true;
+    if (fractal_type == 0 || fractal_type == 2) {        // zy = two*zx*zy + cy; zx = zx2 - zy2 + cx
+        ok &= mul(o.t0, o.two, o.zx, P) && mul(o.t1, o.t0, o.zy, P) && add(o.zy, o.t1, o.cy, false, P);
+        ok &= add(o.t2, o.zx2, o.zy2, true, P) && add(o.zx, o.t2, o.cx, false, P);
+    } else if (fractal_type == 1 || fractal_type == 3) { // zy = two*|zx|*|zy| - cy
+        copy(o.t2, o.zx);
+        o.t2.neg = 0;
+        round_p(o.t2, P);  // abs() rounds to the context
+        ok &= mul(o.t0, o.two, o.t2, P);
+        copy(o.t2, o.zy);
+        o.t2.neg = 0;
+        round_p(o.t2, P);
+        ok &= mul(o.t1, o.t0, o.t2, P) && add(o.zy, o.t1, o.cy, true, P);
+        ok &= add(o.t2, o.zx2, o.zy2, true, P) && add(o.zx, o.t2, o.cx, false, P);
+    } else {                                             // z^n + K z + c
+        copy(o.nr, o.zx);
+        copy(o.ni, o.zy);
+        for (int t = 0; t < gen_n - 1 && ok; ++t) {
+            ok &= mul(o.t0, o.nr, o.zx, P) && mul(o.t1, o.ni, o.zy, P) && add(o.t2, o.t0, o.t1, true, P);
+            ok &= mul(o.t0, o.nr, o.zy, P) && mul(o.t1, o.ni, o.zx, P) && add(o.ni, o.t0, o.t1, false, P);
+            copy(o.nr, o.t2);
+        }
+        Dec& kzr = o.zx2;  // the squares are not needed any more in this step
+        Dec& kzi = o.zy2;
+        ok &= mul(o.t0, o.kr, o.zx, P) && mul(o.t1, o.ki, o.zy, P) && add(kzr, o.t0, o.t1, true, P);
+        ok &= mul(o.t0, o.kr, o.zy, P) && mul(o.t1, o.ki, o.zx, P) && add(kzi, o.t0, o.t1, false, P);
+        ok &= add(o.t0, o.nr, kzr, false, P) && add(o.zx, o.t0, o.cx, false, P);
+        ok &= add(o.t1, o.ni, kzi, false, P) && add(o.zy, o.t1, o.cy, false, P);
+    }
+    return ok;
+}
+
+// ---------------------------------------------------------------- to float64
+// float(Decimal) is the correctly rounded double (CPython converts the decimal
+// string).  Here: the top 36 digits T (and whether any digit below is nonzero)
+// bound the value in [T, T + 1) 10^q; with a 256-bit lower bound M 2^-S of 10^q
+// the value lies in [T M, (T + s) (M + 4|q| + 4)] 2^-S (s = 1 when digits were dropped).  When both ends round to the same double, so
+// does the value; otherwise (a tie, or a value within ~2^-110 of one) the caller
+// takes the decimal module's conversion.  (The table's lower bounds lose at most
+// 2^-254 relative per power of ten, so 10^q 2^S lies in [M, M + 4|q| + 4].)
+
+using u128 = unsigned __int128;
+constexpr int kPowMax = 420;  // 10^-q for q <= 420: every normal double's range
+
+struct Pow10Table {
+    uint64_t m[kPowMax + 1][4];
+    int s[kPowMax + 1];
+    Pow10Table() {
+        uint64_t cur[4] = {0, 0, 0, 1ull << 63};  // 2^255: 10^0 = 2^255 2^-255
+        int S = 255;
+        for (int q = 0; q <= kPowMax; ++q) {
+            std::memcpy(m[q], cur, sizeof cur);
+            s[q] = S;
+            // next = cur * 16 / 10, renormalised to [2^255, 2^256), truncated (a lower bound)
+            uint64_t w[5] = {cur[0] << 4, (cur[1] << 4) | (cur[0] >> 60), (cur[2] << 4) | (cur[1] >> 60),
+                             (cur[3] << 4) | (cur[2] >> 60), cur[3] >> 60};
+            u128 rem = 0;
+            for (int i = 4; i >= 0; --i) {
+                const u128 x = (rem << 64) | w[i];
+                w[i] = (uint64_t)(x / 10);
+                rem = x % 10;
+            }
+            S += 4;
+            if (w[4]) {  // 2^256 <= value: drop one bit
+                for (int i = 0; i < 4; ++i) w[i] = (w[i] >> 1) | (w[i + 1] << 63);
+                S -= 1;
+            }
+            std::memcpy(cur, w, sizeof cur);
+        }
+    }
+};
+
+const Pow10Table& pow10_table() {
+    static const Pow10Table t;  // built once (thread-safe initialisation)
+    return t;
+}
+
+int bitlen(const uint64_t* x, int n) {
+    for (int i = n - 1; i >= 0; --i)
+        if (x[i]) return 64 * i + 64 - __builtin_clzll(x[i]);
+    return 0;
+}
+
+inline int bit(const uint64_t* x, int i) { return (int)((x[i >> 6] >> (i & 63)) & 1); }
+
+// bits [lo, lo + count) of X (count <= 64, lo >= 0, inside n limbs)
+inline uint64_t bits_at(const uint64_t* x, int n, int lo, int count) {
+    const int li = lo >> 6, sh = lo & 63;
+    uint64_t w = x[li] >> sh;
+    if (sh && li + 1 < n) w |= x[li + 1] << (64 - sh);
+    return count == 64 ? w : (w & ((1ull << count) - 1));
+}
+
+// any of bits [0, k) of X set
+inline bool any_below(const uint64_t* x, int k) {
+    const int full = k >> 6;
+    for (int i = 0; i < full; ++i)
+        if (x[i]) return true;
+    const int rest = k & 63;
+    return rest && (x[full] & ((1ull << rest) - 1));
+}
+
+// Round X 2^-S (X: n limbs) to the nearest double, half to even; false outside the
+// normal range.
+bool round_to_double(const uint64_t* x, int n, int S, double* out) {
+    const int b = bitlen(x, n);
+    if (b == 0) {
+        *out = 0.0;
+        return true;
+    }
+    const int e2 = b - 1 - S;
+    if (e2 < -1022 || e2 > 1023) return false;
+    if (b <= 53) {  // exact
+        *out = std::ldexp((double)x[0], -S);
+        return true;
+    }
+    int shift = b - 53;  // the mantissa's unit is 2^(shift - S)
+    uint64_t m = bits_at(x, n, shift, 53);
+    const int r = bit(x, shift - 1);
+    const bool sticky = any_below(x, shift - 1);
+    if (r && (sticky || (m & 1))) {
+        ++m;
+        if (m == (1ull << 53)) {
+            m >>= 1;
+            ++shift;
+        }
+    }
+    *out = std::ldexp((double)m, shift - S);
+    return true;
+}
+
+// a -> float64 as float(Decimal) gives it; false when the bounds do not decide.
+bool to_double(const Dec& a, double* out) {
+    if (is_zero(a)) {
+        *out = a.neg ? -0.0 : 0.0;
+        return true;
+    }
+    static thread_local Dec t;
+    copy(t, a);
+    const int64_t D = digits(t);
+    const int64_t drop = D > 36 ? D - 36 : 0;
+    bool sticky = false;
+    if (drop) {
+        const int64_t pos = drop - 1;
+        const int li = (int)(pos / kBaseDigits), di = (int)(pos % kBaseDigits);
+        sticky = (t.d[li] % (kPow10[di] * 10)) != 0;
+        for (int i = 0; i < li && !sticky; ++i) sticky = t.d[i] != 0;
+        shift_right(t, drop);
+    }
+    u128 T = 0;
+    for (int i = t.n - 1; i >= 0; --i) T = T * kBase + t.d[i];
+    const int64_t q = t.exp;
+    const uint64_t sgn = sticky ? 1 : 0;
+    double lo, hi;
+    if (q >= 0) {
+        u128 N = T;
+        for (int64_t i = 0; i < q; ++i) {
+            if (N > (~(u128)0) / 20) return false;
+            N *= 10;
+        }
+        const uint64_t x[2] = {(uint64_t)N, (uint64_t)(N >> 64)};
+        const u128 N1 = N + (sticky ? 1 : 0);
+        const uint64_t y[2] = {(uint64_t)N1, (uint64_t)(N1 >> 64)};
+        if (!round_to_double(x, 2, 0, &lo) || !round_to_double(y, 2, 0, &hi)) return false;
+    } else {
+        if (-q > kPowMax) return false;
+        const Pow10Table& P = pow10_table();
+        const uint64_t* M = P.m[-q];
+        const int S = P.s[-q];
+        uint64_t L[6] = {0, 0, 0, 0, 0, 0}, U[6] = {0, 0, 0, 0, 0, 0};
+        const uint64_t Tl[2] = {(uint64_t)T, (uint64_t)(T >> 64)};
+        const u128 T1 = T + sgn;
+        const uint64_t Tu[2] = {(uint64_t)T1, (uint64_t)(T1 >> 64)};
+        // M + 4|q| + 4: the table's truncations add at most 2^-254 relative per power
+        uint64_t Mu[4];
+        std::memcpy(Mu, M, sizeof Mu);
+        u128 c = (u128)Mu[0] + (uint64_t)(4 * (-q) + 4);
+        Mu[0] = (uint64_t)c;
+        for (int i = 1; i < 4 && (c >> 64); ++i) {
+            c = (u128)Mu[i] + 1;
+            Mu[i] = (uint64_t)c;
+        }
+        for (int i = 0; i < 2; ++i) {
+            u128 carry = 0;
+            for (int j = 0; j < 4; ++j) {
+                const u128 pl = (u128)Tl[i] * M[j] + L[i + j] + carry;
+                L[i + j] = (uint64_t)pl;
+                carry = pl >> 64;
+            }
+            L[i + 4] += (uint64_t)carry;
+            carry = 0;
+            for (int j = 0; j < 4; ++j) {
+                const u128 pu = (u128)Tu[i] * Mu[j] + U[i + j] + carry;
+                U[i + j] = (uint64_t)pu;
+                carry = pu >> 64;
+            }
+            U[i + 4] += (uint64_t)carry;
+        }
+        if (!round_to_double(L, 6, S, &lo) || !round_to_double(U, 6, S, &hi)) return false;
+    }
+    if (lo != hi) return false;
+    *out = a.neg ? -lo : lo;
+    return true;
+}
+
 }  // namespace
 
 extern "C" int ap_decimal_escape(const int64_t* meta, const uint64_t* limbs, int32_t limb_stride,
@@ -296,71 +533,102 @@ extern "C" int ap_decimal_escape(const int64_t* meta, const uint64_t* limbs, int
         ap::set_error("ap_decimal_escape: bad arguments");
         return AP_E_INVALID;
     }
-    for (int q = 0; q < 6; ++q) {
-        if (meta[3 * q + 2] < 1 || meta[3 * q + 2] > limb_stride) {
-            ap::set_error("ap_decimal_escape: operand %d has %lld limbs (1..%d)", q,
-                          (long long)meta[3 * q + 2], limb_stride);
-            return AP_E_INVALID;
-        }
-    }
-    const int P = prec;
-    // inputs: z0_re, z0_im, c_re, c_im, k_re, k_im (exact, any number of digits)
-    static thread_local Dec v[16];
-    Dec &zx = v[0], &zy = v[1], &cx = v[2], &cy = v[3], &kr = v[4], &ki = v[5];
-    Dec &zx2 = v[6], &zy2 = v[7], &mag = v[8], &t0 = v[9], &t1 = v[10], &t2 = v[11];
-    Dec &nr = v[12], &ni = v[13], &two = v[14], &bail = v[15];
-    load(zx, meta, limbs);
-    load(zy, meta + 3, limbs + limb_stride);
-    load(cx, meta + 6, limbs + 2 * limb_stride);
-    load(cy, meta + 9, limbs + 3 * limb_stride);
-    load(kr, meta + 12, limbs + 4 * limb_stride);
-    load(ki, meta + 15, limbs + 5 * limb_stride);
-    two.neg = 0; two.exp = 0; two.n = 1; two.d[0] = 2;
-    bail.neg = 0; bail.exp = 0; bail.n = 1; bail.d[0] = 65536;
+    static thread_local Orbit o;
+    if (!load_seeds(o, meta, limbs, limb_stride)) return AP_E_INVALID;
     bool ok = true;
     int k = 0;
-    for (; k < max_iter && ok; ++k) {
-        ok &= mul(zx2, zx, zx, P) && mul(zy2, zy, zy, P) && add(mag, zx2, zy2, false, P);
-        if (!ok) break;
-        if (cmp(mag, bail) > 0) break;
-        if (fractal_type == 0 || fractal_type == 2) {        // zy = two*zx*zy + cy; zx = zx2 - zy2 + cx
-            ok &= mul(t0, two, zx, P) && mul(t1, t0, zy, P) && add(zy, t1, cy, false, P);
-            ok &= add(t2, zx2, zy2, true, P) && add(zx, t2, cx, false, P);
-        } else if (fractal_type == 1 || fractal_type == 3) { // zy = two*|zx|*|zy| - cy
-            copy(t2, zx);
-            t2.neg = 0;
-            round_p(t2, P);  // abs() rounds to the context
-            ok &= mul(t0, two, t2, P);
-            copy(t2, zy);
-            t2.neg = 0;
-            round_p(t2, P);
-            ok &= mul(t1, t0, t2, P) && add(zy, t1, cy, true, P);
-            ok &= add(t2, zx2, zy2, true, P) && add(zx, t2, cx, false, P);
-        } else {                                             // z^n + k z + c
-            copy(nr, zx);
-            copy(ni, zy);
-            for (int t = 0; t < gen_n - 1 && ok; ++t) {
-                ok &= mul(t0, nr, zx, P) && mul(t1, ni, zy, P) && add(t2, t0, t1, true, P);  // next_r
-                ok &= mul(t0, nr, zy, P) && mul(t1, ni, zx, P) && add(ni, t0, t1, false, P); // next_i
-                copy(nr, t2);
-            }
-            Dec& kzr = zx2;  // zx2, zy2 are not needed any more in this step
-            Dec& kzi = zy2;
-            ok &= mul(t0, kr, zx, P) && mul(t1, ki, zy, P) && add(kzr, t0, t1, true, P);
-            ok &= mul(t0, kr, zy, P) && mul(t1, ki, zx, P) && add(kzi, t0, t1, false, P);
-            ok &= add(t0, nr, kzr, false, P) && add(zx, t0, cx, false, P);
-            ok &= add(t1, ni, kzi, false, P) && add(zy, t1, cy, false, P);
-        }
+    for (; k < max_iter; ++k) {
+        if (!(ok = squares(o, prec))) break;
+        if (cmp(o.mag, o.bail) > 0) break;
+        if (!(ok = step(o, fractal_type, gen_n, prec))) break;
     }
     if (!ok) {
         ap::set_error("ap_decimal_escape: operand too long for %d limbs", kMaxLimbs);
         return AP_E_INVALID;
     }
     *k_out = k;
-    mag2_meta[0] = mag.neg;
-    mag2_meta[1] = mag.exp;
-    mag2_meta[2] = mag.n;
-    std::memcpy(mag2_limbs, mag.d, sizeof(uint64_t) * mag.n);
+    mag2_meta[0] = o.mag.neg;
+    mag2_meta[1] = o.mag.exp;
+    mag2_meta[2] = o.mag.n;
+    std::memcpy(mag2_limbs, o.mag.d, sizeof(uint64_t) * o.mag.n);
+    return AP_OK;
+}
+
+// The orbit loop of the Decimal reference orbit (decimal_orbit: the reference's
+// Decimal iteration, math_core/high_precision.py:706-875): ref_re/ref_im (max_iter + 1
+// float64) receive float(Z_k); *ref_len = the escape step or max_iter; for Mandelbrot
+// and its Julia set an exactly repeating orbit found at power-of-two checkpoints has its
+// cycle copied to the end.  AP_E_UNSUPPORTED when a conversion is not decided by the
+// bounds (the caller then runs the decimal module's loop).
+extern "C" int ap_decimal_orbit(const int64_t* meta, const uint64_t* limbs, int32_t limb_stride,
+                                int32_t prec, int32_t fractal_type, int32_t gen_n, int32_t max_iter,
+                                double* ref_re, double* ref_im, int32_t* ref_len) {
+    if (!meta || !limbs || !ref_re || !ref_im || !ref_len || prec < 1 || prec > 1500 || limb_stride < 1 ||
+        limb_stride > kMaxLimbs / 2 || fractal_type < 0 || fractal_type > 4 ||
+        (fractal_type == 4 && (gen_n < 1 || gen_n > 64)) || max_iter < 0) {
+        ap::set_error("ap_decimal_orbit: bad arguments");
+        return AP_E_INVALID;
+    }
+    static thread_local Orbit o;
+    static thread_local Dec sx, sy;
+    if (!load_seeds(o, meta, limbs, limb_stride)) return AP_E_INVALID;
+    const bool periodic = fractal_type == 0 || fractal_type == 2;
+    int check_step = 8, saved_k = 0;
+    copy(sx, o.zx);
+    copy(sy, o.zy);
+    int len = max_iter;
+    for (int k = 0; k < max_iter; ++k) {
+        if (!to_double(o.zx, ref_re + k) || !to_double(o.zy, ref_im + k)) {
+            ap::set_error("ap_decimal_orbit: conversion not decided");
+            return AP_E_UNSUPPORTED;
+        }
+        if (!squares(o, prec)) goto too_long;
+        if (cmp(o.mag, o.bail) > 0) {
+            len = k;
+            break;
+        }
+        if (periodic) {
+            if (k == check_step) {
+                check_step <<= 1;
+                saved_k = k;
+                copy(sx, o.zx);
+                copy(sy, o.zy);
+            } else if (k > saved_k && cmp(o.zx, sx) == 0 && cmp(o.zy, sy) == 0) {
+                const int period = k - saved_k;
+                for (int j = k; j <= max_iter; ++j) {
+                    ref_re[j] = ref_re[j - period];
+                    ref_im[j] = ref_im[j - period];
+                }
+                *ref_len = max_iter;
+                return AP_OK;
+            }
+        }
+        if (!step(o, fractal_type, gen_n, prec)) goto too_long;
+    }
+    if (!to_double(o.zx, ref_re + len) || !to_double(o.zy, ref_im + len)) {
+        ap::set_error("ap_decimal_orbit: conversion not decided");
+        return AP_E_UNSUPPORTED;
+    }
+    *ref_len = len;
+    return AP_OK;
+too_long:
+    ap::set_error("ap_decimal_orbit: operand too long for %d limbs", kMaxLimbs);
+    return AP_E_INVALID;
+}
+
+// float(Decimal) of one value (AP_E_UNSUPPORTED when the bounds do not decide), for
+// checking the conversion against the decimal module.
+extern "C" int ap_decimal_to_double(const int64_t* meta, const uint64_t* limbs, double* out) {
+    if (!meta || !limbs || !out || meta[2] < 1 || meta[2] > kMaxLimbs) {
+        ap::set_error("ap_decimal_to_double: bad arguments");
+        return AP_E_INVALID;
+    }
+    static thread_local Dec a;
+    load(a, meta, limbs);
+    if (!to_double(a, out)) {
+        ap::set_error("ap_decimal_to_double: not decided");
+        return AP_E_UNSUPPORTED;
+    }
     return AP_OK;
 }
 

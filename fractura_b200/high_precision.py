@@ -270,6 +270,30 @@ def decimal_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
     orbit is detected at power-of-two checkpoints and its cycle is copied to
     the end of the arrays.
     """
+    import ctypes as C
+    ref_re = np.zeros(max_iter + 1, dtype=np.float64)
+    ref_im = np.zeros(max_iter + 1, dtype=np.float64)
+    # natively (ap_decimal_orbit: the decimal module's arithmetic without the Python
+    # lock), unless an operand is longer than it holds or a conversion is undecided
+    args = _native_seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki)
+    if args is not None:
+        meta, limbs, stride = args
+        n = C.c_int32(0)
+        rc = _native().ap_decimal_orbit(
+            meta.ctypes.data_as(C.c_void_p), limbs.ctypes.data_as(C.c_void_p), int(stride),
+            int(_orbit_context(prec_bits).prec), int(fractal_type), int(gen_n), int(max_iter),
+            ref_re.ctypes.data_as(C.c_void_p), ref_im.ctypes.data_as(C.c_void_p), C.byref(n))
+        if rc == 0:
+            return ref_re, ref_im, int(n.value)
+        ref_re[:] = 0.0
+        ref_im[:] = 0.0
+    return decimal_orbit_py(cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
+                            gen_n, gen_kr, gen_ki)
+
+
+def decimal_orbit_py(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0, julia_cx=0.0, julia_cy=0.0,
+                     prec_bits=256, gen_n=3, gen_kr=0.25, gen_ki=1.0):
+    """The same loop in Python's decimal module (operands of any length)."""
     ref_re = np.zeros(max_iter + 1, dtype=np.float64)
     ref_im = np.zeros(max_iter + 1, dtype=np.float64)
     with localcontext(_orbit_context(prec_bits)):
@@ -311,6 +335,21 @@ def _dec_parts(d):
     return t.sign, int(t.exponent), [int(digits[max(0, i - 8):i]) for i in range(len(digits), 0, -8)]
 
 
+def _native_seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki):
+    """(meta, limbs, stride) of the six seeds of the native Decimal loops, as _start and
+    the reference form them, or None when an operand is longer than they hold."""
+    zx, zy, c_x, c_y = _start(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy)
+    parts = [_dec_parts(v) for v in (zx, zy, c_x, c_y, Decimal(str(gen_kr)), Decimal(str(gen_ki)))]
+    stride = max(len(p[2]) for p in parts)
+    if stride > 200:
+        return None
+    meta = np.array([[p[0], p[1], len(p[2])] for p in parts], dtype=np.int64)
+    limbs = np.zeros((6, stride), dtype=np.uint64)
+    for q, p in enumerate(parts):
+        limbs[q, :len(p[2])] = p[2]
+    return meta, limbs, stride
+
+
 def decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
                           julia_cx=0.0, julia_cy=0.0, prec_bits=256,
                           gen_n=3, gen_kr=0.25, gen_ki=1.0):
@@ -321,15 +360,9 @@ def decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type=0,
     import ctypes as C
     from . import _lib
     ctx = _orbit_context(prec_bits)
-    zx, zy, c_x, c_y = _start(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy)
-    seeds = [zx, zy, c_x, c_y, Decimal(str(gen_kr)), Decimal(str(gen_ki))]
-    parts = [_dec_parts(v) for v in seeds]
-    stride = max(len(p[2]) for p in parts)
-    if stride <= 200:
-        meta = np.array([[p[0], p[1], len(p[2])] for p in parts], dtype=np.int64)
-        limbs = np.zeros((6, stride), dtype=np.uint64)
-        for q, p in enumerate(parts):
-            limbs[q, :len(p[2])] = p[2]
+    args = _native_seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
+    if args is not None:
+        meta, limbs, stride = args
         k = C.c_int32(0)
         mag_meta = np.zeros(3, dtype=np.int64)
         mag_limbs = np.zeros(400, dtype=np.uint64)

@@ -322,6 +322,22 @@ AP_API int ap_decimal_escape(const int64_t* meta, const uint64_t* limbs, int32_t
                              int32_t prec, int32_t fractal_type, int32_t gen_n, int32_t max_iter,
                              int32_t* k_out, int64_t* mag2_meta, uint64_t* mag2_limbs);
 
+/* The orbit loop of the same Decimal iteration (decimal_orbit, the reference orbit of
+ * math_core/high_precision.py:706-875 when the fixed-point runs disagree), on the host:
+ * seeds as for ap_decimal_escape; ref_re/ref_im (max_iter + 1 float64) receive float(Z_k),
+ * correctly rounded; *ref_len = the escape step or max_iter; an exactly repeating
+ * Mandelbrot/Julia orbit found at power-of-two checkpoints has its cycle copied to the end.
+ * AP_E_UNSUPPORTED when a value's conversion is not decided by the bounds this code keeps
+ * (a tie or a near-tie, a value above 2^127 or outside the normal double range): the
+ * caller then iterates in the decimal module. */
+AP_API int ap_decimal_orbit(const int64_t* meta, const uint64_t* limbs, int32_t limb_stride,
+                            int32_t prec, int32_t fractal_type, int32_t gen_n, int32_t max_iter,
+                            double* ref_re, double* ref_im, int32_t* ref_len);
+
+/* float(Decimal) of one value (meta: neg, exp, n; limbs: n base-1e8 limbs), or
+ * AP_E_UNSUPPORTED as above; for checking the conversion against the decimal module. */
+AP_API int ap_decimal_to_double(const int64_t* meta, const uint64_t* limbs, double* out);
+
 /* One operation of that arithmetic (op 0 add, 1 subtract, 2 multiply, 3 compare into
  * *cmp_out), for checking it against the decimal module; out: 3 + 400 entries. */
 AP_API int ap_decimal_arith(int32_t op, const int64_t* a_meta, const uint64_t* a_limbs,

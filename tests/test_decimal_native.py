@@ -121,3 +121,68 @@ def test_escape_loops_equal_the_python_loop(formula, prec_bits):
         got = hp.decimal_escape_scalar(cx, cy, 1500, ft, jx, jy, prec_bits, n, 0.1, 0.2)
         want = hp.decimal_escape_scalar_py(cx, cy, 1500, ft, jx, jy, prec_bits, n, 0.1, 0.2)
         assert got == want, (cx, cy, got, want)
+
+
+def native_float(d):
+    L = _lib.load()
+    m, limbs = _enc(d)
+    out = C.c_double(0.0)
+    rc = L.ap_decimal_to_double(m.ctypes.data_as(C.c_void_p), limbs.ctypes.data_as(C.c_void_p), C.byref(out))
+    return None if rc != 0 else out.value
+
+
+def test_conversion_equals_float_of_decimal():
+    """Correctly rounded float64 of decimals of every length and of the scales orbits
+    produce (1e-300 .. 1e30); undecided only at ties or within ~2^-110 of one, and
+    above 2^127 (values no orbit reaches), where the decimal module converts."""
+    rng = np.random.default_rng(11)
+    undecided = 0
+    for _ in range(20000):
+        d = _rand_dec(rng, max_digits=int(rng.integers(2, 700)), exp_range=(-400, 5))
+        if not (Decimal("1e-300") < abs(d) < Decimal("1e300")):
+            continue
+        got = native_float(d)
+        if got is None:
+            undecided += abs(d) < Decimal("1e30")
+            continue
+        want = float(d)
+        assert got == want and np.signbit(got) == np.signbit(want), (d, got, want)
+    assert undecided == 0
+    # exact values, ties and their neighbours
+    for x in (1.0, 0.1, 1e-80, 3.0e-300, 65536.0, 123456.789, -2.5e-17):
+        d = Decimal(x)  # the exact binary value
+        assert native_float(d) == x
+        nxt = np.nextafter(x, np.inf)
+        half = (Decimal(x) + Decimal(float(nxt))) / 2  # an exact tie
+        assert native_float(half) in (None, float(half))
+        for eps in (Decimal("1e-400"), -Decimal("1e-400")):
+            assert native_float(half + eps) in (None, float(half + eps))
+    assert native_float(Decimal("-0")) == 0.0 and np.signbit(native_float(Decimal("-0")))
+
+
+@pytest.mark.parametrize("formula", FORMULAS, ids=lambda f: f"type{f[0]}_n{f[3]}")
+@pytest.mark.parametrize("prec_bits", [150, 400])
+def test_orbit_loops_equal_the_python_loop(formula, prec_bits):
+    ft, jx, jy, n = formula
+    rng = np.random.default_rng(3 * prec_bits + 7 * ft + n)
+    for _ in range(6):
+        if ft in (2, 3):
+            x, y = rng.uniform(-1.5, 1.5), rng.uniform(-1.0, 1.0)
+        else:
+            x, y = rng.uniform(-2.0, 0.6), rng.uniform(-1.2, 1.2)
+        cx = Decimal(repr(x)) + Decimal(int(rng.integers(1, 10 ** 9))).scaleb(-int(rng.integers(20, 90)))
+        cy = Decimal(repr(y)) - Decimal(int(rng.integers(1, 10 ** 9))).scaleb(-int(rng.integers(20, 90)))
+        got = hp.decimal_orbit(cx, cy, 1500, ft, jx, jy, prec_bits, n, 0.1, 0.2)
+        want = hp.decimal_orbit_py(cx, cy, 1500, ft, jx, jy, prec_bits, n, 0.1, 0.2)
+        assert got[2] == want[2]
+        assert np.array_equal(got[0].view(np.uint64), want[0].view(np.uint64))
+        assert np.array_equal(got[1].view(np.uint64), want[1].view(np.uint64))
+
+
+@pytest.mark.parametrize("c", [("0", "0"), ("-1", "0"), ("-0.1", "0.1"), ("-1.3", "0.05"), ("0.25", "0")])
+def test_periodic_orbits_equal_the_python_loop(c):
+    cx, cy = Decimal(c[0]), Decimal(c[1])
+    got = hp.decimal_orbit(cx, cy, 5000, 0, 0.0, 0.0, 300)
+    want = hp.decimal_orbit_py(cx, cy, 5000, 0, 0.0, 0.0, 300)
+    assert got[2] == want[2] == 5000
+    assert np.array_equal(got[0], want[0]) and np.array_equal(got[1], want[1])
