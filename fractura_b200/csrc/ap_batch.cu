@@ -5,22 +5,36 @@
 // BLA rows, no in-kernel colour) with its own parameters and outputs.  Each
 // tile is cut into patches of patch_w x patch_h = 256 pixels; patches are
 // numbered tile after tile (the host orders tiles by estimated cost, largest
-// first).  The grid holds blocks_per_sm blocks per SM for the whole batch; each
-// warp takes the next eighth of a patch (32 pixels) from one global counter
-// (atomicAdd), looks its tile up by binary search over the tiles' first patch
-// numbers, evaluates its pixels with coarse_pixel (the per-frame kernel's code, so
-// values are identical) and takes the next, until the counter passes the end.
-// Nothing waits on anything: a warp that finds the queue empty exits.
+// first).  The grid holds blocks_per_sm blocks per SM for the whole batch.  The
+// queue is one global pixel counter.  Each lane of a warp holds one pixel as a
+// resumable PixelRun (the per-frame kernel's pixel_begin / pixel_advance /
+// pixel_finish, so values are identical) and runs it for kQuantum loop steps at a
+// time.  Between quanta, once kRefill or more lanes are idle (or all are), the warp
+// takes that many consecutive pixels with one atomicAdd, so the new pixels are
+// neighbours that start together and share orbit records; each lane looks its
+// pixel's tile up by binary search over the tiles' first patch numbers.  Nothing
+// waits on anything: a warp whose lanes all find the queue empty exits.
 #include "ap_coarse.cuh"
 
 namespace ap {
 
 static_assert(sizeof(ApTileDesc) % 16 == 0, "tile descriptors are 16-byte aligned records");
 
-// One variant of the pixel loop per (formula class, BLA): separate functions, so
-// each keeps the register allocation it has in the per-frame kernel.
-template <int ARITH, int FT, bool BLA>
-__device__ __noinline__ void tile_pixel(const ApTileDesc* __restrict__ t, int i, int j) {
+// Steps a lane runs on its pixel before the warp lets lanes whose pixel finished take
+// new ones (lanes wait at most this long for each other), and the number of idle lanes
+// that triggers a refill.  Refilling single lanes scatters the warp's orbit indices
+// (one record load per lane instead of one per warp); 128 / 16 was the fastest pair
+// on the 64-tile batch (quanta 128-2048, thresholds 8-32).
+#ifndef AP_BATCH_QUANTUM
+#define AP_BATCH_QUANTUM 128
+#endif
+#ifndef AP_BATCH_REFILL
+#define AP_BATCH_REFILL 16
+#endif
+constexpr int kQuantum = AP_BATCH_QUANTUM;
+constexpr int kRefill = AP_BATCH_REFILL;
+
+inline __device__ ApFrameBuffers tile_buffers(const ApTileDesc* t) {
     ApFrameBuffers b{};
     b.orbit_packed = t->orbit_packed;
     b.bla_packed = t->bla_packed;
@@ -29,24 +43,53 @@ __device__ __noinline__ void tile_pixel(const ApTileDesc* __restrict__ t, int i,
     b.s64 = t->s64;
     b.glitch_out = t->glitch_out;
     b.counters = t->counters;
-    coarse_pixel<ARITH, FT, BLA>(t->p, b, i, j);
+    return b;
+}
+
+// One variant of the pixel loop per (formula class, BLA): separate functions, so
+// each keeps the register allocation it has in the per-frame kernel.
+template <int ARITH, int FT, bool BLA>
+__device__ __noinline__ void tile_advance(const ApTileDesc* __restrict__ t, PixelRun& s) {
+    pixel_advance<ARITH, FT, BLA, true>(t->p, tile_buffers(t), s, kQuantum);
 }
 
 template <int ARITH>
-__device__ __forceinline__ void batch_pixel(const ApTileDesc* t, int i, int j) {
+__device__ __forceinline__ void batch_advance(const ApTileDesc* t, PixelRun& s) {
     const bool bla = t->p.bla_levels > 1 && t->bla_packed != nullptr;
     switch (t->p.fractal_type) {
     case 1:
-    case 3: tile_pixel<ARITH, kFtShip, false>(t, i, j); break;
+    case 3: tile_advance<ARITH, kFtShip, false>(t, s); break;
     case 4:
-        if (bla) tile_pixel<ARITH, kFtMulti, true>(t, i, j);
-        else tile_pixel<ARITH, kFtMulti, false>(t, i, j);
+        if (bla) tile_advance<ARITH, kFtMulti, true>(t, s);
+        else tile_advance<ARITH, kFtMulti, false>(t, s);
         break;
     default:
-        if (bla) tile_pixel<ARITH, kFtQuad, true>(t, i, j);
-        else tile_pixel<ARITH, kFtQuad, false>(t, i, j);
+        if (bla) tile_advance<ARITH, kFtQuad, true>(t, s);
+        else tile_advance<ARITH, kFtQuad, false>(t, s);
         break;
     }
+}
+
+// Pixel u of the batch (patches of 256 pixels, numbered tile after tile; row-major in a
+// patch) -> its tile and its (i, j); false when it falls outside the tile.
+__device__ __forceinline__ bool batch_pixel_at(const ApTileDesc* __restrict__ tiles,
+                                               const int64_t* __restrict__ first, int n, int patch_w,
+                                               int patch_h, long long u, const ApTileDesc** t, int* i,
+                                               int* j) {
+    const long long item = u >> 8;  // the patch
+    const int q = (int)(u & 255);
+    int lo = 0, hi = n - 1;  // last tile whose first patch <= item
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    *t = tiles + lo;
+    const long long local = item - first[lo];
+    const int px = ((*t)->p.width + patch_w - 1) / patch_w;
+    *i = (int)(local % px) * patch_w + q % patch_w;
+    *j = (int)(local / px) * patch_h + q / patch_w;
+    return *i < (*t)->p.width && *j < (*t)->p.height;
 }
 
 template <int ARITH, int MINB>
@@ -54,30 +97,50 @@ __global__ void __launch_bounds__(256, MINB) batch_kernel(const ApTileDesc* __re
                                                           const int64_t* __restrict__ first,
                                                           int n, int patch_w, int patch_h,
                                                           unsigned long long* head) {
-    // Each warp takes the next eighth of a patch (32 of its 256 pixels) on its own:
-    // a warp that finishes early does not wait for the slow warps of its block.
-    const long long total = first[n] * 8;
+    // Lane-level work stealing: a lane runs its pixel for up to kQuantum loop
+    // iterations; then, if kRefill or more lanes are idle (or none is busy), the idle
+    // lanes take the next pixels of the queue (one atomicAdd per warp for all of
+    // them), so a warp does not idle on one long pixel while its other lanes' pixels
+    // are done.
+    const long long total = first[n] * 256;
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    PixelRun s;
+    const ApTileDesc* t = nullptr;
+    bool active = false, drained = false;
     for (;;) {
-        unsigned long long got = 0;
-        if (lane == 0) got = atomicAdd(head, 1ULL);
-        const long long unit = (long long)__shfl_sync(0xffffffffu, got, 0);
-        if (unit >= total) break;
-        const long long item = unit >> 3;  // the patch
-        const int q = (int)(unit & 7) * 32 + lane;  // pixel of the patch, row-major
-        const int tx = q % patch_w, ty = q / patch_w;
-        int lo = 0, hi = n - 1;  // last tile whose first patch <= item
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (first[mid] <= item) lo = mid;
-            else hi = mid - 1;
+        const unsigned need = __ballot_sync(full, !active && !drained);
+        const unsigned busy = __ballot_sync(full, active);
+        if (need && (__popc(need) >= kRefill || busy == 0)) {
+            const int leader = __ffs(need) - 1;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(head, (unsigned long long)__popc(need));
+            base = __shfl_sync(full, base, leader);
+            if (!active && !drained) {
+                const long long u = (long long)base + __popc(need & ((1u << lane) - 1u));
+                int i = 0, j = 0;
+                if (u >= total) {
+                    drained = true;
+                } else if (batch_pixel_at(tiles, first, n, patch_w, patch_h, u, &t, &i, &j)) {
+                    // the set-up differs between formulas only in the series start,
+                    // which Burning Ship types do not take
+                    const bool ship = t->p.fractal_type == 1 || t->p.fractal_type == 3;
+                    active = ship ? pixel_begin<ARITH, kFtShip>(t->p, tile_buffers(t), i, j, s)
+                                  : pixel_begin<ARITH, kFtQuad>(t->p, tile_buffers(t), i, j, s);
+                }
+            }
         }
-        const ApTileDesc& t = tiles[lo];
-        const long long local = item - first[lo];
-        const int px = (t.p.width + patch_w - 1) / patch_w;
-        const int i = (int)(local % px) * patch_w + tx;
-        const int j = (int)(local / px) * patch_h + ty;
-        if (i < t.p.width && j < t.p.height) batch_pixel<ARITH>(&t, i, j);
+        if (__ballot_sync(full, active) == 0) {
+            if (__all_sync(full, drained)) break;
+            continue;
+        }
+        if (active) {
+            batch_advance<ARITH>(t, s);
+            if (s.stage == 3) {
+                pixel_finish(t->p, tile_buffers(t), s);
+                active = false;
+            }
+        }
     }
 }
 

@@ -32,29 +32,38 @@ __device__ __forceinline__ double4 ldg4(const double4* p) {
     return make_double4(a.x, a.y, c.x, c.y);
 }
 
-// One pixel (i, j) of a coarse pass: the whole stage-1 / stage-2 loop and the
-// output writes.  Shared by the per-frame kernel below and the persistent
-// batch kernel (ap_batch.cu), so both give identical values.
-template <int ARITH, int FT, bool BLA>
-__device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFrameBuffers& b, int i,
-                                             int j) {
-    constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
-    const int idx = j * p.width + i;
-    if (p.rebase_pass > 0 && b.glitch_in[idx] == 0) return;
+// One pixel of a coarse pass, resumable: pixel_begin sets it up, pixel_advance runs
+// its stage-1 (perturbation) and stage-2 (direct) loops -- all of them, or at most
+// `budget` loop iterations (steps or leaps) per call when BUDGET is set, so that a
+// persistent kernel can hand a lane whose pixel finished a new one -- and
+// pixel_finish writes its outputs.  coarse_pixel runs the three in a row; the
+// per-frame kernel below and the batch kernel (ap_batch.cu) share this code, so both
+// give identical values.
+struct PixelRun {
+    double dzx, dzy;  // stage 1: the delta
+    double zx, zy;    // stage 2: z itself
+    double dcx, dcy;  // the pixel's offset from the reference
+    int idx, k, k0, k2, glitch, leaps, skipped;
+    int stage;        // 1 perturbation, 2 direct, 3 done
+    SampleOut o;
+};
 
+template <int ARITH, int FT>
+__device__ __forceinline__ bool pixel_begin(const ApFrameParams& p, const ApFrameBuffers& b, int i, int j,
+                                            PixelRun& s) {
+    s.idx = j * p.width + i;
+    if (p.rebase_pass > 0 && b.glitch_in[s.idx] == 0) return false;
     const double sub_offset = ((double)p.factor - 1.0) * 0.5;
     const double sub_i = (double)(i * p.factor) + sub_offset;
     const double sub_j = (double)(j * p.factor) + sub_offset;
-    const double dcy = (p.ref_py - sub_j) * p.dy_hi;
-    const double dcx = (sub_i - p.ref_px) * p.dx_hi;
+    s.dcy = (p.ref_py - sub_j) * p.dy_hi;
+    s.dcx = (sub_i - p.ref_px) * p.dx_hi;
     const bool julia = (p.fractal_type == 2 || p.fractal_type == 3);
-    const int ref_len = p.ref_len, max_iter = p.max_iter;
-    const double4* __restrict__ orb = reinterpret_cast<const double4*>(b.orbit_packed);
-
-    double dzx = julia ? dcx : 0.0, dzy = julia ? dcy : 0.0;
-    int k = 0;
+    s.dzx = julia ? s.dcx : 0.0;
+    s.dzy = julia ? s.dcy : 0.0;
+    s.k = 0;
     if (p.bbsa_skip > 0 && FT != kFtShip) {
-        const double ux = dcx * p.bbsa_inv_r, uy = dcy * p.bbsa_inv_r;
+        const double ux = s.dcx * p.bbsa_inv_r, uy = s.dcy * p.bbsa_inv_r;
         if (ux * ux + uy * uy <= 1.0) {
             bool eight = false;
             for (int q = 8; q < 16; ++q) eight |= (p.bbsa[q] != 0.0);
@@ -66,141 +75,183 @@ __device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFra
                 tr = ux * ar - uy * ai;
                 ti = ux * ai + uy * ar;
             }
-            dzx = tr;
-            dzy = ti;
-            k = p.bbsa_skip;
+            s.dzx = tr;
+            s.dzy = ti;
+            s.k = p.bbsa_skip;
         }
     }
-    const double dcpx = julia ? 0.0 : dcx, dcpy = julia ? 0.0 : dcy;
-    const bool strict = p.strict_glitch > 0;
-    const bool esc_glitch = (p.flags & AP_FLAG_ESCAPE_GLITCH) != 0;
-    const int k0 = k;
-    int glitch = 0, leaps = 0, skipped = 0, k2 = -1;
-    const double inv_ln = inv_ln_for(p.fractal_type, p.gen_n);
-    const double* __restrict__ R = b.bla_packed;
-    const double4* __restrict__ AB =
-        reinterpret_cast<const double4*>(b.bla_packed + (size_t)ref_len * 16);
-    const int max_level = p.bla_levels - 1;
+    s.k0 = s.k;
+    s.k2 = -1;
+    s.glitch = s.leaps = s.skipped = 0;
+    s.stage = 1;
+    s.o = interior_sample();
+    return true;
+}
 
-    SampleOut o;
-    bool finished = false;
-    while (k < ref_len) {
-        const double4 Z = ldg4(orb + k);
-        const double rx = Z.x, ry = Z.y;
-        const double zx = rx + dzx, zy = ry + dzy;
-        const double dz_mag2 = dzx * dzx + dzy * dzy;
-        // One branch on the common path: inside the safe radius (no test can fire)
-        // and outside the level-0 BLA radius (no leap), the step runs straight
-        // through.  The packed radii are 0 wherever k + 2^d >= ref_len, so no level
-        // is admissible at the last step without a separate bound check.
-        const bool unsafe = !(dz_mag2 < Z.z);
-        const bool leap = BLA && (dz_mag2 < Z.w);
-        if (unsafe || leap) {
-            if (unsafe) {
-                const double mag2 = zx * zx + zy * zy;
-                const double r_mag2 = rx * rx + ry * ry;
-                if (mag2 > kBailout) {
-                    if (esc_glitch && strict && k > 15 && r_mag2 < 4.0) glitch = 1;
-                    o = escaped_sample(k, mag2, inv_ln);
-                    finished = true;
-                    break;
-                }
-                // the Pauldelbrot threshold, as the reference forms it
-                const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;
-                if (strict && k > 15 && mag2 < thr) glitch = 1;
+template <int ARITH, int FT, bool BLA, bool BUDGET>
+__device__ __forceinline__ void pixel_advance(const ApFrameParams& p, const ApFrameBuffers& b, PixelRun& s,
+                                              int budget) {
+    constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
+    const bool julia = (p.fractal_type == 2 || p.fractal_type == 3);
+    const int ref_len = p.ref_len, max_iter = p.max_iter;
+    const double4* __restrict__ orb = reinterpret_cast<const double4*>(b.orbit_packed);
+    const double inv_ln = inv_ln_for(p.fractal_type, p.gen_n);
+    int k = s.k, glitch = s.glitch, leaps = s.leaps, skipped = s.skipped;
+    SampleOut o = s.o;
+
+    if (s.stage == 1) {
+        double dzx = s.dzx, dzy = s.dzy;
+        const double dcpx = julia ? 0.0 : s.dcx, dcpy = julia ? 0.0 : s.dcy;
+        const bool strict = p.strict_glitch > 0;
+        const bool esc_glitch = (p.flags & AP_FLAG_ESCAPE_GLITCH) != 0;
+        const double* __restrict__ R = b.bla_packed;
+        const double4* __restrict__ AB =
+            reinterpret_cast<const double4*>(b.bla_packed + (size_t)ref_len * 16);
+        const int max_level = p.bla_levels - 1;
+        bool finished = false, paused = false;
+        while (k < ref_len) {
+            if (BUDGET && --budget < 0) {
+                paused = true;
+                break;
             }
-            if (leap) {
-                const double* row = R + (size_t)k * 16;
-                int hi = max_level;
-                if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
-                // The admissible levels are a prefix 0..lo (radii never increase
-                // with the level), so lo is a count.  Two rounds of three
-                // independent loads: the quarter of the row, then the level in it.
-                int q = 0;
-#pragma unroll
-                for (int t = 1; t <= 3; ++t)
-                    q += (4 * t <= hi && dz_mag2 < __ldg(row + 4 * t)) ? 1 : 0;
-                int lo = 4 * q;
-#pragma unroll
-                for (int t = 1; t <= 3; ++t) {
-                    const int d = 4 * q + t;
-                    lo += (d <= hi && dz_mag2 < __ldg(row + d)) ? 1 : 0;
+            const double4 Z = ldg4(orb + k);
+            const double rx = Z.x, ry = Z.y;
+            const double zx = rx + dzx, zy = ry + dzy;
+            const double dz_mag2 = dzx * dzx + dzy * dzy;
+            // One branch on the common path: inside the safe radius (no test can fire)
+            // and outside the level-0 BLA radius (no leap), the step runs straight
+            // through.  The packed radii are 0 wherever k + 2^d >= ref_len, so no level
+            // is admissible at the last step without a separate bound check.
+            const bool unsafe = !(dz_mag2 < Z.z);
+            const bool leap = BLA && (dz_mag2 < Z.w);
+            if (unsafe || leap) {
+                if (unsafe) {
+                    const double mag2 = zx * zx + zy * zy;
+                    const double r_mag2 = rx * rx + ry * ry;
+                    if (mag2 > kBailout) {
+                        if (esc_glitch && strict && k > 15 && r_mag2 < 4.0) glitch = 1;
+                        o = escaped_sample(k, mag2, inv_ln);
+                        finished = true;
+                        break;
+                    }
+                    // the Pauldelbrot threshold, as the reference forms it
+                    const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;
+                    if (strict && k > 15 && mag2 < thr) glitch = 1;
                 }
-                const double4 e = ldg4(AB + (size_t)k * 16 + lo);
+                if (leap) {
+                    const double* row = R + (size_t)k * 16;
+                    int hi = max_level;
+                    if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
+                    // The admissible levels are a prefix 0..lo (radii never increase
+                    // with the level), so lo is a count.  Two rounds of three
+                    // independent loads: the quarter of the row, then the level in it.
+                    int q = 0;
+#pragma unroll
+                    for (int t = 1; t <= 3; ++t)
+                        q += (4 * t <= hi && dz_mag2 < __ldg(row + 4 * t)) ? 1 : 0;
+                    int lo = 4 * q;
+#pragma unroll
+                    for (int t = 1; t <= 3; ++t) {
+                        const int d = 4 * q + t;
+                        lo += (d <= hi && dz_mag2 < __ldg(row + d)) ? 1 : 0;
+                    }
+                    const double4 e = ldg4(AB + (size_t)k * 16 + lo);
+                    double nx, ny;
+                    if (kCpu) {
+                        nx = (e.x * dzx - e.y * dzy) + (e.z * dcpx - e.w * dcpy);
+                        ny = (e.x * dzy + e.y * dzx) + (e.z * dcpy + e.w * dcpx);
+                    } else {
+                        nx = fma(e.x, dzx, fma(-e.y, dzy, fma(e.z, dcpx, -e.w * dcpy)));
+                        ny = fma(e.x, dzy, fma(e.y, dzx, fma(e.z, dcpy, e.w * dcpx)));
+                    }
+                    dzx = nx;
+                    dzy = ny;
+                    if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) {
+                        o = interior_sample();
+                        o.s = (float)k;
+                        o.s64 = (double)k;
+                        o.k = k;
+                        glitch = 1;
+                        finished = true;
+                        break;
+                    }
+                    k += 1 << lo;
+                    ++leaps;
+                    skipped += 1 << lo;
+                    continue;
+                }
+            }
+            if (FT == kFtQuad) {
                 double nx, ny;
                 if (kCpu) {
-                    nx = (e.x * dzx - e.y * dzy) + (e.z * dcpx - e.w * dcpy);
-                    ny = (e.x * dzy + e.y * dzx) + (e.z * dcpy + e.w * dcpx);
+                    nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+                    ny = 2.0 * (zx * dzy + ry * dzx) + dcpy;
                 } else {
-                    nx = fma(e.x, dzx, fma(-e.y, dzy, fma(e.z, dcpx, -e.w * dcpy)));
-                    ny = fma(e.x, dzy, fma(e.y, dzx, fma(e.z, dcpy, e.w * dcpx)));
+                    nx = fma(2.0 * rx + dzx, dzx, fma(-(2.0 * ry + dzy), dzy, dcpx));
+                    ny = fma(2.0, fma(zx, dzy, ry * dzx), dcpy);
                 }
                 dzx = nx;
                 dzy = ny;
-                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) {
-                    o = interior_sample();
-                    o.s = (float)k;
-                    o.s64 = (double)k;
-                    o.k = k;
-                    glitch = 1;
-                    finished = true;
-                    break;
-                }
-                k += 1 << lo;
-                ++leaps;
-                skipped += 1 << lo;
-                continue;
-            }
-        }
-        if (FT == kFtQuad) {
-            double nx, ny;
-            if (kCpu) {
-                nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
-                ny = 2.0 * (zx * dzy + ry * dzx) + dcpy;
+            } else if (FT == kFtShip) {
+                const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+                const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+                const double ddx = zx * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+                const double ddy = zy * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+                dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcpy;
+                dzx = nx;
             } else {
-                nx = fma(2.0 * rx + dzx, dzx, fma(-(2.0 * ry + dzy), dzy, dcpx));
-                ny = fma(2.0, fma(zx, dzy, ry * dzx), dcpy);
+                double pr = dzx, pi = dzy, qr = rx, qi = ry;
+                for (int t = 0; t < p.gen_n - 1; ++t) {
+                    const double t1r = pr * rx - pi * ry, t1i = pr * ry + pi * rx;
+                    const double sr = pr + qr, si = pi + qi;
+                    const double t2r = sr * dzx - si * dzy, t2i = sr * dzy + si * dzx;
+                    pr = t1r + t2r;
+                    pi = t1i + t2i;
+                    const double nqr = qr * rx - qi * ry, nqi = qr * ry + qi * rx;
+                    qr = nqr;
+                    qi = nqi;
+                }
+                const double kzr = p.gen_kr * dzx - p.gen_ki * dzy;
+                const double kzi = p.gen_kr * dzy + p.gen_ki * dzx;
+                dzx = pr + kzr + dcpx;
+                dzy = pi + kzi + dcpy;
             }
-            dzx = nx;
-            dzy = ny;
-        } else if (FT == kFtShip) {
-            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
-            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
-            const double ddx = zx * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
-            const double ddy = zy * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
-            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcpy;
-            dzx = nx;
-        } else {
-            double pr = dzx, pi = dzy, qr = rx, qi = ry;
-            for (int t = 0; t < p.gen_n - 1; ++t) {
-                const double t1r = pr * rx - pi * ry, t1i = pr * ry + pi * rx;
-                const double sr = pr + qr, si = pi + qi;
-                const double t2r = sr * dzx - si * dzy, t2i = sr * dzy + si * dzx;
-                pr = t1r + t2r;
-                pi = t1i + t2i;
-                const double nqr = qr * rx - qi * ry, nqi = qr * ry + qi * rx;
-                qr = nqr;
-                qi = nqi;
-            }
-            const double kzr = p.gen_kr * dzx - p.gen_ki * dzy;
-            const double kzi = p.gen_kr * dzy + p.gen_ki * dzx;
-            dzx = pr + kzr + dcpx;
-            dzy = pi + kzi + dcpy;
+            ++k;
         }
-        ++k;
+        if (paused) {
+            s.dzx = dzx;
+            s.dzy = dzy;
+            s.k = k;
+            s.glitch = glitch;
+            s.leaps = leaps;
+            s.skipped = skipped;
+            return;
+        }
+        if (finished) {
+            s.stage = 3;
+        } else {
+            // Stage 2: past the end of the reference orbit, iterate z directly.
+            const double4 Zend = ldg4(orb + ref_len);
+            s.zx = Zend.x + dzx;
+            s.zy = Zend.y + dzy;
+            if (ref_len < max_iter) glitch = 1;
+            s.k2 = k;
+            o = interior_sample();
+            s.stage = 2;
+        }
     }
 
-    if (!finished) {
-        // Stage 2: past the end of the reference orbit, iterate z directly.
-        const double4 Zend = ldg4(orb + ref_len);
-        double zx = Zend.x + dzx, zy = Zend.y + dzy;
-        const double cx = julia ? p.julia_cx_hi : p.ref_cx + dcx;
-        const double cy = julia ? p.julia_cy_hi : p.ref_cy + dcy;
-        if (ref_len < max_iter) glitch = 1;
-        k2 = k;
+    if (s.stage == 2) {
+        double zx = s.zx, zy = s.zy;
+        const double cx = julia ? p.julia_cx_hi : p.ref_cx + s.dcx;
+        const double cy = julia ? p.julia_cy_hi : p.ref_cy + s.dcy;
         const bool nan_guard = (p.flags & AP_FLAG_NAN_GUARD) != 0;
-        o = interior_sample();
+        bool paused = false;
         while (k < max_iter) {
+            if (BUDGET && --budget < 0) {
+                paused = true;
+                break;
+            }
             const double zx2 = zx * zx, zy2 = zy * zy;
             const double mag2 = zx2 + zy2;
             if (nan_guard && (isnan(mag2) || isinf(mag2))) {
@@ -234,17 +285,39 @@ __device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFra
             }
             ++k;
         }
+        s.zx = zx;
+        s.zy = zy;
+        if (!paused) s.stage = 3;
     }
-    const int k_end = (o.k == -1) ? max_iter : k;
-    b.iter_map[idx] = o.s;
-    if (b.kmap) b.kmap[idx] = o.k;
-    if (b.s64) b.s64[idx] = o.s64;
-    if (b.glitch_out) b.glitch_out[idx] = glitch ? 1 : 0;
+    s.k = k;
+    s.glitch = glitch;
+    s.leaps = leaps;
+    s.skipped = skipped;
+    s.o = o;
+}
+
+__device__ __forceinline__ void pixel_finish(const ApFrameParams& p, const ApFrameBuffers& b, const PixelRun& s) {
+    const int max_iter = p.max_iter;
+    const int k_end = (s.o.k == -1) ? max_iter : s.k;
+    b.iter_map[s.idx] = s.o.s;
+    if (b.kmap) b.kmap[s.idx] = s.o.k;
+    if (b.s64) b.s64[s.idx] = s.o.s64;
+    if (b.glitch_out) b.glitch_out[s.idx] = s.glitch ? 1 : 0;
     if (b.counters) {
-        const int it1 = (k2 < 0 ? k_end - k0 : k2 - k0) - skipped;
-        const int it2 = k2 < 0 ? 0 : k_end - k2;
-        reinterpret_cast<int4*>(b.counters)[idx] = make_int4(it1, leaps, it2, 0);
+        const int it1 = (s.k2 < 0 ? k_end - s.k0 : s.k2 - s.k0) - s.skipped;
+        const int it2 = s.k2 < 0 ? 0 : k_end - s.k2;
+        reinterpret_cast<int4*>(b.counters)[s.idx] = make_int4(it1, s.leaps, it2, 0);
     }
+}
+
+// One pixel (i, j) of a coarse pass, start to finish.
+template <int ARITH, int FT, bool BLA>
+__device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFrameBuffers& b, int i,
+                                             int j) {
+    PixelRun s;
+    if (!pixel_begin<ARITH, FT>(p, b, i, j, s)) return;
+    pixel_advance<ARITH, FT, BLA, false>(p, b, s, 0);
+    pixel_finish(p, b, s);
 }
 
 }  // namespace ap

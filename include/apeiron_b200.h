@@ -350,8 +350,9 @@ AP_API int ap_decimal_arith(int32_t op, const int64_t* a_meta, const uint64_t* a
  * the number of each tile's first 256-pixel patch (patch_w x patch_h == 256) and the total;
  * tiles should come in decreasing order of expected cost.
  * ap_render_batch: renders all tiles with one persistent kernel of blocks_per_sm blocks per
- * SM whose warps take eighths of patches (32 pixels) from a shared counter (device word
- * *queue_head, reset here);
+ * SM whose lanes take pixels from a shared counter (device word *queue_head, reset here):
+ * each lane keeps one pixel, runs it 128 steps at a time, and a warp with 16 or more idle
+ * lanes refills them with consecutive pixels;
  * tiles and first_patch are device copies of the planned arrays.  min_blocks (4 or 6) picks
  * the register budget the kernel is compiled for; arith is the tiles' common profile.
  * Values equal ap_render_pass's for each tile. */
