@@ -1,11 +1,12 @@
 """Series-approximation ("BBSA") starts against the reference (tests/golden/bbsa_samples.npz).
 
   * ap_bbsa_coeffs (host code of the library, no GPU needed) reproduces
-    compute_bbsa_coeffs (math_core/high_precision.py:537-578): the skip exactly
-    and the 16 coefficients to 1e-11 relative, for orders 4 and 8 at two
-    tolerances on the Mandelbrot (config 3), Julia and Multibrot orbits;
+    compute_bbsa_coeffs (math_core/high_precision.py:537-578) bit for bit (skip
+    and all 16 coefficients), for orders 4 and 8 at two tolerances on the
+    Mandelbrot (config 3), Julia and Multibrot orbits;
   * perturbation samples started from the series (oracle, the same evaluation
-    the device runs) equal cpu_compute_perturbation_sample's values.
+    the device runs) equal cpu_compute_perturbation_sample's values;
+  * whole series-started frames equal render_frame_cpu's.
 """
 import ctypes as C
 from decimal import Decimal
@@ -43,8 +44,10 @@ def test_bbsa_coefficients_match_reference(tag):
     got = coeffs(m, bm["order"], bm["tol"])
     ref = B[tag + "__coeffs"]
     assert int(got[0]) == int(ref[0]) == bm["skip"]
-    scale = np.maximum(np.abs(ref[1:]), 1e-300)
-    assert np.all(np.abs(got[1:] - ref[1:]) <= 1e-11 * scale), np.max(np.abs(got[1:] - ref[1:]) / scale)
+    # bit for bit: the library evaluates the recurrence in the rounding order of the
+    # reference's compiled fast-math kernel
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64)), \
+        np.max(np.abs(got[1:] - ref[1:]) / np.maximum(np.abs(ref[1:]), 1e-300))
 
 
 def test_bbsa_disabled_cases_return_zero():
@@ -76,16 +79,9 @@ def test_series_started_samples_bit_exact(tag):
         int((s.view(np.uint32) != ref_s.view(np.uint32)).sum())
 
 
-# Escape-step agreement of whole frames (rebasing included) with render_frame_cpu when
-# the engine computes its own coefficients.  The reference evaluates the coefficient
-# recurrence with a fastmath kernel whose fused and reassociated forms are not
-# reproduced yet; the coefficients then differ by up to 5e-12 relative, which moves
-# the escape step of the frame's most sensitive pixels.  The Multibrot n = 3 view is
-# ill-conditioned under its series start: two FP64 evaluations whose coefficients
-# differ at 1e-12 disagree on a fifth of the pixels.
+# Whole frames (rebasing included) with the engine's own coefficients equal
+# render_frame_cpu's value for value, the ill-conditioned Multibrot n = 3 view too.
 R, RMETA = load_golden("render_bbsa.npz")
-FRAME_K_AGREEMENT = {"bbsa4_cfg3": 0.9998, "bbsa8_cfg3": 0.9999, "bbsa4_julia": 0.999,
-                     "bbsa8_multibrot3": 0.75}
 
 
 @pytest.mark.parametrize("name", [m["name"] for m in RMETA])
@@ -94,5 +90,5 @@ def test_series_started_frames_against_reference(name):
     m = next(x for x in RMETA if x["name"] == name)
     fr, _ = oracle_pert_frame(m)
     ref = R[name + "__iter"]
-    agree = float(np.mean(np.floor(fr.iter_map) == np.floor(ref)))
-    assert agree >= FRAME_K_AGREEMENT[name], agree
+    assert np.array_equal(fr.iter_map.view(np.uint32), ref.view(np.uint32)), \
+        int((fr.iter_map.view(np.uint32) != ref.view(np.uint32)).sum())
