@@ -528,24 +528,95 @@ def compute_dynamic_max_iter(base_max_iter, plot_width_dec, dynamic_mode,
         return clamped
 
 
+def plan_probe(center_x_dec, center_y_dec, plot_width_dec, search_max, target_w=128, target_h=72,
+               fractal_type=0, julia_cx=0.0, julia_cy=0.0, gen_n=3, gen_kr=0.25, gen_ki=1.0,
+               precision_mode="1e-300 (Perturbation)", bbsa_tol=1e-4, bbsa_order=4, arith=None):
+    """Parameters of the adaptive max-iter probe's one coarse pass (host code):
+    (ApFrameParams, (re, im, ref_len) of the reference orbit or None on the direct
+    tiers).  math_core/engine.py:1069-1278, the probe kernels of
+    math_core/cuda_kernels.py:1503-1584 and math_core/cpu_kernels.py:1024-1108.
+
+    Pixel (i, j) samples x_min + i dx, y_max - j dy with dx = w / (W - 1): the
+    view's corners are pixel centres, as on the render's grid at factor 1.  One
+    sample per pixel at max_iter ``search_max``, no chained-BLA leaps, no glitch
+    test, no colour; the tier is chosen as for a frame."""
+    if not isinstance(plot_width_dec, Decimal):
+        plot_width_dec = Decimal(str(plot_width_dec))
+    if not isinstance(center_x_dec, Decimal):
+        center_x_dec = Decimal(str(center_x_dec))
+    if not isinstance(center_y_dec, Decimal):
+        center_y_dec = Decimal(str(center_y_dec))
+    W, H = int(target_w), int(target_h)
+    if W < 1 or H < 1:
+        raise ValueError("target_w and target_h must be positive")
+    arith_code = _arith_code(arith if arith is not None else DEFAULT_ARITH)
+    tier = select_tier(plot_width_dec, precision_mode)
+    p = abi.new_params(width=W, height=H, factor=1, max_iter=int(search_max),
+                       fractal_type=int(fractal_type), tier=tier, arith=arith_code,
+                       gen_n=int(gen_n), gen_kr=float(gen_kr), gen_ki=float(gen_ki), scheme_id=0)
+    if tier in (abi.AP_TIER_FP64, abi.AP_TIER_DD):
+        for k, v in plan_direct_view(W, H, 1, center_x_dec, center_y_dec, plot_width_dec, tier,
+                                     julia_cx, julia_cy).items():
+            setattr(p, k, v)
+        if tier == abi.AP_TIER_FP64:
+            # the probe's FP64 spacing is a float division (math_core/engine.py:1188-1189),
+            # the frame's a Decimal one rounded once: they can differ in the last bit
+            with localcontext(decimal_context(plot_width_dec)):
+                h_f = float(plot_width_dec * (Decimal(H) / Decimal(W)))
+            p.dx_hi = float(plot_width_dec) / max(1, W - 1)
+            p.dy_hi = h_f / max(1, H - 1)
+        p.mode = abi.AP_MODE_COARSE
+        p.flags = abi.AP_FLAG_NO_RGB | (abi.AP_FLAG_MAP_FUSED if arith_code == abi.AP_ARITH_REF_CPU else 0)
+        return p, None
+    from . import perturbation
+    orbit = perturbation.probe_perturbation_params(
+        p, W=W, H=H, search_max=int(search_max), center_x_dec=center_x_dec, center_y_dec=center_y_dec,
+        plot_width_dec=plot_width_dec, tier=tier, fractal_type=int(fractal_type), julia_cx=julia_cx,
+        julia_cy=julia_cy, bbsa_tol=bbsa_tol, bbsa_order=bbsa_order, gen_n=gen_n, gen_kr=gen_kr,
+        gen_ki=gen_ki, arith_code=arith_code)
+    return p, orbit
+
+
+def probe_iter_map(center_x_dec, center_y_dec, plot_width_dec, search_max, target_w=128, target_h=72,
+                   fractal_type=0, julia_cx=0.0, julia_cy=0.0, gen_n=3, gen_kr=0.25, gen_ki=1.0,
+                   precision_mode="1e-300 (Perturbation)", bbsa_tol=1e-4, bbsa_order=4, arith=None,
+                   stream=0):
+    """Smooth escape values of the adaptive max-iter probe (plan_probe's pass on the
+    device), as a host float32 [target_h, target_w] array."""
+    torch = _torch()
+    L = _lib.load()
+    p, orbit = plan_probe(center_x_dec, center_y_dec, plot_width_dec, search_max, target_w, target_h,
+                          fractal_type, julia_cx, julia_cy, gen_n, gen_kr, gen_ki, precision_mode,
+                          bbsa_tol, bbsa_order, arith)
+    st, stream_h = _stream_handle(stream)
+    b = abi.ApFrameBuffers()
+    with torch.cuda.stream(st):
+        d_iter = get_scratch_device_array((p.height, p.width), np.float32, "probe_iter")
+        b.iter_map = _ptr(d_iter)
+        if orbit is not None:
+            from . import perturbation
+            d_re, d_im = perturbation._upload_orbit(torch, orbit[0], orbit[1], orbit[2], 0, "probe")
+            b.ref_re, b.ref_im = _ptr(d_re), _ptr(d_im)
+        _lib.launch(L.ap_render_pass, C.byref(p), C.byref(b), stream_h, what="ap_render_pass")
+        out = _copy_to_host(d_iter, None, st)
+    st.synchronize()
+    return out
+
+
 def probe_adaptive_max_iter(center_x_dec, center_y_dec, plot_width_dec, base_iter,
                             target_w=128, target_h=72, fractal_type=0,
                             julia_cx=0.0, julia_cy=0.0, gen_n=3, gen_kr=0.25, gen_ki=1.0,
                             precision_mode="1e-300 (Perturbation)", bbsa_tol=1e-4, bbsa_order=4,
-                            compute_device="GPU", cpu_threads=2):
-    """128x72 probe render that sets the iteration depth (math_core/engine.py:1063-1281).
-
-    The probe maps pixels at their un-offset positions (x_min + i*dx), as the
-    reference's probe kernels do, and searches up to max(1000, 2*base_iter).
-    """
+                            compute_device="GPU", cpu_threads=2, arith=None, stream=0):
+    """Iteration depth from a target_w x target_h probe (math_core/engine.py:1063-1281):
+    probe_iter_map searched to max(1000, 2 base_iter), then
+    get_adaptive_max_iter_from_probe.  ``arith`` selects the arithmetic profile
+    ("ref_cpu" default: the values of the reference's CPU probe kernels; "ref_cuda":
+    its device kernels)."""
     if compute_device == "CPU":
         raise NotImplementedError("this engine probes on the GPU only (compute_device='CPU')")
     search = min(GLOBAL_MAX_ITER, max(1000, int(base_iter * 2)))
-    h_iter = np.empty((target_h, target_w), np.float32)
-    render_frame_ssaa(target_w, target_h, search, center_x_dec, center_y_dec, plot_width_dec,
-                      None, ssaa_factor=1, color_scheme_id=0, precision_mode=precision_mode,
-                      fractal_type=fractal_type, julia_cx=julia_cx, julia_cy=julia_cy,
-                      bbsa_tol=bbsa_tol, bbsa_order=bbsa_order, glitch_mode="Off (Single-Ref)",
-                      gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki, h_iter_buf=h_iter,
-                      stream_slot=15)
-    return get_adaptive_max_iter_from_probe(h_iter, base_iter)
+    iters = probe_iter_map(center_x_dec, center_y_dec, plot_width_dec, search, target_w, target_h,
+                           fractal_type, julia_cx, julia_cy, gen_n, gen_kr, gen_ki, precision_mode,
+                           bbsa_tol, bbsa_order, arith=arith, stream=stream)
+    return get_adaptive_max_iter_from_probe(iters, base_iter)

@@ -263,6 +263,51 @@ def _coarse_params(p, fe32):
     return q
 
 
+def probe_perturbation_params(p, *, W, H, search_max, center_x_dec, center_y_dec, plot_width_dec,
+                              tier, fractal_type, julia_cx, julia_cy, bbsa_tol, bbsa_order, gen_n,
+                              gen_kr, gen_ki, arith_code):
+    """Reference orbit and parameters of the adaptive max-iter probe's perturbation
+    branches (math_core/engine.py:1120-1179 on the CPU, :1212-1278 on the device).
+
+    Unlike a frame: the series start keeps ``bbsa_tol`` / ``bbsa_order`` as given on
+    the FloatExp tier too, with its radius 0.75 w in 2^-E units there; no chained-BLA
+    leaps; no glitch test (strict_glitch 0).  The sample variant is the plain one: the
+    CPU kernels flag escape glitches and guard NaN, the device's plain sample
+    (math_core/cuda_kernels.py:422, :819) flags escape glitches only.  Returns the host
+    orbit (re, im, ref_len); ``p`` is filled for one coarse pass at factor 1."""
+    ctx = decimal_context(plot_width_dec)
+    floatexp = tier == abi.AP_TIER_FLOATEXP
+    with localcontext(ctx):
+        plot_height_dec = plot_width_dec * (Decimal(H) / Decimal(W))
+        e_scale = compute_floatexp_scale(plot_width_dec) if floatexp else 0
+        scale = Decimal(2) ** e_scale
+        w_view = plot_width_dec * scale
+        dx_f = float(w_view / Decimal(max(1, W - 1)))
+        dy_f = float(plot_height_dec * scale / Decimal(max(1, H - 1)))
+    bcx, bcy, bu, bv, re, im, ref_len = hp.find_optimal_reference_orbit(
+        center_x_dec, center_y_dec, plot_width_dec, plot_height_dec, search_max, W, H,
+        fractal_type=fractal_type, julia_cx=julia_cx, julia_cy=julia_cy, gen_n=gen_n,
+        gen_kr=gen_kr, gen_ki=gen_ki, is_floatexp=floatexp)
+    max_r = float(w_view) * 0.75
+    series = bbsa_coefficients(_lib.load(), re, im, ref_len, max_r, fractal_type, bbsa_tol, bbsa_order,
+                               gen_n, gen_kr, gen_ki, e_scale)
+    _set_series(p, series, 1.0 / max_r if max_r > 0.0 else 1.0)
+    p.dx_hi, p.dy_hi = dx_f, dy_f
+    p.ref_px = float(W - 1) * float(bu)
+    p.ref_py = float(H - 1) * float(bv)
+    p.ref_cx, p.ref_cy = float(bcx), float(bcy)
+    p.julia_cx_hi, p.julia_cy_hi = float(julia_cx), float(julia_cy)
+    p.ref_len = int(ref_len)
+    p.e_scale = int(e_scale)
+    p.bla_levels = 0
+    p.strict_glitch = 0
+    p.rebase_pass = 0
+    p.mode = abi.AP_MODE_COARSE
+    cpu_sem = arith_code == abi.AP_ARITH_REF_CPU
+    p.flags = abi.AP_FLAG_NO_RGB | abi.AP_FLAG_ESCAPE_GLITCH | (abi.AP_FLAG_NAN_GUARD if cpu_sem else 0)
+    return re, im, ref_len
+
+
 def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_iter, center_x_dec,
                               center_y_dec, plot_width_dec, tier, scheme, num_bins, fractal_type,
                               julia_cx, julia_cy, bbsa_tol, bbsa_order, glitch_mode, gen_n, gen_kr,

@@ -22,6 +22,7 @@ same inputs without the reference.  Sections:
   fexp     FloatExp perturbation samples at 1e-1000
            (math_core/cpu_kernels.py:606)
   render3  deep-zoom perturbation frames with Pauldelbrot rebasing
+  probe    adaptive max-iter probe maps and depths (math_core/engine.py:1063)
 """
 import hashlib
 import json
@@ -639,6 +640,73 @@ def gen_strict():
 
 
 # ---------------------------------------------------------------------------
+# Adaptive max-iter probe (math_core/engine.py:1063-1281, CPU branch)
+# ---------------------------------------------------------------------------
+def probe_cases():
+    wl = json.load(open(os.path.join(HERE, "workloads.json")))
+    cx3, cy3 = wl["config3_centre"]
+    cx2, cy2 = wl["config2_centre"]
+    pc = {c[0]: c for c in pert_cases()}
+    P, DD = "1e-300 (Perturbation)", "1e-24 (DD)"
+    cases = [
+        # name, cx, cy, width, base_iter, W, H, type, jx, jy, n, kr, ki, precision, bbsa_tol, bbsa_order
+        ("fp64_overview", "-0.65", "0.0", "3.0", 500, 128, 72, 0, 0.0, 0.0, 3, 0.25, 1.0, P, 1e-4, 4),
+        ("fp64_ship", "-1.75", "-0.03", "0.2", 400, 128, 72, 1, 0.0, 0.0, 3, 0.25, 1.0, P, 1e-4, 4),
+        ("fp64_multibrot4", "0.0", "0.0", "3.0", 300, 96, 54, 4, 0.0, 0.0, 4, 0.1, 0.2, P, 1e-4, 4),
+        ("dd_ship", cx2, cy2, "1e-20", 3000, 64, 36, 1, 0.0, 0.0, 3, 0.25, 1.0, DD, 1e-4, 4),
+        ("dd_mandel", "-0.10109636384562", "0.95628651080914", "4e-18", 1500, 64, 36, 0, 0.0, 0.0, 3, 0.25,
+         1.0, DD, 1e-4, 4),
+        ("pert_cfg3", cx3, cy3, "1e-160", 10000, 64, 36, 0, 0.0, 0.0, 3, 0.25, 1.0, P, 1e-4, 4),
+    ]
+    # No FloatExp view: the reference's CPU FloatExp probe kernel
+    # (math_core/cpu_kernels.py:1087) fails to compile in Numba ("Calling a closure
+    # with *args is unsupported"), so that branch raises; its device kernel is
+    # pinned in the CUDA simulator instead (make_golden_cudasim.py).
+    for (name, order, tol) in (("julia", 4, 1e-4), ("ship_julia", 4, 1e-4), ("multibrot3", 4, 1e-4),
+                               ("ship", 8, 1e-6)):
+        c = pc[name]
+        cases.append((f"pert_{name}", c[2], c[3], c[4], 3000, 64, 36, c[1], c[9], c[10], c[11], c[12], c[13],
+                      P, tol, order))
+    return cases
+
+
+def gen_probe():
+    """The reference's probe (probe_adaptive_max_iter with compute_device='CPU') on
+    views of every tier; its probe map is recorded where it hands it to
+    get_adaptive_max_iter_from_probe, with the depth it returns."""
+    E = R.engine
+    seen = []
+    orig = E.get_adaptive_max_iter_from_probe
+
+    def record(iters, base):
+        seen.append(np.array(iters, np.float32, copy=True))
+        return orig(iters, base)
+
+    E.get_adaptive_max_iter_from_probe = record
+    out = {}
+    meta = []
+    try:
+        for c in probe_cases():
+            (name, cx, cy, w, base, W, H, ft, jx, jy, n, kr, ki, prec, tol, order) = c
+            R.hp.clear_reference_orbit_cache()
+            seen.clear()
+            t0 = time.time()
+            depth = E.probe_adaptive_max_iter(
+                Decimal(cx), Decimal(cy), Decimal(w), base, target_w=W, target_h=H, fractal_type=ft,
+                julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki, precision_mode=prec,
+                bbsa_tol=tol, bbsa_order=order, compute_device="CPU", cpu_threads=8)
+            assert len(seen) == 1
+            print(f"  {name}: {time.time() - t0:.2f}s depth {depth} escaped {np.mean(seen[0] >= 0):.3f}")
+            out[name + "__iter"] = seen[0]
+            meta.append(dict(name=name, cx=cx, cy=cy, width=w, base_iter=base, W=W, H=H, fractal_type=ft,
+                             julia_cx=jx, julia_cy=jy, gen_n=n, gen_kr=kr, gen_ki=ki, precision_mode=prec,
+                             bbsa_tol=tol, bbsa_order=order, depth=int(depth)))
+    finally:
+        E.get_adaptive_max_iter_from_probe = orig
+    save("probe.npz", meta=json.dumps(meta), **out)
+
+
+# ---------------------------------------------------------------------------
 # Ground truth for precision checks: direct iteration in 700-bit arithmetic
 # (mpmath), independent of the reference and of perturbation theory.
 # ---------------------------------------------------------------------------
@@ -696,7 +764,8 @@ def gen_truth():
 
 SECTIONS = {"truth": gen_truth, "fp64": gen_fp64, "render1": gen_render1, "render2": gen_render2, "pert": gen_pert,
             "fexp": gen_fexp, "bbsa": gen_bbsa, "render_bbsa": gen_render_bbsa, "config4": gen_config4,
-            "render3": gen_render3, "strict": gen_strict}
+            "render3": gen_render3, "strict": gen_strict,
+            "probe": gen_probe}
 
 if __name__ == "__main__":
     wanted = sys.argv[1:] or list(SECTIONS)

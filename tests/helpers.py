@@ -228,3 +228,30 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
                                                          m["julia_cy"])
             oracle.strict_eval(q, fr, view, coords, signs, limbs)
     return fr, state.passes
+
+
+def probe_search(base_iter):
+    """Probe depth searched for a base depth (math_core/engine.py:1069)."""
+    from fractura_b200.config import GLOBAL_MAX_ITER
+    return min(GLOBAL_MAX_ITER, max(1000, int(base_iter * 2)))
+
+
+def probe_args(m):
+    """Positional arguments of engine.plan_probe / probe_iter_map for a probe case."""
+    return (Decimal(m["cx"]), Decimal(m["cy"]), Decimal(m["width"]), probe_search(m["base_iter"]),
+            m["W"], m["H"], m["fractal_type"], m["julia_cx"], m["julia_cy"], m["gen_n"], m["gen_kr"],
+            m["gen_ki"], m["precision_mode"], m["bbsa_tol"], m["bbsa_order"])
+
+
+def oracle_probe(m, arith=abi.AP_ARITH_REF_CPU):
+    """Probe map of a probe case through the oracle, on the pass engine.plan_probe plans."""
+    from fractura_b200 import engine
+    from fractura_b200 import high_precision as hp
+    hp.clear_reference_orbit_cache()
+    p, orbit = engine.plan_probe(*probe_args(m), arith=arith)
+    fr = oracle.Frame(m["W"], m["H"], lut=synthetic_lut())
+    if orbit is not None:
+        re, im, rl = orbit
+        fr.ref_re, fr.ref_im = np.ascontiguousarray(re[:rl + 1]), np.ascontiguousarray(im[:rl + 1])
+    oracle.render_pass(p, fr)
+    return fr.iter_map
