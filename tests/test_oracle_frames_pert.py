@@ -7,11 +7,13 @@ from helpers import load_golden, oracle_pert_frame, rgb_mismatch
 
 G, META = load_golden("render_pert.npz")
 
-# The reference's histogram kernel (math_core/cpu_kernels.py:1887) is compiled with
-# fastmath; where LLVM inlines the per-sample function into its supersampling loop the
-# backend contracts that function's multiply-adds, so the smooth values of pixels it
-# re-renders on rebase passes move by a few ulps.  Those pixels are still flagged as
-# glitched in the final map; every other pixel is bit-exact.
+# The reference's histogram kernel (math_core/cpu_kernels.py:1887, fastmath) calls
+# cpu_compute_perturbation_sample with float coordinates at factor 1 and with int64
+# coordinates in its supersampling loop.  Numba compiles the int64 specialisation with
+# the caller's fast-math flags (every floating-point operation of that copy is `fast`;
+# the float copy has none), so its sums are reassociated and fused differently.  The
+# samples it re-renders on rebase passes move slightly; those pixels are still flagged
+# as glitched in the final map, and every other pixel is bit-exact.
 FASTMATH_INLINED = {"cfg3_hist_ssaa2"}
 
 
