@@ -84,29 +84,24 @@ inline void add_s(Fx& r, const Fx& a, int an, const Fx& b, int bn, int L) {
 inline void add(Fx& r, const Fx& a, const Fx& b, int L) { add_s(r, a, a.neg, b, b.neg, L); }
 inline void sub(Fx& r, const Fx& a, const Fx& b, int L) { add_s(r, a, a.neg, b, !b.neg, L); }
 
-// 192-bit column accumulator of the product-scanning (Comba) products below.
+// Column accumulator of the product-scanning (Comba) products below: the value is
+// lo + hi * 2^64, the low and high halves of the products summed in two independent
+// 128-bit sums (a column has at most 2 * kMaxLimbs products, so neither overflows).
+// The carry into the next column is formed once per column, in shift().
 struct Acc3 {
-    u64 c0 = 0, c1 = 0, c2 = 0;
+    u128 lo = 0, hi = 0;
     inline void add(u128 p) {
-        const u128 s0 = (u128)c0 + (u64)p;
-        c0 = (u64)s0;
-        const u128 s1 = (u128)c1 + (u64)(p >> 64) + (u64)(s0 >> 64);
-        c1 = (u64)s1;
-        c2 += (u64)(s1 >> 64);
+        lo += (u64)p;
+        hi += (u64)(p >> 64);
     }
-    inline void add_twice(const Acc3& o) {  // += 2 * o (o below 2^191)
-        const u64 d0 = o.c0 << 1, d1 = (o.c1 << 1) | (o.c0 >> 63), d2 = (o.c2 << 1) | (o.c1 >> 63);
-        const u128 s0 = (u128)c0 + d0;
-        c0 = (u64)s0;
-        const u128 s1 = (u128)c1 + d1 + (u64)(s0 >> 64);
-        c1 = (u64)s1;
-        c2 += d2 + (u64)(s1 >> 64);
+    inline void add_twice(const Acc3& o) {  // += 2 * o
+        lo += o.lo << 1;
+        hi += o.hi << 1;
     }
-    inline u64 shift() {  // take the finished column, move the carries down
-        const u64 out = c0;
-        c0 = c1;
-        c1 = c2;
-        c2 = 0;
+    inline u64 shift() {  // take the finished column, keep the rest as the carry
+        const u64 out = (u64)lo;
+        lo = (lo >> 64) + hi;
+        hi = 0;
         return out;
     }
 };
@@ -157,6 +152,44 @@ inline void twice(Fx& r, const Fx& a, int L) {
         carry = v >> 63;
     }
     r.neg = a.neg;
+}
+
+// mul and sqr with the limb counts fixed at compile time: the same partial products
+// and column sums, with loop bounds the compiler can unroll.  An orbit picks its pair
+// once (pick_products); sizes outside the table use the runtime-bound forms.
+using MulFn = void (*)(Fx&, const Fx&, const Fx&);
+using SqrFn = void (*)(Fx&, const Fx&);
+
+template <int L, int I>
+void mul_fixed(Fx& r, const Fx& a, const Fx& b) { mul(r, a, b, L, I); }
+
+template <int L, int I>
+void sqr_fixed(Fx& r, const Fx& a) { sqr(r, a, L, I); }
+
+struct Products {
+    MulFn mul = nullptr;
+    SqrFn sqr = nullptr;
+};
+
+template <int I>
+Products pick_for(int L) {
+    switch (L) {
+#define AP_FIXED_LIMBS(n) \
+    case n: return {mul_fixed<n, I>, sqr_fixed<n, I>};
+        AP_FIXED_LIMBS(3) AP_FIXED_LIMBS(4) AP_FIXED_LIMBS(5) AP_FIXED_LIMBS(6) AP_FIXED_LIMBS(7)
+        AP_FIXED_LIMBS(8) AP_FIXED_LIMBS(9) AP_FIXED_LIMBS(10) AP_FIXED_LIMBS(11) AP_FIXED_LIMBS(12)
+        AP_FIXED_LIMBS(13) AP_FIXED_LIMBS(14) AP_FIXED_LIMBS(15) AP_FIXED_LIMBS(16) AP_FIXED_LIMBS(17)
+        AP_FIXED_LIMBS(18) AP_FIXED_LIMBS(19) AP_FIXED_LIMBS(20) AP_FIXED_LIMBS(21) AP_FIXED_LIMBS(22)
+        AP_FIXED_LIMBS(23) AP_FIXED_LIMBS(24)
+#undef AP_FIXED_LIMBS
+    default: return {};
+    }
+}
+
+Products pick_products(int L, int I) {
+    if (I == 1) return pick_for<1>(L);
+    if (I == 2) return pick_for<2>(L);
+    return {};
 }
 
 // Correctly rounded float64 (round half to even) of a sign-magnitude value.
@@ -243,6 +276,15 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
         return AP_E_INVALID;
     }
     const int L = limbs, I = int_limbs;
+    const Products fixed = pick_products(L, I);
+    auto MUL = [&](Fx& r, const Fx& a, const Fx& b) {
+        if (fixed.mul) fixed.mul(r, a, b);
+        else mul(r, a, b, L, I);
+    };
+    auto SQR = [&](Fx& r, const Fx& a) {
+        if (fixed.sqr) fixed.sqr(r, a);
+        else sqr(r, a, L, I);
+    };
     // seeds: z0_re, z0_im, c_re, c_im, k_re, k_im, each L limbs
     std::vector<Fx> v(16);
     Fx &zx = v[0], &zy = v[1], &cx = v[2], &cy = v[3], &kr = v[4], &ki = v[5];
@@ -286,8 +328,8 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
                 mix(im);
             }
         }
-        sqr(zx2, zx, L, I);
-        sqr(zy2, zy, L, I);
+        SQR(zx2, zx);
+        SQR(zy2, zy);
         add(mag, zx2, zy2, L);
         if (!mag.neg && cmp_mag(mag.m, bail.m, L) > 0) {
             len = k;
@@ -312,13 +354,13 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
             }
         }
         if (fractal_type == 0 || fractal_type == 2) {  // z^2 + c
-            mul(t0, zx, zy, L, I);
+            MUL(t0, zx, zy);
             sub(t1, zx2, zy2, L);
             add(zx, t1, cx, L);
             twice(t0, t0, L);
             add(zy, t0, cy, L);
         } else if (fractal_type == 1 || fractal_type == 3) {  // Burning Ship: 2|x||y| - c_y
-            mul(t0, zx, zy, L, I);
+            MUL(t0, zx, zy);
             t0.neg = 0;  // |x| |y|
             sub(t1, zx2, zy2, L);
             add(zx, t1, cx, L);
@@ -330,17 +372,17 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
             nr = zx;
             ni = zy;
             for (int t = 0; t < gen_n - 1; ++t) {
-                mul(t0, nr, zx, L, I);
-                mul(t1, ni, zy, L, I);
-                mul(t2, nr, zy, L, I);
-                mul(t3, ni, zx, L, I);
+                MUL(t0, nr, zx);
+                MUL(t1, ni, zy);
+                MUL(t2, nr, zy);
+                MUL(t3, ni, zx);
                 sub(nr, t0, t1, L);
                 add(ni, t2, t3, L);
             }
-            mul(t0, kr, zx, L, I);
-            mul(t1, ki, zy, L, I);
-            mul(t2, kr, zy, L, I);
-            mul(t3, ki, zx, L, I);
+            MUL(t0, kr, zx);
+            MUL(t1, ki, zy);
+            MUL(t2, kr, zy);
+            MUL(t3, ki, zx);
             sub(t0, t0, t1, L);  // Re(K z)
             add(t2, t2, t3, L);  // Im(K z)
             add(t0, nr, t0, L);
