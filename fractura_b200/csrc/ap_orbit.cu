@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "ap_common.cuh"
@@ -155,16 +156,67 @@ inline void twice(Fx& r, const Fx& a, int L) {
 }
 
 // mul and sqr with the limb counts fixed at compile time: the same partial products
-// and column sums, with loop bounds the compiler can unroll.  An orbit picks its pair
+// and column sums as mul / sqr, every column written out by the templates below.  An orbit picks its pair
 // once (pick_products); sizes outside the table use the runtime-bound forms.
 using MulFn = void (*)(Fx&, const Fx&, const Fx&);
 using SqrFn = void (*)(Fx&, const Fx&);
 
-template <int L, int I>
-void mul_fixed(Fx& r, const Fx& a, const Fx& b) { mul(r, a, b, L, I); }
+// Column col of a product: the partial products a[i] * b[col - i] for i in [i0, i0 + n),
+// one expression each (a fold over an index sequence), so every column is unrolled.
+template <int COL, int I0, size_t... K>
+inline void column_sum(Acc3& acc, const u64* a, const u64* b, std::index_sequence<K...>) {
+    (acc.add((u128)a[I0 + (int)K] * b[COL - I0 - (int)K]), ...);
+}
+
+template <int L, int I, int COL>
+inline void mul_column(Acc3& acc, const u64* a, const u64* b, u64* r) {
+    constexpr int i0 = COL - (L - 1) > 0 ? COL - (L - 1) : 0;
+    constexpr int i1 = COL < L - 1 ? COL : L - 1;
+    column_sum<COL, i0>(acc, a, b, std::make_index_sequence<i1 - i0 + 1>{});
+    const u64 limb = acc.shift();
+    if constexpr (COL >= L - I) r[COL - (L - I)] = limb;
+}
+
+template <int L, int I, size_t... C>
+inline void mul_columns(Acc3& acc, const u64* a, const u64* b, u64* r, std::index_sequence<C...>) {
+    constexpr int lo = L - I - 2 > 0 ? L - I - 2 : 0;
+    (mul_column<L, I, lo + (int)C>(acc, a, b, r), ...);
+}
+
+// Off-diagonal pairs of column col of a square (i < col - i), summed once.
+template <int L, int I, int COL>
+inline void sqr_column(Acc3& acc, const u64* a, u64* r) {
+    constexpr int i0 = COL - (L - 1) > 0 ? COL - (L - 1) : 0;
+    constexpr int n_off = (COL + 1) / 2 - i0 > 0 ? (COL + 1) / 2 - i0 : 0;  // i in [i0, ceil(col/2))
+    Acc3 off;
+    column_sum<COL, i0>(off, a, a, std::make_index_sequence<n_off>{});
+    acc.add_twice(off);
+    if constexpr ((COL & 1) == 0 && COL / 2 < L) acc.add((u128)a[COL / 2] * a[COL / 2]);
+    const u64 limb = acc.shift();
+    if constexpr (COL >= L - I) r[COL - (L - I)] = limb;
+}
+
+template <int L, int I, size_t... C>
+inline void sqr_columns(Acc3& acc, const u64* a, u64* r, std::index_sequence<C...>) {
+    constexpr int lo = L - I - 2 > 0 ? L - I - 2 : 0;
+    (sqr_column<L, I, lo + (int)C>(acc, a, r), ...);
+}
 
 template <int L, int I>
-void sqr_fixed(Fx& r, const Fx& a) { sqr(r, a, L, I); }
+void mul_fixed(Fx& r, const Fx& a, const Fx& b) {
+    constexpr int lo = L - I - 2 > 0 ? L - I - 2 : 0, top = 2 * L - I - 1;
+    Acc3 acc;
+    mul_columns<L, I>(acc, a.m, b.m, r.m, std::make_index_sequence<top - lo + 1>{});
+    r.neg = (a.neg ^ b.neg) && !is_zero(r.m, L);
+}
+
+template <int L, int I>
+void sqr_fixed(Fx& r, const Fx& a) {
+    constexpr int lo = L - I - 2 > 0 ? L - I - 2 : 0, top = 2 * L - I - 1;
+    Acc3 acc;
+    sqr_columns<L, I>(acc, a.m, r.m, std::make_index_sequence<top - lo + 1>{});
+    r.neg = 0;
+}
 
 struct Products {
     MulFn mul = nullptr;
