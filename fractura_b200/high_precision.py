@@ -106,11 +106,11 @@ def _probe_pool():
 
 def _pair_pool():
     """Threads that run the higher-precision orbit beside the lower one (the native
-    call releases the GIL); one per core, since a batch computes many orbits at once."""
+    call releases the GIL)."""
     global _PAIR_POOL
     with _PAIR_LOCK:
         if _PAIR_POOL is None:
-            _PAIR_POOL = ThreadPoolExecutor(max_workers=max(4, os.cpu_count() or 4), thread_name_prefix="orbit")
+            _PAIR_POOL = ThreadPoolExecutor(max_workers=4, thread_name_prefix="orbit")
         return _PAIR_POOL
 
 
