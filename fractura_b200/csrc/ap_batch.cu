@@ -23,8 +23,9 @@ static_assert(sizeof(ApTileDesc) % 16 == 0, "tile descriptors are 16-byte aligne
 // Steps a lane runs on its pixel before the warp lets lanes whose pixel finished take
 // new ones (lanes wait at most this long for each other), and the number of idle lanes
 // that triggers a refill.  Refilling single lanes scatters the warp's orbit indices
-// (one record load per lane instead of one per warp); 128 / 16 was the fastest pair
-// on the 64-tile batch (quanta 128-2048, thresholds 8-32).
+// (one record load per lane instead of one per warp).  On the 64-tile batch quanta
+// 96-160 with thresholds 16-20 are equally fast (within 1 %); threshold 12 and below,
+// or quanta of 512 and above, are slower (quanta 96-2048, thresholds 8-32 tried).
 #ifndef AP_BATCH_QUANTUM
 #define AP_BATCH_QUANTUM 128
 #endif
