@@ -142,3 +142,40 @@ def test_fixed_point_conversion():
     with pytest.raises(OverflowError):
         hp.to_fixed(Decimal(2) ** 70, 2)
     assert [hp.orbit_int_limbs(t, n) for t, n in ((0, 3), (1, 3), (4, 3), (4, 4), (4, 8))] == [1, 1, 1, 2, 3]
+
+
+@pytest.mark.parametrize("int_limbs", [1, 2])
+@pytest.mark.parametrize("fractal_type,gen_n", [(0, 2), (1, 2), (4, 5)])
+def test_fixed_size_products_at_every_size(fractal_type, gen_n, int_limbs):
+    """The products with compile-time limb counts (3-24 limbs) give the orbit the
+    runtime-bound products give: a point that escapes within a few dozen steps has the
+    same float64 orbit at every precision with 64 or more fractional bits beyond a
+    double's, so each table size must match the 40-limb run (runtime path) exactly."""
+    need = hp.orbit_int_limbs(fractal_type, gen_n)
+    if int_limbs < need:
+        pytest.skip("needs more integer limbs")
+    # just past the cusp at 1/4 (about 30 steps), and an outer Multibrot point
+    cx, cy = Decimal("0.2600000000000000123"), Decimal("0.0010000000000000456")
+    if fractal_type == 4:
+        cx, cy = Decimal("0.41"), Decimal("0.53")
+
+    import ctypes as C
+    from fractura_b200 import _lib
+    lib = hp._native()
+
+    def run(L):
+        sd = hp._seeds(fractal_type, cx, cy, 0.0, 0.0, 0.25, 1.0, L, int_limbs)
+        re, im = np.zeros(401), np.zeros(401)
+        n, m2 = C.c_int32(0), C.c_double(0.0)
+        _lib.check(lib.ap_reference_orbit(sd.ctypes.data_as(C.c_void_p), L, int_limbs, fractal_type, gen_n, 400,
+                                          0, re.ctypes.data_as(C.c_void_p), im.ctypes.data_as(C.c_void_p),
+                                          C.byref(n), C.byref(m2), None), "ap_reference_orbit")
+        return re, im, n.value
+
+    want = run(40)  # beyond the fixed-size table: the runtime-bound products
+    assert 2 < want[2] < 400
+    k = want[2] + 1
+    for L in range(int_limbs + 2, 25):
+        re, im, n = run(L)
+        assert n == want[2], (L, n, want[2])
+        assert np.array_equal(re[:k], want[0][:k]) and np.array_equal(im[:k], want[1][:k]), L
