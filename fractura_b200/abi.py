@@ -5,7 +5,7 @@ compares the sizes against the library's own ``sizeof`` report.
 """
 import ctypes as C
 
-AP_ABI_VERSION = 5
+AP_ABI_VERSION = 6
 
 AP_OK = 0
 AP_E_INVALID = -1
@@ -31,6 +31,7 @@ AP_FLAG_NAN_GUARD = 4
 AP_FLAG_ITER_LAST_SUB = 8
 AP_FLAG_MAP_FUSED = 16
 AP_FLAG_HIST_COLOUR = 32
+AP_FLAG_REBASE = 64
 
 
 class ApFrameParams(C.Structure):

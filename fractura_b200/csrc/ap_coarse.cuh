@@ -45,6 +45,7 @@ struct PixelRun {
     double dcx, dcy;  // the pixel's offset from the reference
     int idx, k, k0, k2, glitch, leaps, skipped;
     int stage;        // 1 perturbation, 2 direct, 3 done
+    int m, rebases;   // one-pass rebasing: reference index (k counts iterations), restarts
     SampleOut o;
 };
 
@@ -81,6 +82,8 @@ __device__ __forceinline__ bool pixel_begin(const ApFrameParams& p, const ApFram
         }
     }
     s.k0 = s.k;
+    s.m = s.k;
+    s.rebases = 0;
     s.k2 = -1;
     s.glitch = s.leaps = s.skipped = 0;
     s.stage = 1;
@@ -296,6 +299,158 @@ __device__ __forceinline__ void pixel_advance(const ApFrameParams& p, const ApFr
     s.o = o;
 }
 
+// One-pass rebasing (AP_FLAG_REBASE), for orbits that start at Z_0 = 0 (fractal
+// types 0, 1, 4).  k counts the pixel's iterations, m indexes the reference.  At
+// each step z = Z_m + dz is tested for escape; when |z| < |dz| -- the delta has
+// outgrown the value it perturbs, where a plain delta would lose its precision --
+// or when the reference has ended (m == ref_len), the delta restarts from the start
+// of the orbit: dz <- z, m <- 0 (Zhuoran, fractalforums.org 2021).  A pixel is never
+// flagged glitched (only a NaN/Inf delta is) and never falls back to direct
+// iteration, so one pass serves every pixel.  The packed safe radius also rules
+// out the rebase test (|dz| < |Z|/2), so the common path is the same single branch
+// as pixel_advance's.  Leaps are capped so that k never passes max_iter.
+template <int ARITH, int FT, bool BLA, bool BUDGET>
+__device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApFrameBuffers& b, PixelRun& s,
+                                               int budget) {
+    constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
+    const int ref_len = p.ref_len, max_iter = p.max_iter;
+    const double4* __restrict__ orb = reinterpret_cast<const double4*>(b.orbit_packed);
+    const double inv_ln = inv_ln_for(p.fractal_type, p.gen_n);
+    const double* __restrict__ R = b.bla_packed;
+    const double4* __restrict__ AB = reinterpret_cast<const double4*>(b.bla_packed + (size_t)ref_len * 16);
+    const int max_level = p.bla_levels - 1;
+    const double dcpx = s.dcx, dcpy = s.dcy;
+    int k = s.k, m = s.m, glitch = s.glitch, leaps = s.leaps, skipped = s.skipped, rebases = s.rebases;
+    double dzx = s.dzx, dzy = s.dzy;
+    SampleOut o = s.o;
+    bool paused = false;
+    while (k < max_iter) {
+        if (BUDGET && --budget < 0) {
+            paused = true;
+            break;
+        }
+        const double4 Z = ldg4(orb + m);
+        const double rx = Z.x, ry = Z.y;
+        const double zx = rx + dzx, zy = ry + dzy;
+        const double dz_mag2 = dzx * dzx + dzy * dzy;
+        const bool unsafe = !(dz_mag2 < Z.z) || m == ref_len;
+        const bool leap = BLA && (dz_mag2 < Z.w);
+        if (unsafe || leap) {
+            if (unsafe) {
+                const double mag2 = zx * zx + zy * zy;
+                if (!(mag2 <= kBailout)) {
+                    if (isnan(mag2)) {
+                        o = interior_sample();
+                        o.s = (float)k;
+                        o.s64 = (double)k;
+                        o.k = k;
+                        glitch = 1;
+                    } else {
+                        o = escaped_sample(k, mag2, inv_ln);
+                    }
+                    s.stage = 3;
+                    break;
+                }
+                if (mag2 < dz_mag2 || (m == ref_len && m > 0)) {
+                    dzx = zx;
+                    dzy = zy;
+                    m = 0;
+                    ++rebases;
+                    continue;
+                }
+            }
+            if (leap) {
+                const double* row = R + (size_t)m * 16;
+                int hi = max_level;
+                if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
+                hi = min(hi, 31 - __clz(max_iter - k));  // k + 2^lo <= max_iter
+                int q = 0;
+#pragma unroll
+                for (int t = 1; t <= 3; ++t)
+                    q += (4 * t <= hi && dz_mag2 < __ldg(row + 4 * t)) ? 1 : 0;
+                int lo = 4 * q;
+#pragma unroll
+                for (int t = 1; t <= 3; ++t) {
+                    const int d = 4 * q + t;
+                    lo += (d <= hi && dz_mag2 < __ldg(row + d)) ? 1 : 0;
+                }
+                const double4 e = ldg4(AB + (size_t)m * 16 + lo);
+                double nx, ny;
+                if (kCpu) {
+                    nx = (e.x * dzx - e.y * dzy) + (e.z * dcpx - e.w * dcpy);
+                    ny = (e.x * dzy + e.y * dzx) + (e.z * dcpy + e.w * dcpx);
+                } else {
+                    nx = fma(e.x, dzx, fma(-e.y, dzy, fma(e.z, dcpx, -e.w * dcpy)));
+                    ny = fma(e.x, dzy, fma(e.y, dzx, fma(e.z, dcpy, e.w * dcpx)));
+                }
+                dzx = nx;
+                dzy = ny;
+                if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) {
+                    o = interior_sample();
+                    o.s = (float)k;
+                    o.s64 = (double)k;
+                    o.k = k;
+                    glitch = 1;
+                    s.stage = 3;
+                    break;
+                }
+                m += 1 << lo;
+                k += 1 << lo;
+                ++leaps;
+                skipped += 1 << lo;
+                continue;
+            }
+        }
+        if (FT == kFtQuad) {
+            double nx, ny;
+            if (kCpu) {
+                nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+                ny = 2.0 * (zx * dzy + ry * dzx) + dcpy;
+            } else {
+                nx = fma(2.0 * rx + dzx, dzx, fma(-(2.0 * ry + dzy), dzy, dcpx));
+                ny = fma(2.0, fma(zx, dzy, ry * dzx), dcpy);
+            }
+            dzx = nx;
+            dzy = ny;
+        } else if (FT == kFtShip) {
+            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+            const double ddx = zx * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+            const double ddy = zy * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcpy;
+            dzx = nx;
+        } else {
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p.gen_n - 1; ++t) {
+                const double t1r = pr * rx - pi * ry, t1i = pr * ry + pi * rx;
+                const double sr = pr + qr, si = pi + qi;
+                const double t2r = sr * dzx - si * dzy, t2i = sr * dzy + si * dzx;
+                pr = t1r + t2r;
+                pi = t1i + t2i;
+                const double nqr = qr * rx - qi * ry, nqi = qr * ry + qi * rx;
+                qr = nqr;
+                qi = nqi;
+            }
+            const double kzr = p.gen_kr * dzx - p.gen_ki * dzy;
+            const double kzi = p.gen_kr * dzy + p.gen_ki * dzx;
+            dzx = pr + kzr + dcpx;
+            dzy = pi + kzi + dcpy;
+        }
+        ++m;
+        ++k;
+    }
+    if (!paused) s.stage = 3;
+    s.dzx = dzx;
+    s.dzy = dzy;
+    s.k = k;
+    s.m = m;
+    s.glitch = glitch;
+    s.leaps = leaps;
+    s.skipped = skipped;
+    s.rebases = rebases;
+    s.o = o;
+}
+
 __device__ __forceinline__ void pixel_finish(const ApFrameParams& p, const ApFrameBuffers& b, const PixelRun& s) {
     const int max_iter = p.max_iter;
     const int k_end = (s.o.k == -1) ? max_iter : s.k;
@@ -306,17 +461,20 @@ __device__ __forceinline__ void pixel_finish(const ApFrameParams& p, const ApFra
     if (b.counters) {
         const int it1 = (s.k2 < 0 ? k_end - s.k0 : s.k2 - s.k0) - s.skipped;
         const int it2 = s.k2 < 0 ? 0 : k_end - s.k2;
-        reinterpret_cast<int4*>(b.counters)[s.idx] = make_int4(it1, s.leaps, it2, 0);
+        reinterpret_cast<int4*>(b.counters)[s.idx] = make_int4(it1, s.leaps, it2, s.rebases);
     }
 }
 
-// One pixel (i, j) of a coarse pass, start to finish.
-template <int ARITH, int FT, bool BLA>
+// One pixel (i, j) of a coarse pass, start to finish (REBASE: AP_FLAG_REBASE).
+template <int ARITH, int FT, bool BLA, bool REBASE>
 __device__ __forceinline__ void coarse_pixel(const ApFrameParams& p, const ApFrameBuffers& b, int i,
                                              int j) {
     PixelRun s;
     if (!pixel_begin<ARITH, FT>(p, b, i, j, s)) return;
-    pixel_advance<ARITH, FT, BLA, false>(p, b, s, 0);
+    if (REBASE)
+        rebase_advance<ARITH, FT, BLA, false>(p, b, s, 0);
+    else
+        pixel_advance<ARITH, FT, BLA, false>(p, b, s, 0);
     pixel_finish(p, b, s);
 }
 

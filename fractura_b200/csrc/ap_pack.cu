@@ -13,15 +13,16 @@ __global__ void __launch_bounds__(256) pack_orbit_kernel(const double* __restric
     if (k >= n) return;
     const double rx = re[k], ry = im[k];
     const double r_mag2 = rx * rx + ry * ry;
-    const double thr = r_mag2 > 1e-8 ? 1e-6 * r_mag2 : -1.0;  // the Pauldelbrot threshold
     // Safe radius s: for |dz| < s the rounded |Z + dz|^2 is neither above the
-    // bailout 65536 (|Z| + s <= 256 (1 - 1e-12)) nor below the Pauldelbrot
-    // threshold 1e-6 |Z|^2 (|Z| - s >= 1e-3 |Z| (1 + 1e-7)); the 1e-12 margins
-    // cover the roundings of |Z|, of Z + dz and of both squares.  Stored as
+    // bailout 65536 (|Z| + s <= 256 (1 - 1e-12)), nor below the Pauldelbrot
+    // threshold 1e-6 |Z|^2, nor below the rounded |dz|^2 (the rebase test):
+    // s <= |Z| (1 - 1e-7) / 2 keeps |Z + dz| >= |Z| - s > s (1 + 1e-7) > |dz|,
+    // and 1e-6 |Z|^2 < s^2 covers the Pauldelbrot threshold.  The 1e-12 margins
+    // cover the roundings of |Z|, of Z + dz and of the squares.  Stored as
     // s^2 (1 - 1e-12) to be compared with the rounded |dz|^2.
     const double rz = sqrt(r_mag2);
     double s = 256.0 * (1.0 - 1e-12) - rz * (1.0 + 1e-12);
-    if (thr >= 0.0) s = fmin(s, rz * (1.0 - 1e-12) * (1.0 - 1.0000001e-3));
+    s = fmin(s, rz * (1.0 - 1e-12) * 0.5 * (1.0 - 1e-7));
     s = s > 0.0 ? s : 0.0;
     // slot 3: the level-0 BLA radius, written by ap_pack_bla (0: no leap)
     out[k] = make_double4(rx, ry, s * s * (1.0 - 1e-12), 0.0);

@@ -44,10 +44,134 @@ __device__ __forceinline__ SampleOut glitch_sample(int k) {
     return o;
 }
 
+// One-pass rebasing (AP_FLAG_REBASE; fractal types 0, 1, 4, whose orbits start at
+// Z_0 = 0): k counts the pixel's iterations, m indexes the reference.  z = Z_m + dz
+// is tested for escape at every step; when |z| < |dz| or the reference has ended
+// (m == ref_len) the delta restarts from the orbit's start, dz <- z, m <- 0
+// (Zhuoran, fractalforums.org 2021).  The leap takes the largest admissible level
+// that ends before the orbit does and does not carry k past max_iter.  Same values as
+// the packed coarse kernel's rebase_advance (ap_coarse.cuh).
+template <int ARITH>
+__device__ __forceinline__ SampleOut rebase_sample_at(const ApFrameParams& p, const ApFrameBuffers& b,
+                                                      double sub_i, double sub_j) {
+    constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
+    const int ft = p.fractal_type;
+    const int ref_len = p.ref_len, max_iter = p.max_iter;
+    const double* __restrict__ re = b.ref_re;
+    const double* __restrict__ im = b.ref_im;
+    const double dcy = (p.ref_py - sub_j) * p.dy_hi;
+    const double dcx = (sub_i - p.ref_px) * p.dx_hi;
+    double dzx = 0.0, dzy = 0.0;
+    int k = 0;
+    if (p.bbsa_skip > 0 && ft != 1) {
+        const double ux = dcx * p.bbsa_inv_r, uy = dcy * p.bbsa_inv_r;
+        if (ux * ux + uy * uy <= 1.0) {
+            const cplx d = bbsa_eval(p.bbsa, ux, uy);
+            dzx = d.r;
+            dzy = d.i;
+            k = p.bbsa_skip;
+        }
+    }
+    const int k0 = k;
+    int m = k, leaps = 0, skipped = 0;
+    auto done = [&](SampleOut o, int k_end) {
+        o.iters = k_end - k0 - skipped;
+        o.iters2 = 0;
+        o.leaps = leaps;
+        return o;
+    };
+    const int levels = p.bla_levels;
+    const bool has_bla = levels > 1 && b.bla != nullptr && (ft == 0 || ft == 4);
+    const size_t L = (size_t)ref_len;
+    const double inv_ln = inv_ln_for(ft, p.gen_n);
+    while (k < max_iter) {
+        const double rx = __ldg(re + m), ry = __ldg(im + m);
+        const double zx = rx + dzx, zy = ry + dzy;
+        const double mag2 = zx * zx + zy * zy;
+        if (!(mag2 <= kBailout)) {
+            if (isnan(mag2)) return done(glitch_sample(k), k);
+            return done(escaped_sample(k, mag2, inv_ln), k);
+        }
+        const double dz_mag2 = dzx * dzx + dzy * dzy;
+        if (mag2 < dz_mag2 || (m == ref_len && m > 0)) {
+            dzx = zx;
+            dzy = zy;
+            m = 0;
+            continue;
+        }
+        if (has_bla && m < ref_len - 1 && dz_mag2 < __ldg(b.bla + (size_t)m * 5 + 4)) {
+            int best = 0, max_d = levels - 1;
+            if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) max_d = min(max_d, 8);
+            max_d = min(max_d, 31 - __clz(max_iter - k));
+            for (int d = max_d; d > 0; --d) {
+                if (m + (1 << d) < ref_len && dz_mag2 < __ldg(b.bla + ((size_t)d * L + m) * 5 + 4)) {
+                    best = d;
+                    break;
+                }
+            }
+            const double* e = b.bla + ((size_t)best * L + m) * 5;
+            const double ar = __ldg(e), ai = __ldg(e + 1), br = __ldg(e + 2), bi = __ldg(e + 3);
+            double nx, ny;
+            if (kCpu) {
+                nx = (ar * dzx - ai * dzy) + (br * dcx - bi * dcy);
+                ny = (ar * dzy + ai * dzx) + (br * dcy + bi * dcx);
+            } else {
+                nx = fma(ar, dzx, fma(-ai, dzy, fma(br, dcx, -bi * dcy)));
+                ny = fma(ar, dzy, fma(ai, dzx, fma(br, dcy, bi * dcx)));
+            }
+            dzx = nx;
+            dzy = ny;
+            if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) return done(glitch_sample(k), k);
+            m += 1 << best;
+            k += 1 << best;
+            ++leaps;
+            skipped += 1 << best;
+            continue;
+        }
+        if (ft == 0) {
+            double nx, ny;
+            if (kCpu) {
+                nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
+                ny = 2.0 * ((rx + dzx) * dzy + ry * dzx) + dcy;
+            } else {
+                nx = fma(2.0 * rx + dzx, dzx, fma(-(2.0 * ry + dzy), dzy, dcx));
+                ny = fma(2.0, fma(rx + dzx, dzy, ry * dzx), dcy);
+            }
+            dzx = nx;
+            dzy = ny;
+        } else if (ft == 1) {
+            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
+            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+            const double ddx = (rx + dzx) * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+            const double ddy = (ry + dzy) * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcy;
+            dzx = nx;
+        } else {
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p.gen_n - 1; ++t) {
+                const cplx t1 = cmul(pr, pi, rx, ry);
+                const cplx t2 = cmul(pr + qr, pi + qi, dzx, dzy);
+                pr = t1.r + t2.r;
+                pi = t1.i + t2.i;
+                const cplx q = cmul(qr, qi, rx, ry);
+                qr = q.r;
+                qi = q.i;
+            }
+            const cplx kz = cmul(p.gen_kr, p.gen_ki, dzx, dzy);
+            dzx = pr + kz.r + dcx;
+            dzy = pi + kz.i + dcy;
+        }
+        ++m;
+        ++k;
+    }
+    return done(interior_sample(), max_iter);
+}
+
 template <int ARITH>
 __device__ __forceinline__ SampleOut perturb_sample_at(const ApFrameParams& p,
                                                        const ApFrameBuffers& b, double sub_i,
                                                        double sub_j) {
+    if (p.flags & AP_FLAG_REBASE) return rebase_sample_at<ARITH>(p, b, sub_i, sub_j);
     constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
     const int ft = p.fractal_type;
     const bool julia = (ft == 2 || ft == 3);

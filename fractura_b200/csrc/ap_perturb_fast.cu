@@ -6,7 +6,7 @@
 
 namespace ap {
 
-template <int ARITH, int FT, bool BLA>
+template <int ARITH, int FT, bool BLA, bool REBASE>
 __global__ void __launch_bounds__(256, 4) perturb_coarse_kernel(const ApFrameParams p,
                                                                 const ApFrameBuffers b) {
     // each warp takes an 8 x 4 patch of its block's 16 x 16 pixels: neighbours
@@ -15,16 +15,20 @@ __global__ void __launch_bounds__(256, 4) perturb_coarse_kernel(const ApFramePar
     const int i = blockIdx.x * 16 + (w & 1) * 8 + (l & 7);
     const int j = blockIdx.y * 16 + (w >> 1) * 4 + (l >> 3);
     if (i >= p.width || j >= p.height) return;
-    coarse_pixel<ARITH, FT, BLA>(p, b, i, j);
+    coarse_pixel<ARITH, FT, BLA, REBASE>(p, b, i, j);
 }
 
 template <int ARITH, int FT>
 static void launch_ft(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
     dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
-    if (p.bla_levels > 1)
-        perturb_coarse_kernel<ARITH, FT, true><<<grid, 256, 0, st>>>(p, b);
-    else
-        perturb_coarse_kernel<ARITH, FT, false><<<grid, 256, 0, st>>>(p, b);
+    const bool rebase = (p.flags & AP_FLAG_REBASE) != 0;
+    if (p.bla_levels > 1) {
+        if (rebase) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b);
+        else perturb_coarse_kernel<ARITH, FT, true, false><<<grid, 256, 0, st>>>(p, b);
+    } else {
+        if (rebase) perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b);
+        else perturb_coarse_kernel<ARITH, FT, false, false><<<grid, 256, 0, st>>>(p, b);
+    }
 }
 
 template <int ARITH>

@@ -190,6 +190,20 @@ int validate_frame(const ApFrameParams* p, const ApFrameBuffers* b, int hist_res
         set_error("glitch_in is required on rebase passes");
         return AP_E_INVALID;
     }
+    if (p->flags & AP_FLAG_REBASE) {
+        if (p->tier != AP_TIER_PERTURB) {
+            set_error("AP_FLAG_REBASE serves the FP64-delta tier (AP_TIER_PERTURB)");
+            return AP_E_UNSUPPORTED;
+        }
+        if (p->fractal_type == 2 || p->fractal_type == 3) {
+            set_error("AP_FLAG_REBASE serves orbits that start at 0 (fractal_type 0, 1, 4)");
+            return AP_E_UNSUPPORTED;
+        }
+        if (p->ref_len < 1 || p->rebase_pass != 0) {
+            set_error("AP_FLAG_REBASE needs ref_len >= 1 and rebase_pass 0");
+            return AP_E_INVALID;
+        }
+    }
     if (p->tier >= AP_TIER_PERTURB) {
         if (!b->ref_re || !b->ref_im || p->ref_len < 0) {
             set_error("perturbation tiers need the reference orbit");

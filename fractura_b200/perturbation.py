@@ -21,6 +21,10 @@ from . import high_precision as hp
 
 BLA_LEVELS = 16
 MAX_REBASE_PASSES = 4
+# glitch_mode of the one-pass rebasing form (AP_FLAG_REBASE): every pixel restarts its
+# delta from the orbit's start when |z| < |dz| or the reference ends, in the same pass.
+# The reference has no such mode; its modes re-render glitched pixels around new references.
+ONE_PASS_REBASING = "One-Pass Rebasing"
 
 # Host<->device traffic of the last perturbation frame (bytes), for benchmarking.
 LAST_FRAME_STATS = {"h2d_bytes": 0, "d2h_bytes": 0, "rebase_passes": 0, "strict_pixels": 0, "strict_tier": 0}
@@ -346,8 +350,13 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
             fe32 = (float(plot_width_dec * (Decimal(2) ** fe_e) / Decimal(max(1, W - 1))) / float(factor),
                     float(plot_height_dec * (Decimal(2) ** fe_e) / Decimal(max(1, H - 1))) / float(factor),
                     int(fe_e))
-    strict = 1 if ("Auto Rebasing" in glitch_mode or "Strict" in glitch_mode
-                   or "Pauldelbrot" in glitch_mode) else 0
+    one_pass = ONE_PASS_REBASING in glitch_mode
+    if one_pass and (tier != abi.AP_TIER_PERTURB or fractal_type in (2, 3) or fp32_deltas):
+        raise NotImplementedError(
+            f"{ONE_PASS_REBASING!r} serves FP64-delta frames (widths 1e-300 .. 1e-12) of "
+            "Mandelbrot, Burning Ship and Multibrot")
+    strict = 0 if one_pass else (1 if ("Auto Rebasing" in glitch_mode or "Strict" in glitch_mode
+                                       or "Pauldelbrot" in glitch_mode) else 0)
     LAST_FRAME_STATS.update(h2d_bytes=0, d2h_bytes=0, rebase_passes=0, strict_pixels=0, strict_tier=0)
 
     bcx, bcy, bu, bv, re, im, ref_len = hp.find_optimal_reference_orbit(
@@ -389,6 +398,9 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     # BLA variant (NaN guard), their histogram resolve passes the plain one (escape glitch).
     unified_flags = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_NAN_GUARD
     resolve_flags = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_ESCAPE_GLITCH
+    if one_pass:
+        unified_flags |= abi.AP_FLAG_REBASE
+        resolve_flags |= abi.AP_FLAG_REBASE
     _lib.device_op(fr.glitch_in.zero_)
     orbit = (d_re, d_im)
     cdf = None

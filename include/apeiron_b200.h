@@ -26,7 +26,7 @@ extern "C" {
 #define AP_API
 #endif
 
-#define AP_ABI_VERSION 5
+#define AP_ABI_VERSION 6
 
 /* Return codes. */
 #define AP_OK 0
@@ -58,6 +58,14 @@ extern "C" {
 #define AP_FLAG_ITER_LAST_SUB 8u   /* supersample passes write the last sub-sample to the iter map */
 #define AP_FLAG_MAP_FUSED 16u      /* pixel -> c mapping as fma(i, dx, x_min) */
 #define AP_FLAG_HIST_COLOUR 32u    /* colour through the CDF table (scheme 11 resolve passes) */
+/* One-pass rebasing (AP_TIER_PERTURB, fractal types 0, 1, 4; no counterpart in the
+ * reference, which rebases by whole re-render passes, math_core/engine.py:1890-2113).
+ * Each pixel keeps its own iteration count n and a reference index m.  When
+ * |Z_m + dz| < |dz| (the delta has outgrown the value it perturbs) or the reference
+ * ends (m == ref_len), the delta restarts from the orbit's start: dz <- Z_m + dz,
+ * m <- 0 (Zhuoran, fractalforums.org 2021).  No pixel is flagged glitched (only a
+ * NaN/Inf delta is), there is no direct-iteration stage, and rebase_pass must be 0. */
+#define AP_FLAG_REBASE 64u
 
 typedef struct ApFrameParams {
     int32_t width, height;     /* output pixels */
@@ -110,7 +118,8 @@ typedef struct ApFrameBuffers {
     int32_t* counters;         /* optional [H, W, 4]: work done for the pixel by this pass, summed
                                   over its sub-samples: [0] iterations stepped one at a time
                                   (direct tiers; perturbation stage 1), [1] BLA leaps taken,
-                                  [2] perturbation stage-2 (direct) steps, [3] zero.  16-byte aligned;
+                                  [2] perturbation stage-2 (direct) steps, [3] rebases
+                                  (AP_FLAG_REBASE coarse passes on packed inputs; otherwise zero).  16-byte aligned;
                                   written only for pixels the pass evaluates. */
     const double* orbit_packed; /* optional [ref_len + 1, 4] from ap_pack_orbit */
     const double* bla_packed;   /* optional, from ap_pack_bla (needs orbit_packed) */
@@ -170,9 +179,9 @@ AP_API int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height
 
 /* Reference orbit in the layout the perturbation kernels read: per step the
  * 32-byte record (Z_re, Z_im, safe radius^2, level-0 BLA radius^2).  While the
- * rounded |dz|^2 is below the safe radius^2 neither the escape test nor the glitch
+ * rounded |dz|^2 is below the safe radius^2 neither the escape test, the glitch
  * test (|Z + dz|^2 < 1e-6 |Z|^2 where |Z|^2 > 1e-8, math_core/cpu_kernels.py:428-431)
- * can fire at that step.  The level-0 radius is written by ap_pack_bla; this call
+ * nor the rebase test of AP_FLAG_REBASE (|Z + dz| < |dz|) can fire at that step.  The level-0 radius is written by ap_pack_bla; this call
  * leaves it 0 (no leap).  out: [ref_len + 1, 4] float64. */
 AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref_len, double* out,
                          void* stream);

@@ -633,8 +633,12 @@ static Sample glitch_at(int k) {
     return o;
 }
 
+static Sample rebase_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
+                               double sub_j);
+
 static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
                              double sub_j) {
+    if (p->flags & AP_FLAG_REBASE) return rebase_sample_at(p, b, sub_i, sub_j);
     const int ft = p->fractal_type, cpu = p->arith == AP_ARITH_REF_CPU;
     const int julia = (ft == 2 || ft == 3);
     const int ref_len = p->ref_len, max_iter = p->max_iter;
@@ -778,6 +782,131 @@ static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, do
     Sample o = interior();
     o.glitch = glitch;
     return o;
+}
+
+/* ------------------------------------------------------------------------- */
+/* One-pass rebasing (AP_FLAG_REBASE).  The reference has no such sample: it   */
+/* rebases by re-rendering glitched pixels around new references              */
+/* (engine.py:1890-2113).  This restates the engine's extension, Zhuoran's    */
+/* rebasing (fractalforums.org 2021), in the operation order of the FP64-delta */
+/* sample above; its values are pinned by the 700-bit ground truth            */
+/* (tests/golden/truth_cfg3.npz) rather than by reference output.             */
+/*   k counts the pixel's iterations, m indexes the reference (Z_0 = 0).      */
+/*   Each step: z = Z_m + dz; escape when |z|^2 > 65536 (NaN: glitch);        */
+/*   when |z|^2 < |dz|^2, or m == ref_len > 0: dz <- z, m <- 0;               */
+/*   else the largest BLA level with m + 2^d < ref_len, k + 2^d <= max_iter   */
+/*   and |dz|^2 < r_d^2 (levels 0..8 only for an underflowed |dz|^2);         */
+/*   else one perturbation step.  Interior after max_iter.                    */
+/* ------------------------------------------------------------------------- */
+static int floor_log2(int v) {
+    int r = 0;
+    while (v > 1) {
+        v >>= 1;
+        r++;
+    }
+    return r;
+}
+
+static Sample rebase_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
+                               double sub_j) {
+    const int ft = p->fractal_type, cpu = p->arith == AP_ARITH_REF_CPU;
+    const int ref_len = p->ref_len, max_iter = p->max_iter;
+    const double* re = b->ref_re;
+    const double* im = b->ref_im;
+    const double dcy = (p->ref_py - sub_j) * p->dy_hi;
+    const double dcx = (sub_i - p->ref_px) * p->dx_hi;
+    double dzx = 0.0, dzy = 0.0;
+    int k = 0;
+    if (p->bbsa_skip > 0 && (ft == 0 || ft == 4) &&
+        (dcx * p->bbsa_inv_r) * (dcx * p->bbsa_inv_r) + (dcy * p->bbsa_inv_r) * (dcy * p->bbsa_inv_r) <= 1.0) {
+        eval_bbsa(p->bbsa, dcx * p->bbsa_inv_r, dcy * p->bbsa_inv_r, &dzx, &dzy);
+        k = p->bbsa_skip;
+    }
+    int m = k;
+    const int levels = p->bla_levels;
+    const int has_bla = levels > 1 && b->bla != NULL && (ft == 0 || ft == 4);
+    const double inv_ln = inv_ln_for(ft, p->gen_n);
+    const size_t L = (size_t)ref_len;
+    while (k < max_iter) {
+        const double rx = re[m], ry = im[m];
+        const double zx = rx + dzx, zy = ry + dzy;
+        const double mag2 = zx * zx + zy * zy;
+        if (!(mag2 <= BAILOUT)) {
+            if (isnan(mag2)) return glitch_at(k);
+            return escaped(k, mag2, inv_ln);
+        }
+        const double dz_mag2 = dzx * dzx + dzy * dzy;
+        if (mag2 < dz_mag2 || (m == ref_len && m > 0)) {
+            dzx = zx;
+            dzy = zy;
+            m = 0;
+            continue;
+        }
+        if (has_bla && m < ref_len - 1 && dz_mag2 < b->bla[(size_t)m * 5 + 4]) {
+            int best = 0, max_d = levels - 1;
+            if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) max_d = max_d > 8 ? 8 : max_d;
+            const int cap = floor_log2(max_iter - k);
+            if (max_d > cap) max_d = cap;
+            for (int d = max_d; d > 0; d--) {
+                if (m + (1 << d) < ref_len && dz_mag2 < b->bla[((size_t)d * L + m) * 5 + 4]) {
+                    best = d;
+                    break;
+                }
+            }
+            const double* e = b->bla + ((size_t)best * L + m) * 5;
+            const double ar = e[0], ai = e[1], br = e[2], bi = e[3];
+            double nx, ny;
+            if (cpu) {
+                nx = (ar * dzx - ai * dzy) + (br * dcx - bi * dcy);
+                ny = (ar * dzy + ai * dzx) + (br * dcy + bi * dcx);
+            } else {
+                nx = fma(ar, dzx, fma(-ai, dzy, fma(br, dcx, -bi * dcy)));
+                ny = fma(ar, dzy, fma(ai, dzx, fma(br, dcy, bi * dcx)));
+            }
+            dzx = nx;
+            dzy = ny;
+            if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) return glitch_at(k);
+            m += 1 << best;
+            k += 1 << best;
+            continue;
+        }
+        if (ft == 0) {
+            double nx, ny;
+            if (cpu) {
+                nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
+                ny = 2.0 * ((rx + dzx) * dzy + ry * dzx) + dcy;
+            } else {
+                nx = fma(2.0 * rx + dzx, dzx, fma(-(2.0 * ry + dzy), dzy, dcx));
+                ny = fma(2.0, fma(rx + dzx, dzy, ry * dzx), dcy);
+            }
+            dzx = nx;
+            dzy = ny;
+        } else if (ft == 1) {
+            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
+            const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
+            const double ddx = (rx + dzx) * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+            const double ddy = (ry + dzy) * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcy;
+            dzx = nx;
+        } else {
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p->gen_n - 1; t++) {
+                double t1r, t1i, t2r, t2i;
+                c_mul(pr, pi, rx, ry, &t1r, &t1i);
+                c_mul(pr + qr, pi + qi, dzx, dzy, &t2r, &t2i);
+                pr = t1r + t2r;
+                pi = t1i + t2i;
+                c_mul(qr, qi, rx, ry, &qr, &qi);
+            }
+            double kr, ki;
+            c_mul(p->gen_kr, p->gen_ki, dzx, dzy, &kr, &ki);
+            dzx = pr + kr + dcx;
+            dzy = pi + ki + dcy;
+        }
+        m++;
+        k++;
+    }
+    return interior();
 }
 
 /* ------------------------------------------------------------------------- */
@@ -1430,6 +1559,35 @@ static void grid_row(void* vctx, int j) {
         if (c->s64) c->s64[idx] = o.s64;
         if (c->kmap) c->kmap[idx] = o.k;
     }
+}
+
+/* Samples of any tier at sub-sample coordinates (columns xs, rows ys), each mapped as the
+ * unified pass maps it (sample_at). */
+typedef struct {
+    const ApFrameParams* p;
+    const ApFrameBuffers* b;
+    const double* xs;
+    const double* ys;
+    int W;
+    double* s64;
+    int32_t* kmap;
+} SampleGridCtx;
+
+static void sample_grid_row(void* vctx, int j) {
+    const SampleGridCtx* c = (const SampleGridCtx*)vctx;
+    for (int i = 0; i < c->W; i++) {
+        Sample o = sample_at(c->p, c->b, c->xs[i], c->ys[j]);
+        size_t idx = (size_t)j * c->W + i;
+        c->s64[idx] = o.s64;
+        c->kmap[idx] = o.k;
+    }
+}
+
+APO_EXPORT int apo_sample_grid(const ApFrameParams* p, const ApFrameBuffers* b, const double* xs,
+                               const double* ys, int W, int H, double* s64, int32_t* kmap) {
+    SampleGridCtx c = {p, b, xs, ys, W, s64, kmap};
+    parallel_rows(H, sample_grid_row, &c);
+    return AP_OK;
 }
 
 APO_EXPORT int apo_fp64_grid(const ApFrameParams* p, const double* xs, const double* ys, int W, int H,

@@ -49,6 +49,8 @@ def lib():
         L.apo_fp64_grid.argtypes = [P, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                     C.c_void_p, C.c_void_p, C.c_void_p]
         L.apo_set_threads.argtypes = [C.c_int]
+        L.apo_sample_grid.argtypes = [P, B, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                      C.c_void_p]
         L.apo_pert_grid.argtypes = [P, B, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                                     C.c_void_p, C.c_void_p]
         L.apo_build_bla.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_int,
@@ -83,6 +85,20 @@ def fp64_grid(params, xs, ys):
     _check(lib().apo_fp64_grid(C.byref(params), ptr(xs), ptr(ys), W, H, ptr(s32), ptr(s64), ptr(k)),
            "fp64_grid")
     return s32, s64, k
+
+
+def sample_grid(params, xs, ys):
+    """Samples of the direct tiers (FP64, double-double) at sub-sample coordinates xs
+    (columns) x ys (rows), mapped as the unified pass maps them.  Returns (s64, k)."""
+    xs = np.ascontiguousarray(xs, np.float64)
+    ys = np.ascontiguousarray(ys, np.float64)
+    H, W = len(ys), len(xs)
+    s64 = np.empty((H, W), np.float64)
+    k = np.empty((H, W), np.int32)
+    b = abi.ApFrameBuffers()
+    _check(lib().apo_sample_grid(C.byref(params), C.byref(b), ptr(xs), ptr(ys), W, H, ptr(s64), ptr(k)),
+           "sample_grid")
+    return s64, k
 
 
 def pert_grid(params, ref_re, ref_im, bla, xs, ys, with_s64=False):

@@ -7,6 +7,7 @@ from decimal import Decimal, localcontext
 import numpy as np
 
 import oracle
+import ref_orbit
 from fractura_b200 import abi
 from fractura_b200.config import compute_floatexp_scale, decimal_context
 from fractura_b200.engine import plan_direct_view
@@ -72,7 +73,6 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
     """A perturbation-tier frame through the oracle, pass for pass as the engine issues it
     (fractura_b200.perturbation.render_perturbation_frame), including the rebase loop.
     ``bla_eps`` selects the dc-aware BLA table (the engine's bla_form="accurate")."""
-    from fractura_b200 import high_precision as hp
     from fractura_b200.config import compute_required_prec_bits
     from fractura_b200.perturbation import RebaseState, max_delta_c, select_rebase_pixel
     W, H, f, mi = m["W"], m["H"], m["factor"], m["max_iter"]
@@ -88,10 +88,10 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
         two_e = Decimal(2) ** e_scale
         dx_f = float(pw * two_e / Decimal(max(1, W - 1)))
         dy_f = float(ph * two_e / Decimal(max(1, H - 1)))
-    hp.clear_reference_orbit_cache()
-    bcx, bcy, bu, bv, re, im, rl = hp.find_optimal_reference_orbit(
-        cxd, cyd, pw, ph, mi, W, H, fractal_type=ft, julia_cx=m["julia_cx"], julia_cy=m["julia_cy"],
-        gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"], is_floatexp=floatexp)
+    # the oracle's own Decimal restatement of the reference's orbit search (oracle/ref_orbit.py)
+    bcx, bcy, bu, bv, re, im, rl = ref_orbit.find_reference(
+        cxd, cyd, pw, ph, mi, ft=ft, julia_cx=m["julia_cx"], julia_cy=m["julia_cy"],
+        n=m["gen_n"], kr=m["gen_kr"], ki=m["gen_ki"])
     order = m["bbsa_order"]
     if floatexp and order in (4, 8):
         order = 32  # the reference maps series starts to chained BLA on this tier
@@ -125,7 +125,8 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
     fr.ref_re, fr.ref_im = np.ascontiguousarray(re[:rl + 1]), np.ascontiguousarray(im[:rl + 1])
     fr.bla = table(re, im, rl, float(W - 1) * float(bu) * float(f),
                    float(H - 1) * float(bv) * float(f)) if use_bla else None
-    strict = 1 if "Pauldelbrot" in m["glitch_mode"] or "Strict" in m["glitch_mode"] else 0
+    one_pass = "One-Pass Rebasing" in m["glitch_mode"]
+    strict = 0 if one_pass else (1 if "Pauldelbrot" in m["glitch_mode"] or "Strict" in m["glitch_mode"] else 0)
     p = abi.new_params(width=W, height=H, factor=f, max_iter=mi, fractal_type=ft,
                        tier=abi.AP_TIER_FLOATEXP if floatexp else abi.AP_TIER_PERTURB, arith=arith,
                        e_scale=e_scale, gen_n=m["gen_n"], gen_kr=m["gen_kr"],
@@ -139,6 +140,9 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
     set_series(p, series(re, im, rl))
     uf = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_NAN_GUARD
     rf = (abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem else abi.AP_FLAG_ESCAPE_GLITCH
+    if one_pass:
+        uf |= abi.AP_FLAG_REBASE
+        rf |= abi.AP_FLAG_REBASE
 
     def resolve(q):
         bla_keep = fr.bla
@@ -181,12 +185,9 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
             break
         state.visited.add(chosen)
         gr, gc = chosen
-        with localcontext(ctx):
-            r_cx = (cxd - pw / Decimal(2)) + (Decimal(gc) / Decimal(max(1, W - 1))) * pw
-            r_cy = (cyd + ph / Decimal(2)) - (Decimal(gr) / Decimal(max(1, H - 1))) * ph
-        r_re, r_im, r_len = hp.compute_single_highprec_orbit(
-            r_cx, r_cy, mi, ft, m["julia_cx"], m["julia_cy"], bits,
-            gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"])
+        r_cx, r_cy = ref_orbit.pixel_c(cxd, cyd, pw, ph, W, H, gc, gr)
+        r_re, r_im, r_len = ref_orbit.orbit(r_cx, r_cy, mi, ft, m["julia_cx"], m["julia_cy"], bits,
+                                            n=m["gen_n"], kr=m["gen_kr"], ki=m["gen_ki"])
         fr.ref_re, fr.ref_im = np.ascontiguousarray(r_re[:r_len + 1]), np.ascontiguousarray(r_im[:r_len + 1])
         fr.bla = table(r_re, r_im, r_len, float(gc) * f, float(gr) * f) if use_bla else None
         fr.glitch_in[...] = g
@@ -219,7 +220,7 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
         tier = None if cpu_sem else strict_device_tier(pw, ft)
         if len(coords) and tier is None:
             vals = strict_values(coords, W, H, mi, cxd, cyd, pw, ph, ft, m["julia_cx"], m["julia_cy"],
-                                 m["gen_n"], m["gen_kr"], m["gen_ki"], scalar=hp.decimal_escape_scalar)
+                                 m["gen_n"], m["gen_kr"], m["gen_ki"], scalar=_oracle_escape)
             q = abi.ApFrameParams.from_buffer_copy(p)
             q.arith = abi.AP_ARITH_REF_CPU
             oracle.set_pixels(q, fr, coords, vals)
@@ -228,6 +229,12 @@ def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.
                                                          m["julia_cy"])
             oracle.strict_eval(q, fr, view, coords, signs, limbs)
     return fr, state.passes
+
+
+def _oracle_escape(cx, cy, max_iter, fractal_type, julia_cx, julia_cy, bits, gen_n=3, gen_kr=0.25, gen_ki=1.0):
+    """The Strict Metric's host value of one pixel through the oracle's Decimal restatement."""
+    return ref_orbit.escape(cx, cy, max_iter, fractal_type, julia_cx, julia_cy, bits, n=gen_n, kr=gen_kr,
+                            ki=gen_ki)
 
 
 def probe_search(base_iter):

@@ -97,7 +97,7 @@ def test_packed_orbit_and_bla_layouts():
     r2 = re * re + im * im
     assert np.array_equal(got[:, 0], re) and np.array_equal(got[:, 1], im)
     assert not got[:, 3].any()  # level-0 radius: filled by ap_pack_bla
-    # safe radius: inside it neither the bailout nor the Pauldelbrot threshold is reachable
+    # safe radius: inside it neither the bailout nor the Pauldelbrot threshold is reachable,
     safe2 = got[:, 2]
     s = np.sqrt(safe2)
     rz = np.sqrt(r2)
@@ -107,6 +107,8 @@ def test_packed_orbit_and_bla_layouts():
     assert np.all(safe2[rz >= 256.0] == 0.0)
     glitchable = inside & (r2 > 1e-8)
     assert np.all((rz[glitchable] - s[glitchable]) ** 2 > 1e-6 * r2[glitchable])
+    # ... nor the one-pass rebase test |Z + dz| < |dz|: |Z| - s > s
+    assert np.all(rz[inside] - s[inside] > s[inside])
     assert np.count_nonzero(safe2) > 0.9 * len(safe2)
     T = oracle.build_bla(re, im, rl, 0, 1e-6, 16, 3, 0.25, 1.0)
     d_T = torch.from_numpy(T).cuda()
