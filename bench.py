@@ -66,6 +66,12 @@ FLOPS_DD_SHIP = 124.0
 # FloatExp perturbation step (FP64 mantissa): the FP64-delta step (25) plus the
 # exponent-scaled Z terms and the renormalisation test (10)                          -> 35
 FLOPS_STEP1_FEXP = 35.0
+# One-pass rebasing (AP_FLAG_REBASE), per step: z = Z + dz (2), |dz|^2 (3, the safe,
+# leap and rebase tests), |z|^2 (3, escape and rebase tests), dz' = (2Z + dz) dz + dc (13)
+#                                                                                    -> 21
+# per leap: z (2), |z|^2 (3), |dz|^2 (3), A dz + B dc (14)                           -> 22
+FLOPS_STEP_REBASE = 21.0
+FLOPS_LEAP_REBASE = 22.0
 
 
 # --------------------------------------------------------------- workloads
@@ -76,12 +82,13 @@ def _centres():
 
 def workload_cfg3():
     cx, cy = _centres()["config3_centre"]
-    return dict(name="mandelbrot_perturb_bla_pauldelbrot_1920x1080_w1e-160", W=1920, H=1080,
+    return dict(name="mandelbrot_perturb_bla_rebase_1920x1080_w1e-160", W=1920, H=1080,
                 max_iter=200000, cx=cx, cy=cy, width="1e-160", scheme=0, factor=1, fractal_type=0,
                 precision_mode="1e-300 (Perturbation)", bbsa_order=32, bbsa_tol=1e-6,
-                glitch_mode="Pauldelbrot", arith="ref_cpu", dtype="f64", bla_form="accurate",
-                form="FP64 deltas, dc-aware chained BLA (eps 1e-14), Pauldelbrot with up to 4 "
-                     "rebase passes")
+                glitch_mode="One-Pass Rebasing", arith="ref_cpu", dtype="f64", bla_form="accurate",
+                form="FP64 deltas, dc-aware chained BLA (eps 1e-14), one-pass rebasing "
+                     "(every pixel restarts its delta when |z| < |dz| or the reference ends; "
+                     "no re-render pass)")
 
 
 def workload_cfg1():
@@ -497,6 +504,8 @@ def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla, direct_flop
                 p = args[0]._obj
                 if p.tier in (abi.AP_TIER_FP64, abi.AP_TIER_DD):
                     total += direct_flops * float(c[0])
+                elif p.flags & abi.AP_FLAG_REBASE:
+                    total += FLOPS_STEP_REBASE * float(c[0]) + FLOPS_LEAP_REBASE * float(c[1])
                 elif p.tier == abi.AP_TIER_FLOATEXP:
                     total += (f1 - 25.0 + FLOPS_STEP1_FEXP) * float(c[0]) + FLOPS_LEAP * float(c[1]) + \
                         FLOPS_STEP2 * float(c[2])
@@ -754,7 +763,9 @@ def our_arm(args, wl, rank, world, local_rank):
     if perturb:
         n_cmp = max(3, args.steps // 10)
         plain = record_form(torch, _lib, engine, wl, stream,
-                            Form("plain", dict(bbsa_order=0), "plain FP64 deltas, no BLA, same glitch handling"),
+                            Form("plain", dict(bbsa_order=0, glitch_mode="Pauldelbrot"),
+                                 "plain FP64 deltas, no BLA, Pauldelbrot with up to 4 rebase passes "
+                                 "(the reference's form)"),
                             kmap, s64)
         p_ms, _ = timed_replay(torch, _lib, plain.ops, stream, n_cmp, flush)
         plain_sum = summarise_form(plain, p_ms, wl=wl)
@@ -766,10 +777,15 @@ def our_arm(args, wl, rank, world, local_rank):
                  "plain FP64 deltas, one reference, no rebasing"),
             Form("chosen_single_reference", dict(chosen.over, **single),
                  chosen.desc + ", one reference, no rebasing"),
-            Form("reference_bla", dict(bla_form="reference"),
-                 "FP64 deltas with the reference's BLA table (tol 1e-6), same glitch handling"),
-            Form("fp32_floatexp", dict(chosen.over, delta_form="fp32"),
-                 "FP32 mantissa + int exponent deltas, accurate BLA, same glitch handling"),
+            Form("plain_one_pass", dict(bbsa_order=0), "plain FP64 deltas, no BLA, one-pass rebasing"),
+            Form("chosen_pauldelbrot", dict(chosen.over, glitch_mode="Pauldelbrot"),
+                 "FP64 deltas, dc-aware chained BLA, Pauldelbrot with up to 4 rebase passes"),
+            Form("reference_bla", dict(bla_form="reference", glitch_mode="Pauldelbrot"),
+                 "FP64 deltas with the reference's BLA table (tol 1e-6), Pauldelbrot with up to 4 "
+                 "rebase passes"),
+            Form("fp32_floatexp", dict(chosen.over, delta_form="fp32", glitch_mode="Pauldelbrot"),
+                 "FP32 mantissa + int exponent deltas, accurate BLA, Pauldelbrot with up to 4 rebase "
+                 "passes"),
         ]
         for f in extra:
             record_form(torch, _lib, engine, wl, stream, f, kmap, s64)
