@@ -51,7 +51,8 @@ __global__ void __launch_bounds__(256) histogram_kernel(const float* __restrict_
 
 // One block of 1024 threads: inclusive prefix sum of the histogram in exact
 // integer arithmetic, then cdf[b] = float32(prefix[b] / total) as the
-// float64 scan of math_core/cuda_kernels.py:1929-1996 produces it.
+// float64 scan of math_core/cuda_kernels.py:1929-1996 produces it.  Serves bin
+// counts above kChunkMaxBins (cdf_chunk_kernel below serves the rest).
 constexpr int kScanThreads = 1024;
 
 __global__ void __launch_bounds__(kScanThreads) cdf_kernel(const int* __restrict__ hist,
@@ -90,6 +91,91 @@ __global__ void __launch_bounds__(kScanThreads) cdf_kernel(const int* __restrict
         run += hist[q];
         cdf[q] = total > 0.0 ? (float)((double)run / total)
                              : (float)((double)q / (double)(num_bins - 1));
+    }
+}
+
+// Chunked form for up to kChunkMaxBins bins (the reference's 65536): block b scans bins
+// [4096 b, 4096 (b + 1)).  Every block first reads all counts, coalesced, for the sum of
+// the bins before its chunk and the total (256 KiB from L2 at 65536 bins), so no block
+// waits on another; then each thread takes 16 consecutive bins, the thread sums are
+// scanned across the block, and each bin gets cdf = float32(float64(prefix) / total) with
+// the same exact integer prefix and division as cdf_kernel.
+constexpr int kChunkBins = 4096;
+constexpr int kChunkThreads = 256;
+constexpr int kChunkPerThread = kChunkBins / kChunkThreads;  // 16
+constexpr int kChunkMaxBins = 65536;
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(kChunkThreads) cdf_chunk_kernel(const int* __restrict__ hist,
+                                                                  int num_bins, float* __restrict__ cdf) {
+    __shared__ long long red_before[kChunkThreads / 32], red_total[kChunkThreads / 32];
+    __shared__ long long scan_s[kChunkThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int start = blockIdx.x * kChunkBins;
+    long long before = 0, total = 0;
+    if ((num_bins & 3) == 0 && (reinterpret_cast<uintptr_t>(hist) & 15u) == 0) {
+        const int4* h4 = reinterpret_cast<const int4*>(hist);
+        const int n4 = num_bins >> 2, s4 = start >> 2;
+#pragma unroll 4
+        for (int q = t; q < n4; q += kChunkThreads) {
+            const int4 v = __ldg(h4 + q);
+            const long long s = (long long)v.x + v.y + v.z + v.w;
+            total += s;
+            if (q < s4) before += s;
+        }
+    } else {
+#pragma unroll 4
+        for (int q = t; q < num_bins; q += kChunkThreads) {
+            const long long v = __ldg(hist + q);
+            total += v;
+            if (q < start) before += v;
+        }
+    }
+    before = warp_sum_ll(before);
+    total = warp_sum_ll(total);
+    if (lane == 0) {
+        red_before[warp] = before;
+        red_total[warp] = total;
+    }
+    __syncthreads();
+    before = total = 0;
+#pragma unroll
+    for (int w = 0; w < kChunkThreads / 32; ++w) {
+        before += red_before[w];
+        total += red_total[w];
+    }
+    // this thread's 16 bins and their sum
+    const int b0 = start + t * kChunkPerThread;
+    long long c[kChunkPerThread];
+    long long mine = 0;
+#pragma unroll
+    for (int q = 0; q < kChunkPerThread; ++q) {
+        c[q] = (b0 + q < num_bins) ? (long long)__ldg(hist + b0 + q) : 0LL;
+        mine += c[q];
+    }
+    // exclusive scan of the thread sums across the block
+    long long v = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) scan_s[warp] = v;
+    __syncthreads();
+    long long run = before + (v - mine);
+    for (int w = 0; w < warp; ++w) run += scan_s[w];
+    const double tot = (double)total;
+#pragma unroll
+    for (int q = 0; q < kChunkPerThread; ++q) {
+        const int b = b0 + q;
+        if (b >= num_bins) break;
+        run += c[q];
+        cdf[b] = tot > 0.0 ? (float)((double)run / tot) : (float)((double)b / (double)(num_bins - 1));
     }
 }
 
@@ -188,6 +274,11 @@ extern "C" int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t he
     ap::histogram_kernel<<<blocks, 256, 0, st>>>(iter_map, n, inv_max, num_bins, hist);
     int rc = ap::check_launch("histogram_kernel");
     if (rc != AP_OK) return rc;
+    if (num_bins <= ap::kChunkMaxBins) {
+        const int blocks = (num_bins + ap::kChunkBins - 1) / ap::kChunkBins;
+        ap::cdf_chunk_kernel<<<blocks, ap::kChunkThreads, 0, st>>>(hist, num_bins, cdf);
+        return ap::check_launch("cdf_chunk_kernel");
+    }
     ap::cdf_kernel<<<1, ap::kScanThreads, 0, st>>>(hist, num_bins, cdf);
     return ap::check_launch("cdf_kernel");
 }
