@@ -113,10 +113,10 @@ def workload_cfg3():
     return dict(name="mandelbrot_perturb_1920x1080_w1e-160_maxiter200000", W=1920, H=1080,
                 max_iter=200000, cx=cx, cy=cy, width="1e-160", scheme=0, factor=1, fractal_type=0,
                 precision_mode="1e-300 (Perturbation)", bbsa_order=32, bbsa_tol=1e-6,
-                glitch_mode="One-Pass Rebasing", arith="ref_cpu", dtype="f64", bla_form="accurate",
+                glitch_mode="One-Pass Rebasing", arith="fast", dtype="f64", bla_form="accurate",
                 form="FP64 deltas, dc-aware chained BLA (eps 1e-14), one-pass rebasing "
                      "(every pixel restarts its delta when |z| < |dz| or the reference ends; "
-                     "no re-render pass)",
+                     "no re-render pass), fused-multiply-add step (arith 'fast')",
                 ref_form="FP64 deltas, the reference's chained BLA (tol 1e-6), Pauldelbrot with up to "
                          "4 rebase passes")
 
@@ -141,7 +141,7 @@ def workload_cfg2():
 def workload_cfg3b():
     wl = workload_cfg3()
     wl.update(name="mandelbrot_floatexp_1920x1080_w1e-1000_maxiter200000", width="1e-1000",
-              glitch_mode="Pauldelbrot",
+              glitch_mode="Pauldelbrot", arith="ref_cuda",
               form="FloatExp deltas (FP64 mantissa, int exponent), dc-aware chained BLA (eps 1e-14), "
                    "Pauldelbrot with up to 4 rebase passes")
     return wl
@@ -684,30 +684,33 @@ def frame_arm(args, wl, rank, world, local_rank, steps, headline):
     if perturb and wl["width"] == "1e-160" and headline:
         n_cmp = max(3, steps // 10)
         plain = record_form(torch, _lib, engine, wl, stream,
-                            Form("plain", dict(bbsa_order=0, glitch_mode="Pauldelbrot", bla_form=None),
+                            Form("plain", dict(bbsa_order=0, glitch_mode="Pauldelbrot", bla_form=None,
+                                               arith="ref_cuda"),
                                  "plain FP64 deltas, no BLA, Pauldelbrot with up to 4 rebase passes "
-                                 "(the reference's form)"),
+                                 "(the reference's CUDA form)"),
                             kmap, s64)
         p_ms, _ = timed_replay(torch, _lib, plain.ops, stream, n_cmp, flush)
         plain_sum = summarise_form(plain, p_ms, wl=wl)
         chosen_sum = summarise_form(chosen, step_ms, plain=plain, wl=wl)
         forms = {}
         single = dict(glitch_mode="Off (Single-Ref)")
+        cuda = dict(arith="ref_cuda")
         extra = [
-            Form("chosen_ref_cuda", dict(arith="ref_cuda"),
-                 chosen.desc + "; CUDA-source arithmetic profile (explicit fused multiply-adds)"),
-            Form("plain_single_reference", dict(bbsa_order=0, bla_form=None, **single),
+            Form("chosen_ref_cuda", dict(cuda), "the chosen form in the CUDA-source arithmetic profile"),
+            Form("chosen_ref_cpu", dict(arith="ref_cpu"), "the chosen form in the CPU-kernel arithmetic "
+                                                          "profile (no fused multiply-adds)"),
+            Form("plain_single_reference", dict(bbsa_order=0, bla_form=None, **single, **cuda),
                  "plain FP64 deltas, one reference, no rebasing"),
-            Form("chosen_single_reference", dict(single),
+            Form("chosen_single_reference", dict(single, **cuda),
                  "FP64 deltas, dc-aware chained BLA, one reference, no rebasing"),
             Form("plain_one_pass", dict(bbsa_order=0, bla_form=None),
                  "plain FP64 deltas, no BLA, one-pass rebasing"),
-            Form("chosen_pauldelbrot", dict(glitch_mode="Pauldelbrot"),
+            Form("chosen_pauldelbrot", dict(glitch_mode="Pauldelbrot", **cuda),
                  "FP64 deltas, dc-aware chained BLA, Pauldelbrot with up to 4 rebase passes"),
-            Form("reference_bla", dict(bla_form="reference", glitch_mode="Pauldelbrot"),
+            Form("reference_bla", dict(bla_form="reference", glitch_mode="Pauldelbrot", **cuda),
                  "FP64 deltas with the reference's BLA table (tol 1e-6), Pauldelbrot with up to 4 "
                  "rebase passes"),
-            Form("fp32_floatexp", dict(delta_form="fp32", glitch_mode="Pauldelbrot"),
+            Form("fp32_floatexp", dict(delta_form="fp32", glitch_mode="Pauldelbrot", **cuda),
                  "FP32 mantissa + int exponent deltas, dc-aware BLA, Pauldelbrot with up to 4 rebase "
                  "passes"),
         ]

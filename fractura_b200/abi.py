@@ -20,6 +20,7 @@ AP_TIER_FLOATEXP32 = 4
 
 AP_ARITH_REF_CPU = 0
 AP_ARITH_REF_CUDA = 1
+AP_ARITH_FAST = 2
 
 AP_MODE_COARSE = 0
 AP_MODE_FULL = 1

@@ -60,7 +60,7 @@ DYNAMIC_ITER_MODES = ["Off", "On (Sqrt Scaling)", "On (Linear Scaling)", "On (Ad
 ACCURATE_BLA_EPS = 1e-14
 
 # Arithmetic profiles (see include/apeiron_b200.h): which multiply-adds are fused.
-ARITH_PROFILES = {"ref_cpu": 0, "ref_cuda": 1}
+ARITH_PROFILES = {"ref_cpu": 0, "ref_cuda": 1, "fast": 2}
 
 
 def decimal_context(plot_width_dec=None, extra_digits=150):

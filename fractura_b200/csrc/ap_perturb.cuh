@@ -50,11 +50,12 @@ __device__ __forceinline__ SampleOut glitch_sample(int k) {
 // (m == ref_len) the delta restarts from the orbit's start, dz <- z, m <- 0
 // (Zhuoran, fractalforums.org 2021).  The leap takes the largest admissible level
 // that ends before the orbit does and does not carry k past max_iter.  Same values as
-// the packed coarse kernel's rebase_advance (ap_coarse.cuh).
+// the packed coarse kernel's rebase_advance (ap_coarse.cuh), AP_ARITH_FAST included.
 template <int ARITH>
 __device__ __forceinline__ SampleOut rebase_sample_at(const ApFrameParams& p, const ApFrameBuffers& b,
                                                       double sub_i, double sub_j) {
     constexpr bool kCpu = (ARITH == AP_ARITH_REF_CPU);
+    const bool fast = !kCpu && p.arith == AP_ARITH_FAST;  // served by the CUDA-profile instance
     const int ft = p.fractal_type;
     const int ref_len = p.ref_len, max_iter = p.max_iter;
     const double* __restrict__ re = b.ref_re;
@@ -87,12 +88,12 @@ __device__ __forceinline__ SampleOut rebase_sample_at(const ApFrameParams& p, co
     while (k < max_iter) {
         const double rx = __ldg(re + m), ry = __ldg(im + m);
         const double zx = rx + dzx, zy = ry + dzy;
-        const double mag2 = zx * zx + zy * zy;
+        const double mag2 = fast ? fma(zx, zx, zy * zy) : zx * zx + zy * zy;
         if (!(mag2 <= kBailout)) {
             if (isnan(mag2)) return done(glitch_sample(k), k);
             return done(escaped_sample(k, mag2, inv_ln), k);
         }
-        const double dz_mag2 = dzx * dzx + dzy * dzy;
+        const double dz_mag2 = fast ? fma(dzx, dzx, dzy * dzy) : dzx * dzx + dzy * dzy;
         if (mag2 < dz_mag2 || (m == ref_len && m > 0)) {
             dzx = zx;
             dzy = zy;
@@ -130,7 +131,11 @@ __device__ __forceinline__ SampleOut rebase_sample_at(const ApFrameParams& p, co
         }
         if (ft == 0) {
             double nx, ny;
-            if (kCpu) {
+            if (fast) {
+                const double ax = fma(2.0, rx, dzx), ay = fma(2.0, ry, dzy);
+                nx = fma(ax, dzx, fma(-ay, dzy, dcx));
+                ny = fma(ax, dzy, fma(ay, dzx, dcy));
+            } else if (kCpu) {
                 nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
                 ny = 2.0 * ((rx + dzx) * dzy + ry * dzx) + dcy;
             } else {

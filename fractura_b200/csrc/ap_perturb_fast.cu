@@ -22,7 +22,10 @@ template <int ARITH, int FT>
 static void launch_ft(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
     dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
     const bool rebase = (p.flags & AP_FLAG_REBASE) != 0;
-    if (p.bla_levels > 1) {
+    if constexpr (ARITH == AP_ARITH_FAST) {  // validated: AP_ARITH_FAST passes are rebasing passes
+        if (p.bla_levels > 1) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b);
+        else perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b);
+    } else if (p.bla_levels > 1) {
         if (rebase) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b);
         else perturb_coarse_kernel<ARITH, FT, true, false><<<grid, 256, 0, st>>>(p, b);
     } else {
@@ -52,6 +55,7 @@ int launch_perturb_fast(const ApFrameParams& p, const ApFrameBuffers& b, cudaStr
     ApFrameParams q = p;
     if (!bla) q.bla_levels = 0;
     if (q.arith == AP_ARITH_REF_CPU) launch_arith<AP_ARITH_REF_CPU>(q, b, st);
+    else if (q.arith == AP_ARITH_FAST) launch_arith<AP_ARITH_FAST>(q, b, st);
     else launch_arith<AP_ARITH_REF_CUDA>(q, b, st);
     return check_launch("perturb_coarse_kernel");
 }

@@ -127,6 +127,7 @@ template <int TIER>
 static int launch_arith(const ApFrameParams& p, const ApFrameBuffers& b, int hist_resolve,
                         cudaStream_t st) {
     if (p.arith == AP_ARITH_REF_CPU) return launch_pass<TIER, AP_ARITH_REF_CPU>(p, b, hist_resolve, st);
+    // AP_ARITH_FAST passes are one-pass rebasing passes: rebase_sample_at reads p.arith
     return launch_pass<TIER, AP_ARITH_REF_CUDA>(p, b, hist_resolve, st);
 }
 
@@ -156,9 +157,13 @@ int validate_frame(const ApFrameParams* p, const ApFrameBuffers* b, int hist_res
         set_error("unknown tier %d", p->tier);
         return AP_E_INVALID;
     }
-    if (p->arith != AP_ARITH_REF_CPU && p->arith != AP_ARITH_REF_CUDA) {
+    if (p->arith != AP_ARITH_REF_CPU && p->arith != AP_ARITH_REF_CUDA && p->arith != AP_ARITH_FAST) {
         set_error("unknown arithmetic profile %d", p->arith);
         return AP_E_INVALID;
+    }
+    if (p->arith == AP_ARITH_FAST && !(p->flags & AP_FLAG_REBASE)) {
+        set_error("AP_ARITH_FAST serves one-pass rebasing passes (AP_FLAG_REBASE) only");
+        return AP_E_UNSUPPORTED;
     }
     if (p->mode < AP_MODE_COARSE || p->mode > AP_MODE_EDGE) {
         set_error("unknown mode %d", p->mode);

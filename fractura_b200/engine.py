@@ -332,7 +332,8 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
     """Render one frame and return its RGB image (math_core/engine.py:1339-2135).
 
     Same arguments as the reference; ``arith`` optionally selects the
-    arithmetic profile ("ref_cpu" default, or "ref_cuda"), ``delta_form``
+    arithmetic profile ("ref_cpu" default, "ref_cuda", or "fast": the engine's own
+    fused form, for glitch_mode "One-Pass Rebasing" only), ``delta_form``
     the perturbation delta arithmetic: "fp64" (default, the reference's) or
     "fp32" (FP32 mantissas with integer exponents on coarse passes of
     Mandelbrot/Julia frames), ``bla_form`` the chained-BLA table: "reference"
@@ -382,6 +383,8 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
     if not isinstance(center_y_dec, Decimal):
         center_y_dec = Decimal(str(center_y_dec))
     arith_code = _arith_code(arith if arith is not None else DEFAULT_ARITH)
+    if arith_code == abi.AP_ARITH_FAST and "One-Pass Rebasing" not in str(glitch_mode):
+        raise ValueError("arith='fast' serves glitch_mode 'One-Pass Rebasing' only")
     if delta_form not in (None, "fp64", "fp32"):
         raise ValueError(f"delta_form must be 'fp64' or 'fp32', not {delta_form!r}")
     if bla_form not in (None, "reference", "accurate"):
@@ -550,6 +553,8 @@ def plan_probe(center_x_dec, center_y_dec, plot_width_dec, search_max, target_w=
     if W < 1 or H < 1:
         raise ValueError("target_w and target_h must be positive")
     arith_code = _arith_code(arith if arith is not None else DEFAULT_ARITH)
+    if arith_code == abi.AP_ARITH_FAST and "One-Pass Rebasing" not in str(glitch_mode):
+        raise ValueError("arith='fast' serves glitch_mode 'One-Pass Rebasing' only")
     tier = select_tier(plot_width_dec, precision_mode)
     p = abi.new_params(width=W, height=H, factor=1, max_iter=int(search_max),
                        fractal_type=int(fractal_type), tier=tier, arith=arith_code,

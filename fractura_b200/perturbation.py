@@ -351,6 +351,8 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
                     float(plot_height_dec * (Decimal(2) ** fe_e) / Decimal(max(1, H - 1))) / float(factor),
                     int(fe_e))
     one_pass = ONE_PASS_REBASING in glitch_mode
+    if arith_code == abi.AP_ARITH_FAST and not one_pass:
+        raise ValueError(f"arith='fast' serves glitch_mode {ONE_PASS_REBASING!r} only")
     if one_pass and (tier != abi.AP_TIER_PERTURB or fractal_type in (2, 3) or fp32_deltas):
         raise NotImplementedError(
             f"{ONE_PASS_REBASING!r} serves FP64-delta frames (widths 1e-300 .. 1e-12) of "

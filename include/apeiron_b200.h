@@ -45,6 +45,9 @@ extern "C" {
  * multiply-adds are fused, so the engine can reproduce either reference. */
 #define AP_ARITH_REF_CPU 0   /* the reference's Numba CPU kernels as compiled (x86-64, FMA where LLVM fused) */
 #define AP_ARITH_REF_CUDA 1  /* the reference's CUDA sources: explicit cuda.fma fused, nothing else */
+#define AP_ARITH_FAST 2      /* the engine's own fused form of the one-pass rebasing step (AP_FLAG_REBASE
+                                only; no reference counterpart): 2 Z + dz, the step and |dz|^2 each
+                                as fused multiply-adds, leaps as AP_ARITH_REF_CUDA */
 
 /* Launch modes of the unified render pass (cuda_kernels.py:1615-1917). */
 #define AP_MODE_COARSE 0     /* one centred sample per pixel -> iter map + RGB */

@@ -797,6 +797,9 @@ static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, do
 /*   else the largest BLA level with m + 2^d < ref_len, k + 2^d <= max_iter   */
 /*   and |dz|^2 < r_d^2 (levels 0..8 only for an underflowed |dz|^2);         */
 /*   else one perturbation step.  Interior after max_iter.                    */
+/*   AP_ARITH_FAST (this form only): |dz|^2, |z|^2 as fma(x, x, y*y); the     */
+/*   Mandelbrot step a = fma(2, Z, dz), dz' = fma(a, dz, ...) + dc fused;       */
+/*   leaps in the CUDA profile's form.                                        */
 /* ------------------------------------------------------------------------- */
 static int floor_log2(int v) {
     int r = 0;
@@ -810,6 +813,7 @@ static int floor_log2(int v) {
 static Sample rebase_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
                                double sub_j) {
     const int ft = p->fractal_type, cpu = p->arith == AP_ARITH_REF_CPU;
+    const int fast = p->arith == AP_ARITH_FAST;
     const int ref_len = p->ref_len, max_iter = p->max_iter;
     const double* re = b->ref_re;
     const double* im = b->ref_im;
@@ -830,12 +834,12 @@ static Sample rebase_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, 
     while (k < max_iter) {
         const double rx = re[m], ry = im[m];
         const double zx = rx + dzx, zy = ry + dzy;
-        const double mag2 = zx * zx + zy * zy;
+        const double mag2 = fast ? fma(zx, zx, zy * zy) : zx * zx + zy * zy;
         if (!(mag2 <= BAILOUT)) {
             if (isnan(mag2)) return glitch_at(k);
             return escaped(k, mag2, inv_ln);
         }
-        const double dz_mag2 = dzx * dzx + dzy * dzy;
+        const double dz_mag2 = fast ? fma(dzx, dzx, dzy * dzy) : dzx * dzx + dzy * dzy;
         if (mag2 < dz_mag2 || (m == ref_len && m > 0)) {
             dzx = zx;
             dzy = zy;
@@ -872,7 +876,11 @@ static Sample rebase_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, 
         }
         if (ft == 0) {
             double nx, ny;
-            if (cpu) {
+            if (fast) { /* a = 2Z + dz rounded once; (a dz) + dc fused */
+                const double ax = fma(2.0, rx, dzx), ay = fma(2.0, ry, dzy);
+                nx = fma(ax, dzx, fma(-ay, dzy, dcx));
+                ny = fma(ax, dzy, fma(ay, dzx, dcy));
+            } else if (cpu) {
                 nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
                 ny = 2.0 * ((rx + dzx) * dzy + ry * dzx) + dcy;
             } else {

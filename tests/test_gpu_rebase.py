@@ -28,9 +28,10 @@ RS, RMETA = load_golden("render_pert.npz")
 
 P99_BOUND = 1e-4
 K_IDENTICAL_BOUND = 0.999
+ARITH = {"ref_cpu": abi.AP_ARITH_REF_CPU, "ref_cuda": abi.AP_ARITH_REF_CUDA, "fast": abi.AP_ARITH_FAST}
 
 
-@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda"])
+@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda", "fast"])
 def test_config3_one_pass_frame_meets_accuracy_bound(arith):
     import torch
     m = next(x for x in PMETA if x["name"] == "cfg3")
@@ -56,7 +57,7 @@ def test_config3_one_pass_frame_meets_accuracy_bound(arith):
     dcm = max_delta_c(m["ref_px"], m["ref_py"], W, H, m["dx"], m["dy"])
     T = oracle.build_bla_dc(re, im, rl, 0, engine.ACCURATE_BLA_EPS, dcm, 16, 3, 0.25, 1.0)
     p = abi.new_params(width=W, height=H, max_iter=m["max_iter"], tier=abi.AP_TIER_PERTURB,
-                       arith=abi.AP_ARITH_REF_CPU if arith == "ref_cpu" else abi.AP_ARITH_REF_CUDA,
+                       arith=ARITH[arith],
                        dx_hi=m["dx"], dy_hi=m["dy"], ref_px=m["ref_px"], ref_py=m["ref_py"], ref_len=rl,
                        bla_levels=16, flags=abi.AP_FLAG_REBASE)
     _, g, ko, so = oracle.pert_grid(p, re, im, T, cols.astype(np.float64), rows.astype(np.float64),
@@ -71,7 +72,7 @@ FRAME_CASES = ["cfg3_bla_pauldelbrot", "cfg3_plain", "cfg3_hist", "cfg3_ssaa2", 
 
 
 @pytest.mark.parametrize("name", FRAME_CASES)
-@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda"])
+@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda", "fast"])
 @pytest.mark.parametrize("bla_form", ["reference", "accurate"])
 def test_one_pass_frames_match_oracle(name, arith, bla_form):
     import torch
@@ -89,8 +90,7 @@ def test_one_pass_frames_match_oracle(name, arith, bla_form):
         bbsa_order=m["bbsa_order"], glitch_mode=ONE_PASS_REBASING, gen_n=m["gen_n"], gen_kr=m["gen_kr"],
         gen_ki=m["gen_ki"], h_iter_buf=it, arith=arith, bla_form=bla_form, _extra_out=(kmap, s64))
     assert perturbation.LAST_FRAME_STATS["rebase_passes"] == 0
-    code = abi.AP_ARITH_REF_CPU if arith == "ref_cpu" else abi.AP_ARITH_REF_CUDA
-    fr, passes = oracle_pert_frame(m, arith=code,
+    fr, passes = oracle_pert_frame(m, arith=ARITH[arith],
                                    bla_eps=engine.ACCURATE_BLA_EPS if bla_form == "accurate" else None)
     assert passes == 0
     assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32)), \
@@ -127,6 +127,25 @@ def test_one_pass_counters_count_rebases():
     assert c[..., 3].min() >= 0 and c[..., 3].mean() > 1.0  # most pixels restart more than once
     assert not c[..., 2].any()    # no direct-iteration stage
     assert np.all(c[..., 0] + c[..., 1] > 0)
+
+
+def test_fast_profile_serves_one_pass_rebasing_only():
+    """arith='fast' is the one-pass form's own arithmetic: other glitch modes and other
+    passes refuse it."""
+    with pytest.raises(ValueError):
+        engine.render_frame_ssaa(64, 36, 1000, Decimal("-0.75"), Decimal("0.1"), Decimal("1e-14"), None,
+                                 precision_mode="1e-300 (Perturbation)", glitch_mode="Pauldelbrot",
+                                 arith="fast")
+    import torch
+    L = _lib.load()
+    it = torch.zeros((8, 8), dtype=torch.float32, device="cuda")
+    orbit = torch.zeros(5, dtype=torch.float64, device="cuda")
+    p = abi.new_params(width=8, height=8, max_iter=10, tier=abi.AP_TIER_PERTURB, ref_len=4,
+                       arith=abi.AP_ARITH_FAST, flags=abi.AP_FLAG_NO_RGB)
+    b = abi.ApFrameBuffers()
+    b.iter_map = C.c_void_p(it.data_ptr())
+    b.ref_re = b.ref_im = C.c_void_p(orbit.data_ptr())
+    assert L.ap_render_pass(C.byref(p), C.byref(b), None) == abi.AP_E_UNSUPPORTED
 
 
 def test_one_pass_rejects_unserved_cases():

@@ -48,7 +48,7 @@ def errors(k, s64, ts):
     return float(np.percentile(err, 99)), float(np.mean(k == np.floor(ts))), float(err.max())
 
 
-@pytest.mark.parametrize("arith", [abi.AP_ARITH_REF_CPU, abi.AP_ARITH_REF_CUDA])
+@pytest.mark.parametrize("arith", [abi.AP_ARITH_REF_CPU, abi.AP_ARITH_REF_CUDA, abi.AP_ARITH_FAST])
 @pytest.mark.parametrize("bla", [True, False])
 def test_one_pass_config3_meets_accuracy_bound(arith, bla):
     ts, rows, cols = truth()
