@@ -19,6 +19,10 @@
 
 #include "ap_common.cuh"
 
+#ifndef AP_REBASE_PREFETCH
+#define AP_REBASE_PREFETCH 0
+#endif
+
 namespace ap {
 
 constexpr int kFtQuad = 0;   // Mandelbrot (0) and its Julia set (2)
@@ -327,19 +331,41 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
     double dzx = s.dzx, dzy = s.dzy;
     SampleOut o = s.o;
     bool paused = false;
+#if AP_REBASE_PREFETCH
+    double4 Znext = ldg4(orb + m);
+#endif
     while (k < max_iter) {
         if (BUDGET && --budget < 0) {
             paused = true;
             break;
         }
+#if AP_REBASE_PREFETCH
+        // the record of the common path's next step is requested one step ahead
+        const double4 Z = Znext;
+        Znext = ldg4(orb + min(m + 1, ref_len));
+#else
         const double4 Z = ldg4(orb + m);
+#endif
         const double rx = Z.x, ry = Z.y;
-        const double zx = rx + dzx, zy = ry + dzy;
+        // z itself: every step but the fused Mandelbrot one uses it; that one forms it
+        // only where a test can fire
+        constexpr bool kLateZ = kFast && FT == kFtQuad;
+        double zx = 0.0, zy = 0.0;
+        if (!kLateZ) {
+            zx = rx + dzx;
+            zy = ry + dzy;
+        }
         const double dz_mag2 = kFast ? fma(dzx, dzx, dzy * dzy) : dzx * dzx + dzy * dzy;
-        const bool unsafe = !(dz_mag2 < Z.z) || m == ref_len;
+        // ap_pack_orbit leaves the orbit's last record (m == ref_len) with safe radius 0,
+        // so the end of the reference takes this branch without a test of its own
+        const bool unsafe = !(dz_mag2 < Z.z);
         const bool leap = BLA && (dz_mag2 < Z.w);
         if (unsafe || leap) {
             if (unsafe) {
+                if (kLateZ) {
+                    zx = rx + dzx;
+                    zy = ry + dzy;
+                }
                 const double mag2 = kFast ? fma(zx, zx, zy * zy) : zx * zx + zy * zy;
                 if (!(mag2 <= kBailout)) {
                     if (isnan(mag2)) {
@@ -359,6 +385,9 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                     dzy = zy;
                     m = 0;
                     ++rebases;
+#if AP_REBASE_PREFETCH
+                    Znext = ldg4(orb);
+#endif
                     continue;
                 }
             }
@@ -401,6 +430,9 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                 k += 1 << lo;
                 ++leaps;
                 skipped += 1 << lo;
+#if AP_REBASE_PREFETCH
+                Znext = ldg4(orb + m);
+#endif
                 continue;
             }
         }

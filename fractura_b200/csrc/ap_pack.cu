@@ -24,6 +24,7 @@ __global__ void __launch_bounds__(256) pack_orbit_kernel(const double* __restric
     double s = 256.0 * (1.0 - 1e-12) - rz * (1.0 + 1e-12);
     s = fmin(s, rz * (1.0 - 1e-12) * 0.5 * (1.0 - 1e-7));
     s = s > 0.0 ? s : 0.0;
+    if (k == n - 1) s = 0.0;  // the orbit's end is never a safe step (the rebase kernels rely on it)
     // slot 3: the level-0 BLA radius, written by ap_pack_bla (0: no leap)
     out[k] = make_double4(rx, ry, s * s * (1.0 - 1e-12), 0.0);
 }

@@ -6,8 +6,12 @@
 
 namespace ap {
 
+#ifndef AP_REBASE_MIN_BLOCKS
+#define AP_REBASE_MIN_BLOCKS 4
+#endif
+
 template <int ARITH, int FT, bool BLA, bool REBASE>
-__global__ void __launch_bounds__(256, 4) perturb_coarse_kernel(const ApFrameParams p,
+__global__ void __launch_bounds__(256, REBASE ? AP_REBASE_MIN_BLOCKS : 4) perturb_coarse_kernel(const ApFrameParams p,
                                                                 const ApFrameBuffers b) {
     // each warp takes an 8 x 4 patch of its block's 16 x 16 pixels: neighbours
     // follow similar paths through the loop, so compact warps diverge less

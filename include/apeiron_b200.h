@@ -184,7 +184,8 @@ AP_API int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t height
  * 32-byte record (Z_re, Z_im, safe radius^2, level-0 BLA radius^2).  While the
  * rounded |dz|^2 is below the safe radius^2 neither the escape test, the glitch
  * test (|Z + dz|^2 < 1e-6 |Z|^2 where |Z|^2 > 1e-8, math_core/cpu_kernels.py:428-431)
- * nor the rebase test of AP_FLAG_REBASE (|Z + dz| < |dz|) can fire at that step.  The level-0 radius is written by ap_pack_bla; this call
+ * nor the rebase test of AP_FLAG_REBASE (|Z + dz| < |dz|) can fire at that step.  The
+ * last record (step ref_len) always has safe radius 0.  The level-0 radius is written by ap_pack_bla; this call
  * leaves it 0 (no leap).  out: [ref_len + 1, 4] float64. */
 AP_API int ap_pack_orbit(const double* ref_re, const double* ref_im, int32_t ref_len, double* out,
                          void* stream);
