@@ -95,6 +95,7 @@ class ApGradView(C.Structure):
 
 AP_STRICT_DD = 1
 AP_STRICT_LIMBS = 2
+AP_STRICT_FP64 = 3
 AP_STRICT_NLIMBS = 34
 
 

@@ -15,6 +15,7 @@
 // as many SMs as possible: the pass is latency-bound, not throughput-bound.
 #include "ap_common.cuh"
 #include "ap_dd.cuh"
+#include "ap_fp64.cuh"
 
 namespace ap {
 namespace {
@@ -184,6 +185,10 @@ __global__ void __launch_bounds__(kStrictThreads) strict_eval_kernel(
     float s;
     if (v.tier == AP_STRICT_DD) {
         s = dd_sample_at<AP_ARITH_REF_CUDA>(p, (double)c, (double)r).s;
+    } else if (v.tier == AP_STRICT_FP64) {
+        const double x = p.x_min_hi + (double)c * p.dx_hi;
+        const double y = p.y_max_hi - (double)r * p.dy_hi;
+        s = fp64_sample<AP_ARITH_REF_CUDA>(x, y, p).s;
     } else {
         uint32_t* mine = s_pix + threadIdx.x * kCStride;
         for (int i = 0; i < 2 * NL; ++i) mine[i] = __ldg(limbs + (size_t)q * 2 * NL + i);
@@ -211,7 +216,7 @@ extern "C" int ap_strict_eval(const ApFrameParams* p, const ApFrameBuffers* b, c
                               int32_t n, void* stream) {
     if (!p || !b || !v || !b->iter_map || !b->rgb || !b->lut || n < 0 || (n > 0 && !coords) ||
         p->width <= 0 || p->height <= 0 || p->max_iter < 0 ||
-        (v->tier != AP_STRICT_DD && v->tier != AP_STRICT_LIMBS) ||
+        (v->tier != AP_STRICT_DD && v->tier != AP_STRICT_LIMBS && v->tier != AP_STRICT_FP64) ||
         (v->tier == AP_STRICT_LIMBS && n > 0 && (!signs || !limbs))) {
         ap::set_error("ap_strict_eval: bad arguments");
         return AP_E_INVALID;

@@ -431,6 +431,97 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
     return out
 
 
+def compute_bbsa_coeffs_cuda(d_ref_re, d_ref_im, ref_len, max_r, fractal_type, bbsa_tol=1e-4, bbsa_order=4,
+                             gen_n=3, gen_kr=0.25, gen_ki=1.0, E_scale=0, stream=0, h_ref_re=None,
+                             h_ref_im=None):
+    """(skip, a1_re, a1_im, ..., a8_re, a8_im) of the series-approximation start of one
+    reference orbit (math_core/engine.py:426-470): the reference's guards (types 0, 2, 4,
+    positive tolerance, order and radius, ref_len >= 2; chained-BLA order 32 has no
+    series), then the library's host recurrence (ap_bbsa_coeffs) on the host copy of the
+    orbit (h_ref_re / h_ref_im, else a copy of the device arrays)."""
+    from .perturbation import bbsa_coefficients
+    zero = (0,) + (0.0,) * 16
+    if fractal_type not in (0, 2, 4) or bbsa_tol <= 0.0 or bbsa_order <= 0 or ref_len < 2 or max_r <= 0.0:
+        return zero
+    if bbsa_order == 32:
+        return zero
+
+    def host(a):
+        if a is None:
+            return None
+        if hasattr(a, "detach"):
+            return a.detach().cpu().numpy()
+        return np.asarray(a)
+    re = host(h_ref_re) if h_ref_re is not None else host(d_ref_re)
+    im = host(h_ref_im) if h_ref_im is not None else host(d_ref_im)
+    out = bbsa_coefficients(_lib.load(), re, im, int(ref_len), float(max_r), int(fractal_type), float(bbsa_tol),
+                            int(bbsa_order), int(gen_n), float(gen_kr), float(gen_ki), int(E_scale))
+    return (int(out[0]),) + tuple(float(x) for x in out[1:17])
+
+
+def eval_glitched_pixels_fallback_cuda(d_out_rgb, d_glitch_out, d_lut, glitched_indices, target_w, target_h,
+                                       max_iter, center_x_dec, center_y_dec, plot_width_dec, plot_height_dec,
+                                       color_scheme_id, fractal_type, julia_cx, julia_cy, gen_n=3, gen_kr=0.25,
+                                       gen_ki=1.0, palette_offset=0.0, color_density=1.0, color_contrast=1.0,
+                                       d_cdf_lut=None, num_bins=2048, cmap_name="inferno", is_hdr=False,
+                                       stream=0, d_iter_map=None, stream_slot=0):
+    """Re-evaluate the listed glitched pixels ((row, col) pairs) each on its own orbit and
+    write their value, colour and cleared glitch flag (Strict Metric fallback of the CUDA
+    path, math_core/engine.py:270-410).  Tiers as the reference picks them: FP64 at widths
+    >= 1e-12, double-double >= 1e-30, 34-limb fixed point >= 1e-315 (Multibrot on the
+    host), the host beyond.  With d_cdf_lut the colour is the histogram transfer.  The
+    device arrays are torch CUDA tensors; d_lut None takes the registered LUT of cmap_name."""
+    from .perturbation import strict_device_inputs, strict_device_tier, strict_values
+    torch = _torch()
+    coords = np.asarray(glitched_indices, dtype=np.int64).reshape(-1, 2).astype(np.int32)
+    if len(coords) == 0:
+        return
+    st, stream_h = _stream_handle(stream)
+    W, H = int(target_w), int(target_h)
+    pw = plot_width_dec if isinstance(plot_width_dec, Decimal) else Decimal(str(plot_width_dec))
+    ph = plot_height_dec if isinstance(plot_height_dec, Decimal) else Decimal(str(plot_height_dec))
+    cx = center_x_dec if isinstance(center_x_dec, Decimal) else Decimal(str(center_x_dec))
+    cy = center_y_dec if isinstance(center_y_dec, Decimal) else Decimal(str(center_y_dec))
+    hist = d_cdf_lut is not None
+    p = abi.new_params(width=W, height=H, max_iter=int(max_iter), fractal_type=int(fractal_type),
+                       tier=abi.AP_TIER_FP64, arith=abi.AP_ARITH_REF_CUDA, gen_n=int(gen_n),
+                       gen_kr=float(gen_kr), gen_ki=float(gen_ki), scheme_id=11 if hist else int(color_scheme_id),
+                       num_bins=int(num_bins), palette_offset=float(palette_offset),
+                       color_density=float(color_density), color_contrast=float(color_contrast),
+                       is_hdr=int(bool(is_hdr)))
+    lut = d_lut if d_lut is not None else get_device_lut(cmap_name, is_hdr)
+    it = d_iter_map if d_iter_map is not None else get_scratch_device_array((H, W), np.float32,
+                                                                            f"fallback_iter_{stream_slot}")
+    b = abi.ApFrameBuffers()
+    b.rgb, b.glitch_out, b.lut, b.iter_map = _ptr(d_out_rgb), _ptr(d_glitch_out), _ptr(lut), _ptr(it)
+    b.cdf = _ptr(d_cdf_lut) if hist else None
+    L = _lib.load()
+    tier = strict_device_tier(pw, int(fractal_type))
+    with torch.cuda.stream(st):
+        dev = it.device
+
+        def upload(a):
+            return torch.from_numpy(np.ascontiguousarray(a)).to(dev, non_blocking=False)
+
+        d_coords = upload(coords)
+        if tier is None:
+            values = strict_values(coords, W, H, int(max_iter), cx, cy, pw, ph, int(fractal_type), julia_cx,
+                                   julia_cy, gen_n, gen_kr, gen_ki)
+            d_vals = upload(values)
+            q = abi.ApFrameParams.from_buffer_copy(p)
+            q.arith = abi.AP_ARITH_REF_CPU  # the host evaluator colours with the CPU transfer functions
+            _lib.launch(L.ap_set_pixels, C.byref(q), C.byref(b), _ptr(d_coords), _ptr(d_vals),
+                        int(len(coords)), stream_h, what="ap_set_pixels")
+        else:
+            q, view, signs, limbs = strict_device_inputs(p, coords, tier, W, H, cx, cy, pw, ph, julia_cx,
+                                                         julia_cy)
+            d_signs = upload(signs) if signs is not None else None
+            d_limbs = upload(limbs.view(np.int32)) if limbs is not None else None
+            _lib.launch(L.ap_strict_eval, C.byref(q), C.byref(b), C.byref(view), _ptr(d_coords),
+                        _ptr(d_signs), _ptr(d_limbs), int(len(coords)), stream_h, what="ap_strict_eval")
+        st.synchronize()
+
+
 def _copy_to_host(dev, host, st):
     """Device -> host copy on stream ``st`` into ``host`` (or a new array)."""
     torch = _torch()

@@ -580,8 +580,10 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
 
 def strict_device_tier(plot_width_dec, fractal_type):
     """Device tier of the CUDA path's Strict Metric fallback (math_core/engine.py:285-296,
-    :330): double-double down to 1e-30, 34-limb fixed point down to 1e-315 except for
-    Multibrot, None where the reference evaluates on the host."""
+    :330): FP64 down to 1e-12, double-double down to 1e-30, 34-limb fixed point down to
+    1e-315 except for Multibrot, None where the reference evaluates on the host."""
+    if plot_width_dec >= Decimal("1e-12"):
+        return abi.AP_STRICT_FP64
     if plot_width_dec >= Decimal("1e-30"):
         return abi.AP_STRICT_DD
     if plot_width_dec >= Decimal("1e-315") and fractal_type != 4:
@@ -623,7 +625,7 @@ def strict_device_inputs(p, coords, tier, W, H, center_x_dec, center_y_dec, plot
         y_max = center_y_dec + (plot_height_dec / Decimal(2))
         dx = plot_width_dec / Decimal(max(1, W - 1))
         dy = plot_height_dec / Decimal(max(1, H - 1))
-        if tier == abi.AP_STRICT_DD:
+        if tier in (abi.AP_STRICT_DD, abi.AP_STRICT_FP64):
             q.x_min_hi, q.x_min_lo = to_dd(x_min, ctx)
             q.y_max_hi, q.y_max_lo = to_dd(y_max, ctx)
             q.dx_hi, q.dx_lo = to_dd(dx, ctx)

@@ -255,6 +255,8 @@ AP_API int ap_set_pixels(const ApFrameParams* p, const ApFrameBuffers* b, const 
  * Colours use p->arith's transfer functions and, for scheme 11, b->cdf. */
 #define AP_STRICT_DD 1
 #define AP_STRICT_LIMBS 2
+#define AP_STRICT_FP64 3   /* views of width >= 1e-12: c = x_min_hi + col dx_hi, y_max_hi - row dy_hi
+                              in FP64, iterated as compute_fp64_sample (the CUDA source form) */
 #define AP_STRICT_NLIMBS 34
 typedef struct ApStrictView {
     int32_t tier;

@@ -1499,7 +1499,7 @@ static float ml_sample(int cxs, const uint32_t* cxl, int cys, const uint32_t* cy
 }
 
 /* eval_glitched_pixels_cuda_kernel / _hist_ (math_core/cuda_kernels.py:2450-2569):
-   each listed pixel iterated on its own in double-double or in fixed point, then the
+   each listed pixel iterated on its own in FP64, double-double or fixed point, then the
    float32 value, its colour (black below 0) and a cleared glitch flag written. */
 APO_EXPORT int apo_strict_eval(const ApFrameParams* p, const ApFrameBuffers* b, const ApStrictView* v,
                                const int32_t* coords, const int32_t* signs, const uint32_t* limbs, int n) {
@@ -1512,6 +1512,10 @@ APO_EXPORT int apo_strict_eval(const ApFrameParams* p, const ApFrameBuffers* b, 
         float s;
         if (v->tier == AP_STRICT_DD) {
             s = dd_sample_at(&q, (double)c, (double)r).s;
+        } else if (v->tier == AP_STRICT_FP64) { /* precision_tier 0, cuda_kernels.py:2474-2477 */
+            const double x = p->x_min_hi + (double)c * p->dx_hi;
+            const double y = p->y_max_hi - (double)r * p->dy_hi;
+            s = fp64_sample(x, y, &q).s;
         } else {
             const uint32_t* l = limbs + (size_t)t * 2 * ML_N;
             s = ml_sample(signs[2 * t], l, signs[2 * t + 1], l + ML_N, p->max_iter, p->fractal_type,

@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ by running the reference.
 
-Run in a container that holds the reference tree (default /root/reference,
-override with APEIRON_REFERENCE_ROOT):
+Run where the reference's source tree is available, with APEIRON_REFERENCE_ROOT set to
+it (the directory holding config.py and math_core/):
 
-    python tests/golden/make_golden.py [section ...]
+    APEIRON_REFERENCE_ROOT=<reference tree> python tests/golden/make_golden.py [section ...]
 
 Every fixture records the inputs it was made from, so the tests rebuild the
 same inputs without the reference.  Sections:

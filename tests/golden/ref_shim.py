@@ -10,7 +10,10 @@ import os
 import sys
 import types
 
-REF_ROOT = os.environ.get("APEIRON_REFERENCE_ROOT", "/root/reference")
+REF_ROOT = os.environ.get("APEIRON_REFERENCE_ROOT")
+if not REF_ROOT:
+    raise SystemExit("set APEIRON_REFERENCE_ROOT to the reference's source tree (the directory that holds "
+                     "config.py and math_core/) to regenerate fixtures")
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 

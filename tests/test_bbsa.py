@@ -92,3 +92,31 @@ def test_series_started_frames_against_reference(name):
     ref = R[name + "__iter"]
     assert np.array_equal(fr.iter_map.view(np.uint32), ref.view(np.uint32)), \
         int((fr.iter_map.view(np.uint32) != ref.view(np.uint32)).sum())
+
+
+@pytest.mark.parametrize("tag", [m["tag"] for m in BMETA])
+def test_engine_compute_bbsa_coeffs_cuda_matches_reference(tag):
+    """engine.compute_bbsa_coeffs_cuda (the drop-in for math_core/engine.py:426) returns
+    the reference's (skip, 16 coefficients) tuple, bit for bit, from device or host arrays."""
+    from fractura_b200 import engine
+    bm = next(x for x in BMETA if x["tag"] == tag)
+    m = pert_case(bm["name"])
+    re, im = P[m["name"] + "__re"], P[m["name"] + "__im"]
+    got = engine.compute_bbsa_coeffs_cuda(re, im, m["ref_len"], float(Decimal(m["width"])) * 0.75,
+                                          m["fractal_type"], bbsa_tol=bm["tol"], bbsa_order=bm["order"],
+                                          gen_n=m["gen_n"], gen_kr=m["gen_kr"], gen_ki=m["gen_ki"],
+                                          h_ref_re=re, h_ref_im=im)
+    ref = B[tag + "__coeffs"]
+    assert got[0] == int(ref[0]) and isinstance(got[0], int)
+    assert np.array_equal(np.array(got[1:], np.float64).view(np.uint64), ref[1:].view(np.uint64))
+
+
+def test_engine_compute_bbsa_coeffs_cuda_guards():
+    from fractura_b200 import engine
+    m = pert_case("cfg3")
+    re, im = P["cfg3__re"], P["cfg3__im"]
+    zero = (0,) + (0.0,) * 16
+    assert engine.compute_bbsa_coeffs_cuda(re, im, m["ref_len"], 1e-160, 1) == zero          # Burning Ship
+    assert engine.compute_bbsa_coeffs_cuda(re, im, m["ref_len"], 1e-160, 0, bbsa_order=32) == zero
+    assert engine.compute_bbsa_coeffs_cuda(re, im, 1, 1e-160, 0) == zero                     # ref_len < 2
+    assert engine.compute_bbsa_coeffs_cuda(re, im, m["ref_len"], 0.0, 0) == zero             # max_r <= 0

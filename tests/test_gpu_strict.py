@@ -113,3 +113,74 @@ def test_strict_frame_fixed_point_tier_through_engine():
     fr, _ = oracle_pert_frame(m, arith=1)
     assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32))
     assert rgb_mismatch(rgb, fr.rgb)[0] == 0
+
+
+@pytest.mark.parametrize("name", [m["name"] for m in SIM_FRAMES])
+def test_public_fallback_equals_reference_kernels(name):
+    """engine.eval_glitched_pixels_fallback_cuda (the drop-in for math_core/engine.py:270)
+    on the views where the reference's own fallback was run (Numba's CUDA simulator):
+    the iteration map, RGB and cleared glitch flags equal the reference's."""
+    import torch
+    from fractura_b200.palette import synthetic_lut
+    m = next(x for x in SIM_FRAMES if x["name"] == name)
+    W, H = m["W"], m["H"]
+    gl = SIM[f"frame_{name}__glitch_in"]
+    pw = Decimal(m["width"])
+    ph = pw * (Decimal(H) / Decimal(W))
+    d_rgb = torch.zeros((H, W, 3), dtype=torch.uint8, device="cuda")
+    d_gl = torch.from_numpy(gl.copy()).cuda()
+    d_it = torch.full((H, W), -7.0, dtype=torch.float32, device="cuda")
+    d_lut = torch.from_numpy(synthetic_lut()).cuda()
+    d_cdf = torch.from_numpy(np.ascontiguousarray(SIM[f"frame_{name}__cdf"])).cuda() if m["scheme"] == 11 else None
+    engine.eval_glitched_pixels_fallback_cuda(
+        d_rgb, d_gl, d_lut, np.argwhere(gl > 0), W, H, m["max_iter"], Decimal(m["cx"]), Decimal(m["cy"]), pw, ph,
+        m["scheme"], m["fractal_type"], m["julia_cx"], m["julia_cy"], gen_n=m["gen_n"], gen_kr=m["gen_kr"],
+        gen_ki=m["gen_ki"], d_cdf_lut=d_cdf, num_bins=65536 if m["scheme"] == 11 else 2048, d_iter_map=d_it)
+    it = d_it.cpu().numpy()
+    sel = gl > 0
+    assert np.array_equal(it[sel].view(np.uint32), SIM[f"frame_{name}__iter"][sel].view(np.uint32))
+    assert rgb_mismatch(d_rgb.cpu().numpy()[sel][None], SIM[f"frame_{name}__rgb"][sel][None])[0] == 0
+    assert np.array_equal(d_gl.cpu().numpy(), SIM[f"frame_{name}__glitch_out"])
+
+
+@pytest.mark.parametrize("ft", [0, 1, 2, 4])
+def test_public_fallback_fp64_tier_equals_oracle(ft):
+    """At widths >= 1e-12 the fallback iterates in FP64 (the reference's precision tier 0):
+    device == oracle, and the values equal the FP64 samples at c = x_min + col dx."""
+    import torch
+    from fractura_b200.palette import synthetic_lut
+    from fractura_b200.perturbation import strict_device_inputs, strict_device_tier
+    W, H, mi = 40, 24, 3000
+    cx, cy = {0: ("-0.7436", "0.1318"), 1: ("-1.76", "0.03"), 2: ("0.01", "0.3"), 4: ("-0.2", "0.75")}[ft]
+    pw = Decimal("1e-11")
+    ph = pw * (Decimal(H) / Decimal(W))
+    rng = np.random.default_rng(ft + 5)
+    coords = np.argwhere(rng.random((H, W)) < 0.3).astype(np.int32)
+    jx, jy = (-0.8, 0.156) if ft == 2 else (0.0, 0.0)
+    d_rgb = torch.zeros((H, W, 3), dtype=torch.uint8, device="cuda")
+    d_gl = torch.ones((H, W), dtype=torch.uint8, device="cuda")
+    d_it = torch.full((H, W), -7.0, dtype=torch.float32, device="cuda")
+    lut = synthetic_lut()
+    engine.eval_glitched_pixels_fallback_cuda(
+        d_rgb, d_gl, torch.from_numpy(lut).cuda(), coords, W, H, mi, Decimal(cx), Decimal(cy), pw, ph, 5, ft,
+        jx, jy, gen_n=3, gen_kr=0.1, gen_ki=0.2, d_iter_map=d_it)
+    fr = oracle.Frame(W, H, lut=lut)
+    fr.iter_map[...] = -7.0
+    fr.glitch_out[...] = 1
+    p = abi.new_params(width=W, height=H, max_iter=mi, fractal_type=ft, scheme_id=5, gen_n=3, gen_kr=0.1,
+                       gen_ki=0.2, arith=abi.AP_ARITH_REF_CUDA)
+    tier = strict_device_tier(pw, ft)
+    assert tier == abi.AP_STRICT_FP64
+    q, view, signs, limbs = strict_device_inputs(p, coords, tier, W, H, Decimal(cx), Decimal(cy), pw, ph, jx, jy)
+    oracle.strict_eval(q, fr, view, coords, signs, limbs)
+    it = d_it.cpu().numpy()
+    assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32))
+    assert rgb_mismatch(d_rgb.cpu().numpy(), fr.rgb)[0] == 0
+    assert np.array_equal(d_gl.cpu().numpy(), fr.glitch_out)
+    assert not fr.glitch_out[coords[:, 0], coords[:, 1]].any()
+    q.tier = abi.AP_TIER_FP64
+    xs = q.x_min_hi + coords[:, 1].astype(np.float64) * q.dx_hi
+    ys = q.y_max_hi - coords[:, 0].astype(np.float64) * q.dy_hi
+    for t in range(len(coords)):
+        s32, _, _ = oracle.fp64_grid(q, xs[t:t + 1], ys[t:t + 1])
+        assert s32[0, 0] == it[coords[t, 0], coords[t, 1]]
