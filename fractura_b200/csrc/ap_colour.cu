@@ -283,6 +283,42 @@ extern "C" int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t he
     return ap::check_launch("cdf_kernel");
 }
 
+extern "C" int ap_histogram(const float* iter_map, int32_t width, int32_t height, int32_t max_iter,
+                            int32_t num_bins, int32_t* hist, void* stream) {
+    if (!iter_map || !hist || width < 0 || height < 0 || num_bins < 2 || num_bins > (1 << 24)) {
+        ap::set_error("ap_histogram: bad arguments");
+        return AP_E_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(int32_t) * (size_t)num_bins, st);
+    if (e != cudaSuccess) {
+        ap::set_error("ap_histogram: memset: %s", cudaGetErrorString(e));
+        return AP_E_CUDA;
+    }
+    const size_t n = (size_t)width * height;
+    if (n == 0) return AP_OK;
+    const double inv_max = 1.0 / fmax(1.0, (double)max_iter);
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 148 * 16) blocks = 148 * 16;
+    ap::histogram_kernel<<<blocks, 256, 0, st>>>(iter_map, n, inv_max, num_bins, hist);
+    return ap::check_launch("histogram_kernel");
+}
+
+extern "C" int ap_cdf_from_histogram(const int32_t* hist, int32_t num_bins, float* cdf, void* stream) {
+    if (!hist || !cdf || num_bins < 2 || num_bins > (1 << 24)) {
+        ap::set_error("ap_cdf_from_histogram: bad arguments");
+        return AP_E_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (num_bins <= ap::kChunkMaxBins) {
+        const int blocks = (num_bins + ap::kChunkBins - 1) / ap::kChunkBins;
+        ap::cdf_chunk_kernel<<<blocks, ap::kChunkThreads, 0, st>>>(hist, num_bins, cdf);
+        return ap::check_launch("cdf_chunk_kernel");
+    }
+    ap::cdf_kernel<<<1, ap::kScanThreads, 0, st>>>(hist, num_bins, cdf);
+    return ap::check_launch("cdf_kernel");
+}
+
 extern "C" int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stream) {
     if (!p || !b || !b->iter_map || !b->rgb || !b->lut || p->width <= 0 || p->height <= 0) {
         ap::set_error("ap_colour: bad arguments");

@@ -24,6 +24,8 @@ int check_launch(const char* what);
 // Coarse-pass perturbation kernel on packed inputs (ap_perturb_fast.cu);
 // AP_E_UNSUPPORTED when the pass is not one it serves.
 int launch_perturb_fast(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st);
+int launch_perturb_fast_rows(const ApFrameParams& p, const ApFrameBuffers& b, int row0, int rows,
+                             cudaStream_t st);
 
 // FP32-mantissa FloatExp tier (ap_fe32.cu).
 int launch_fe32(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st);

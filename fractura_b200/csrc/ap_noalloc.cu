@@ -21,7 +21,8 @@ static __device__ __align__(256) int32_t g_noalloc_hist[kNoAllocMaxBins];
 
 // Device address of g_noalloc_hist per device, looked up once.  The name
 // g_noalloc_hist in host code is only a host-side stand-in, so the address
-// has to come from cudaGetSymbolAddress with the device current.
+// has to come from cudaGetSymbolAddress with the device current.  A device reset
+// reloads the module and makes the kept address stale; the header says so.
 static int32_t* g_noalloc_ptr[kMaxDevices] = {};
 static std::mutex g_noalloc_mu;
 

@@ -12,44 +12,49 @@ namespace ap {
 
 template <int ARITH, int FT, bool BLA, bool REBASE>
 __global__ void __launch_bounds__(256, REBASE ? AP_REBASE_MIN_BLOCKS : 4) perturb_coarse_kernel(const ApFrameParams p,
-                                                                const ApFrameBuffers b) {
+                                                                const ApFrameBuffers b, int row0,
+                                                                int row_end) {
     // each warp takes an 8 x 4 patch of its block's 16 x 16 pixels: neighbours
-    // follow similar paths through the loop, so compact warps diverge less
+    // follow similar paths through the loop, so compact warps diverge less; rows
+    // [row0, row_end) of the frame (a whole frame, or one band of a split frame)
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
     const int i = blockIdx.x * 16 + (w & 1) * 8 + (l & 7);
-    const int j = blockIdx.y * 16 + (w >> 1) * 4 + (l >> 3);
-    if (i >= p.width || j >= p.height) return;
+    const int j = row0 + blockIdx.y * 16 + (w >> 1) * 4 + (l >> 3);
+    if (i >= p.width || j >= row_end) return;
     coarse_pixel<ARITH, FT, BLA, REBASE>(p, b, i, j);
 }
 
 template <int ARITH, int FT>
-static void launch_ft(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
-    dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
+static void launch_ft(const ApFrameParams& p, const ApFrameBuffers& b, int r0, int r1, cudaStream_t st) {
+    dim3 grid((p.width + 15) / 16, (r1 - r0 + 15) / 16);
+    if (grid.y == 0) return;
     const bool rebase = (p.flags & AP_FLAG_REBASE) != 0;
     if constexpr (ARITH == AP_ARITH_FAST) {  // validated: AP_ARITH_FAST passes are rebasing passes
-        if (p.bla_levels > 1) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b);
-        else perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b);
+        if (p.bla_levels > 1) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
+        else perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
     } else if (p.bla_levels > 1) {
-        if (rebase) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b);
-        else perturb_coarse_kernel<ARITH, FT, true, false><<<grid, 256, 0, st>>>(p, b);
+        if (rebase) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
+        else perturb_coarse_kernel<ARITH, FT, true, false><<<grid, 256, 0, st>>>(p, b, r0, r1);
     } else {
-        if (rebase) perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b);
-        else perturb_coarse_kernel<ARITH, FT, false, false><<<grid, 256, 0, st>>>(p, b);
+        if (rebase) perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
+        else perturb_coarse_kernel<ARITH, FT, false, false><<<grid, 256, 0, st>>>(p, b, r0, r1);
     }
 }
 
 template <int ARITH>
-static void launch_arith(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
+static void launch_arith(const ApFrameParams& p, const ApFrameBuffers& b, int r0, int r1, cudaStream_t st) {
     switch (p.fractal_type) {
     case 1:
-    case 3: launch_ft<ARITH, kFtShip>(p, b, st); break;
-    case 4: launch_ft<ARITH, kFtMulti>(p, b, st); break;
-    default: launch_ft<ARITH, kFtQuad>(p, b, st); break;
+    case 3: launch_ft<ARITH, kFtShip>(p, b, r0, r1, st); break;
+    case 4: launch_ft<ARITH, kFtMulti>(p, b, r0, r1, st); break;
+    default: launch_ft<ARITH, kFtQuad>(p, b, r0, r1, st); break;
     }
 }
 
-// Returns AP_E_UNSUPPORTED when the pass is not one this kernel serves.
-int launch_perturb_fast(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
+// Rows [row0, row0 + rows) of the frame p; AP_E_UNSUPPORTED when the pass is not one
+// this kernel serves.
+int launch_perturb_fast_rows(const ApFrameParams& p, const ApFrameBuffers& b, int row0, int rows,
+                             cudaStream_t st) {
     const bool bla = p.bla_levels > 1 && (p.fractal_type == 0 || p.fractal_type == 2 ||
                                           p.fractal_type == 4);
     if (p.tier != AP_TIER_PERTURB || p.mode != AP_MODE_COARSE || !(p.flags & AP_FLAG_NO_RGB) ||
@@ -58,10 +63,15 @@ int launch_perturb_fast(const ApFrameParams& p, const ApFrameBuffers& b, cudaStr
         return AP_E_UNSUPPORTED;
     ApFrameParams q = p;
     if (!bla) q.bla_levels = 0;
-    if (q.arith == AP_ARITH_REF_CPU) launch_arith<AP_ARITH_REF_CPU>(q, b, st);
-    else if (q.arith == AP_ARITH_FAST) launch_arith<AP_ARITH_FAST>(q, b, st);
-    else launch_arith<AP_ARITH_REF_CUDA>(q, b, st);
+    const int r1 = row0 + rows;
+    if (q.arith == AP_ARITH_REF_CPU) launch_arith<AP_ARITH_REF_CPU>(q, b, row0, r1, st);
+    else if (q.arith == AP_ARITH_FAST) launch_arith<AP_ARITH_FAST>(q, b, row0, r1, st);
+    else launch_arith<AP_ARITH_REF_CUDA>(q, b, row0, r1, st);
     return check_launch("perturb_coarse_kernel");
+}
+
+int launch_perturb_fast(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
+    return launch_perturb_fast_rows(p, b, 0, p.height, st);
 }
 
 }  // namespace ap

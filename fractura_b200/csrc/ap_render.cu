@@ -258,3 +258,18 @@ extern "C" int ap_render_pass(const ApFrameParams* p, const ApFrameBuffers* b, v
 extern "C" int ap_resolve_hist_pass(const ApFrameParams* p, const ApFrameBuffers* b, void* stream) {
     return ap::dispatch(p, b, 1, stream);
 }
+
+extern "C" int ap_render_rows(const ApFrameParams* p, const ApFrameBuffers* b, int32_t row0, int32_t rows,
+                              void* stream) {
+    int rc = ap::validate_frame(p, b, 0);
+    if (rc != AP_OK) return rc;
+    if (row0 < 0 || rows < 0 || (long long)row0 + rows > p->height) {
+        ap::set_error("ap_render_rows: rows [%d, %d) outside the frame's %d rows", row0, row0 + rows, p->height);
+        return AP_E_INVALID;
+    }
+    rc = ap::launch_perturb_fast_rows(*p, *b, row0, rows, static_cast<cudaStream_t>(stream));
+    if (rc == AP_E_UNSUPPORTED)
+        ap::set_error("ap_render_rows serves coarse AP_TIER_PERTURB passes without in-kernel colour on "
+                      "packed inputs (ap_pack_orbit, ap_pack_bla)");
+    return rc;
+}

@@ -328,7 +328,7 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
                       compute_device="GPU", cpu_threads=2, palette_offset=0.0,
                       color_density=1.0, color_contrast=1.0, sync_stream=True,
                       d_iter_buf=None, h_iter_buf=None, stream_slot=None, arith=None,
-                      delta_form=None, bla_form=None, _extra_out=None):
+                      delta_form=None, bla_form=None, _extra_out=None, _rows=None, _orbit=None):
     """Render one frame and return its RGB image (math_core/engine.py:1339-2135).
 
     Same arguments as the reference; ``arith`` optionally selects the
@@ -404,6 +404,8 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
                            palette_offset=float(palette_offset), color_density=float(color_density),
                            color_contrast=float(color_contrast),
                            edge_threshold=float(np.float32(edge_threshold)), is_hdr=int(bool(is_hdr)))
+        if _rows is not None and tier < abi.AP_TIER_PERTURB:
+            raise NotImplementedError("bands of a frame serve the perturbation tiers")
         if tier in (abi.AP_TIER_FP64, abi.AP_TIER_DD):
             for k, v in plan_direct_view(W, H, factor, center_x_dec, center_y_dec, plot_width_dec,
                                          tier, julia_cx, julia_cy).items():
@@ -421,7 +423,7 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
                 gen_n=gen_n, gen_kr=gen_kr, gen_ki=gen_ki, edge_threshold=edge_threshold,
                 slot=slot, arith_code=arith_code, extra_out=_extra_out,
                 fp32_deltas=(delta_form == "fp32"),
-                bla_eps=ACCURATE_BLA_EPS if bla_form == "accurate" else None)
+                bla_eps=ACCURATE_BLA_EPS if bla_form == "accurate" else None, rows=_rows, orbit=_orbit)
 
         out = _copy_to_host(fr.rgb, h_rgb_buf, st)
         if h_iter_buf is not None:

@@ -316,8 +316,14 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
                               center_y_dec, plot_width_dec, tier, scheme, num_bins, fractal_type,
                               julia_cx, julia_cy, bbsa_tol, bbsa_order, glitch_mode, gen_n, gen_kr,
                               gen_ki, edge_threshold, slot, arith_code, extra_out=None,
-                              fp32_deltas=False, bla_eps=None):
-    """All device passes of one perturbation-tier frame (math_core/engine.py:1718-2113)."""
+                              fp32_deltas=False, bla_eps=None, rows=None, orbit=None):
+    """All device passes of one perturbation-tier frame (math_core/engine.py:1718-2113).
+
+    ``orbit`` (ref_cx, ref_cy, u, v, re, im, ref_len) replaces the reference search (a
+    split frame's ranks share rank 0's).  ``rows`` = (r0, r1) renders only that band of
+    the coarse pass (ap_render_rows) into the frame-size buffers and returns: no colour,
+    histogram or rebase pass (the split frame does those across ranks); it serves
+    factor 1 and the glitch modes that need no re-render pass."""
     import torch
     from .engine import _buffers, get_scratch_device_array
     L = _lib.load()
@@ -361,10 +367,15 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
                                        or "Pauldelbrot" in glitch_mode) else 0)
     LAST_FRAME_STATS.update(h2d_bytes=0, d2h_bytes=0, rebase_passes=0, strict_pixels=0, strict_tier=0)
 
-    bcx, bcy, bu, bv, re, im, ref_len = hp.find_optimal_reference_orbit(
-        center_x_dec, center_y_dec, plot_width_dec, plot_height_dec, max_iter, W, H,
-        fractal_type=fractal_type, julia_cx=julia_cx, julia_cy=julia_cy, gen_n=gen_n,
-        gen_kr=gen_kr, gen_ki=gen_ki, is_floatexp=floatexp)
+    if rows is not None and (factor != 1 or strict):
+        raise NotImplementedError("a band of a frame serves factor 1 with glitch modes 'One-Pass Rebasing' "
+                                  "or 'Off (Single-Ref)'")
+    if orbit is None:
+        orbit = hp.find_optimal_reference_orbit(
+            center_x_dec, center_y_dec, plot_width_dec, plot_height_dec, max_iter, W, H,
+            fractal_type=fractal_type, julia_cx=julia_cx, julia_cy=julia_cy, gen_n=gen_n,
+            gen_kr=gen_kr, gen_ki=gen_ki, is_floatexp=floatexp)
+    bcx, bcy, bu, bv, re, im, ref_len = orbit
     # Series-approximation start (math_core/engine.py:1816-1840): radius 0.75 w, same
     # inverse radius for every reference of the frame.
     max_r = float(plot_width_dec) * 0.75
@@ -406,6 +417,14 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     _lib.device_op(fr.glitch_in.zero_)
     orbit = (d_re, d_im)
     cdf = None
+    if rows is not None:
+        p.mode = abi.AP_MODE_COARSE
+        p.flags = unified_flags | abi.AP_FLAG_NO_RGB
+        b = _with_packed(_buffers(fr, lut, orbit=orbit, bla=bla, kmap=kmap, s64=s64), packed, fe32 is not None)
+        q = _coarse_params(p, fe32)
+        r0, r1 = int(rows[0]), int(rows[1])
+        _lib.launch(L.ap_render_rows, C.byref(q), C.byref(b), r0, r1 - r0, stream_h, what="ap_render_rows")
+        return dict(ref_len=ref_len, passes=0)
 
     if scheme == 11:
         hist = get_scratch_device_array((num_bins,), np.int32, f"hist_bins_{slot}")

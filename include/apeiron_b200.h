@@ -168,6 +168,16 @@ AP_API int ap_render_pass(const ApFrameParams* p, const ApFrameBuffers* b, void*
  * (math_core/cuda_kernels.py:2038-2234, launched at math_core/engine.py:1596-1635, :2048, :2092). */
 AP_API int ap_resolve_hist_pass(const ApFrameParams* p, const ApFrameBuffers* b, void* stream);
 
+/* Rows [row0, row0 + rows) of the frame p into the frame's full-size buffers (the
+ * other rows are left alone): one band of a frame split across GPUs.  Each pixel is
+ * evaluated exactly as ap_render_pass evaluates it (global row index, the same
+ * reference position), so bands assembled from any split equal the whole frame bit
+ * for bit.  Serves coarse AP_TIER_PERTURB passes without in-kernel colour on packed
+ * inputs (the perturbation tiers' fast kernel); AP_E_UNSUPPORTED otherwise.  No
+ * counterpart in the reference. */
+AP_API int ap_render_rows(const ApFrameParams* p, const ApFrameBuffers* b, int32_t row0, int32_t rows,
+                          void* stream);
+
 /* 8-neighbour edge mask.  Replaces edge_detect_kernel (math_core/cuda_kernels.py:1587). */
 AP_API int ap_edge_detect(const float* iter_map, uint8_t* edge_mask, int32_t width, int32_t height,
                    float threshold, void* stream);
@@ -212,6 +222,16 @@ AP_API int ap_pack_bla(const double* table, int32_t levels, int32_t ref_len, dou
 AP_API int ap_pack_fe32(const double* orbit_packed, int32_t ref_len, const double* table,
                         int32_t levels, double* orbit32_out, double* bla_out, void* stream);
 
+/* The two halves of ap_histogram_cdf, for a frame split across GPUs: ap_histogram counts
+ * (zeroing hist first) the escaped values of one band of the frame (histogram_kernel of
+ * math_core/cuda_kernels.py:1999-2013); after the bands' histograms are summed (an
+ * all-reduce), ap_cdf_from_histogram turns the sum into the normalised CDF exactly as
+ * ap_histogram_cdf does (the float64 scan of :1929-1996).  Neither has its own
+ * counterpart in the reference, which renders a frame on one GPU. */
+AP_API int ap_histogram(const float* iter_map, int32_t width, int32_t height, int32_t max_iter,
+                        int32_t num_bins, int32_t* hist, void* stream);
+AP_API int ap_cdf_from_histogram(const int32_t* hist, int32_t num_bins, float* cdf, void* stream);
+
 /* Largest num_bins ap_histogram_cdf_noalloc accepts (its built-in scratch, 256 KiB per GPU). */
 #define AP_NOALLOC_MAX_BINS 65536
 
@@ -220,8 +240,11 @@ AP_API int ap_pack_fe32(const double* orbit_packed, int32_t ref_len, const doubl
  * The histogram goes to an array compiled into the library (AP_NOALLOC_MAX_BINS
  * int32 per GPU, held from module load until process exit); num_bins above that
  * is rejected with AP_E_INVALID.  The first call on a device looks the array's
- * address up (cudaGetSymbolAddress), so make it before any stream capture.  All
- * calls on a device share the array: calls that overlap on the GPU race. */
+ * address up (cudaGetSymbolAddress), so make it before any stream capture.  The
+ * address is kept for the life of the process: after cudaDeviceReset (or any other
+ * teardown of the device's primary context) this entry point must not be called
+ * again on that device.  All calls on a device share the array: calls that overlap
+ * on the GPU race. */
 AP_API int ap_histogram_cdf_noalloc(const float* iter_map, int32_t width, int32_t height,
                                     int32_t max_iter, int32_t num_bins, float* cdf, void* stream);
 
