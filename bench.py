@@ -84,11 +84,12 @@ FLOPS_LEAP_REBASE = 22.0
 # Derivatives of the smooth value (csrc/ap_adjoint.cu), per iteration of a pixel's orbit:
 #   forward:  |z|^2 (3) + f(z) and f'(z): z^2 + c (8) and 2z (2)                       -> 13
 #             Multibrot n: z^(n-1) (6 (n-1)), z^n and P z (12), sums (4), f' (4), |z|^2 (3)
-#   adjoint:  the segment's forward step again (10; Multibrot 6 (n-1) + 20), the reverse
-#             step's f' recomputed with f (the same), G conj(f') (6), parameter sums
-#             (2; Multibrot 10)                                                      -> 28
+#   adjoint:  the step twice more (the segment's sub-checkpoint replay and the
+#             sub-segment's replay into shared memory: 2 x 10; Multibrot 2 x (6 (n-1) + 20)),
+#             the reverse step's f' (2; Multibrot 6 (n-1) + 4), G conj(f') (6), parameter
+#             sums (2; Multibrot 10)                                                 -> 30
 FLOPS_FWD_QUAD = 13.0
-FLOPS_ADJ_QUAD = 28.0
+FLOPS_ADJ_QUAD = 30.0
 
 
 def flops_fwd_multi(n):
@@ -96,7 +97,7 @@ def flops_fwd_multi(n):
 
 
 def flops_adj_multi(n):
-    return 2.0 * (6.0 * (n - 1) + 20.0) + 16.0
+    return 18.0 * (n - 1) + 60.0
 
 
 L2_FLUSH = "flushed between timed steps (512 MiB write)"

@@ -13,8 +13,9 @@
 //   ap_smooth_forward: s, K and checkpoints z_0, z_C, z_2C, ... (C = ckpt_every);
 //   ap_smooth_adjoint: per pixel, for the upstream gradient g = dL/ds, sweeps the
 //     orbit backwards one checkpoint segment at a time, recomputing the segment's
-//     z from its checkpoint into a per-thread buffer (no orbit is stored), and
-//     accumulates dL/dtheta; per-block sums (deterministic, summed by the caller);
+//     z from its checkpoint (first every 16th z, then each 16-step sub-segment into
+//     shared memory; no orbit is stored), and accumulates dL/dtheta; per-block sums
+//     (deterministic, summed by the caller);
 //   ap_smooth_tangent: forward mode (one tangent per parameter carried beside z),
 //     per-pixel ds/dtheta, the independent check of the adjoint.
 // Holomorphic steps make both sweeps complex multiplications: the adjoint
@@ -24,6 +25,11 @@
 namespace ap {
 
 constexpr int kMaxSegment = 1024;
+// The adjoint replays a checkpoint segment twice: once keeping z every kSub steps (local
+// memory, kMaxSubs values), then, sub-segment by sub-segment from the last, to hold that
+// sub-segment's z in shared memory for the reverse sweep.  No orbit reaches global memory.
+constexpr int kSub = 16;
+constexpr int kMaxSubs = kMaxSegment / kSub;
 
 struct C2d {
     double r, i;
@@ -85,9 +91,14 @@ __global__ void __launch_bounds__(256) smooth_forward_kernel(const ApGradView v,
     double s = -1.0;
     int K = -1;
     if (!skip) {
+        int until_ck = 0, slot = 0;  // steps to the next checkpoint, and its slot
         for (int k = 0; k < v.max_iter; ++k) {
-            if (ckpt && k % v.ckpt_every == 0 && k / v.ckpt_every < n_ck)
-                ckpt[idx * n_ck + k / v.ckpt_every] = make_double2(z.r, z.i);
+            if (until_ck == 0) {
+                if (ckpt && slot < n_ck) ckpt[idx * n_ck + slot] = make_double2(z.r, z.i);
+                ++slot;
+                until_ck = v.ckpt_every;
+            }
+            --until_ck;
             const double m = z.r * z.r + z.i * z.i;
             if (m > kBailout) {
                 const double lm = log(m);
@@ -118,6 +129,7 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
                                                              double* __restrict__ pix_grads,
                                                              double* __restrict__ block_sums) {
     __shared__ double red[5][128];
+    __shared__ double2 buf[kSub][128];  // one sub-segment of z per thread (32 KiB)
     const int tpr = (v.width + 15) / 16;  // blocks of 128 threads cover 16 x 8 pixels
     const int bx = blockIdx.x % tpr, by = blockIdx.x / tpr;
     const int i = bx * 16 + (threadIdx.x & 15);
@@ -132,7 +144,7 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
             double dpx_dw, dpy_dw;
             bool skip;
             pixel_setup(v, i, j, z0, c, dpx_dw, dpy_dw, skip);
-            double2 seg[kMaxSegment];
+            double2 sub[kMaxSubs];  // this segment's sub-checkpoints (local memory, 1 KiB)
             const int C = v.ckpt_every;
             C2d G = {0.0, 0.0};  // dL/dz_{k+1} during the sweep
             C2d gc = {0.0, 0.0}, gp = {0.0, 0.0};
@@ -142,8 +154,8 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
                 const int k1 = min(K, k0 + C);  // this segment's steps z_k -> z_{k+1}, k in [k0, k1)
                 const double2 st = ckpt[idx * n_ck + sg];
                 C2d z = {st.x, st.y}, d;
-                for (int k = k0; k < k1; ++k) {  // inputs z_k0 .. z_(k1-1): at most C values
-                    seg[k - k0] = make_double2(z.r, z.i);
+                for (int k = k0; k < k1; ++k) {  // pass 1: z every kSub steps
+                    if (((k - k0) & (kSub - 1)) == 0) sub[(k - k0) / kSub] = make_double2(z.r, z.i);
                     step_f(v, z, c, z, d);
                 }
                 if (first) {  // the last segment ends at k1 = K: z is z_K
@@ -151,8 +163,19 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
                     G = {gs * dz.r, gs * dz.i};
                     first = false;
                 }
-                for (int k = k1 - 1; k >= k0; --k) {
-                    const C2d zk = {seg[k - k0].x, seg[k - k0].y};
+                for (int s0 = k0 + ((k1 - k0 - 1) / kSub) * kSub; s0 >= k0 && k1 > k0; s0 -= kSub) {
+                  const int s1 = min(k1, s0 + kSub);
+                  {  // pass 2: this sub-segment's inputs z_s0 .. z_(s1-1) into shared memory
+                    const double2 w0 = sub[(s0 - k0) / kSub];
+                    C2d w = {w0.x, w0.y}, dw;
+                    for (int k = s0; k < s1; ++k) {
+                        buf[k - s0][threadIdx.x] = make_double2(w.r, w.i);
+                        step_f(v, w, c, w, dw);
+                    }
+                  }
+                  for (int k = s1 - 1; k >= s0; --k) {
+                    const double2 bk = buf[k - s0][threadIdx.x];
+                    const C2d zk = {bk.x, bk.y};
                     // parameter terms of z_{k+1} = f(z_k)
                     if (v.fractal_type == 2) {
                         gp = cadd2(gp, G);  // dz'/dP = 1
@@ -166,6 +189,7 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
                     C2d zn, dfdz;
                     step_f(v, zk, c, zn, dfdz);
                     G = cmul2(G, {dfdz.r, -dfdz.i});  // G_k = G_{k+1} conj(f'(z_k))
+                  }
                 }
             }
             if (v.fractal_type == 2) gc = G;  // the pixel is z_0

@@ -40,7 +40,7 @@ def whole_frame(v):
                                    precision_mode="1e-300 (Perturbation)", bbsa_order=32, bbsa_tol=1e-6,
                                    glitch_mode=v["glitch_mode"], arith=v["arith"], bla_form="accurate",
                                    d_iter_buf=it)
-    return it.cpu().numpy(), rgb.cpu().numpy()
+    return it.cpu().numpy(), (rgb.cpu().numpy() if hasattr(rgb, "cpu") else np.asarray(rgb))
 
 
 @pytest.mark.parametrize("scheme", [11, 5])
