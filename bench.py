@@ -153,13 +153,14 @@ def workload_cfg4():
     if not tiles:
         raise SystemExit("workloads.json holds no config4_tiles (python tests/golden/make_golden.py config4)")
     return dict(name="batch64_mixed_formulas_w1e-60_1e-12", kind="batch", tiles=tiles,
-                arith="ref_cpu", bla_form="accurate", dtype="f64", W=0, H=0, factor=1,
+                arith="ref_cuda", bla_form="accurate", dtype="f64", W=0, H=0, factor=1,
                 max_iter=max(t["max_iter"] for t in tiles), width="1e-60..1e-12",
-                bbsa_order=32, glitch_mode="Off (Single-Ref)", precision_mode="1e-300 (Perturbation)",
+                bbsa_order=32, glitch_mode="One-Pass Rebasing", precision_mode="1e-300 (Perturbation)",
                 scheme=0, fractal_type=-1,
                 form="one persistent work-stealing kernel over 64 tiles (FP64 deltas, dc-aware "
-                     "chained BLA, Pauldelbrot flags, one reference per tile), CUDA-graph replay, "
-                     "autotuned launch shape")
+                     "chained BLA, one reference per tile: one-pass rebasing for the Mandelbrot, "
+                     "Burning Ship and Multibrot tiles, Pauldelbrot flags for the Julia tiles), "
+                     "CUDA-graph replay, autotuned launch shape")
 
 
 def workload_cfg5():
@@ -301,10 +302,12 @@ def nominal_iterations(kmap, max_iter):
 
 def batch_tiles(wl):
     from fractura_b200 import batch as fb
+    rebase = "One-Pass" in wl.get("glitch_mode", "")
     return [fb.Tile(cx=Decimal(t["cx"]), cy=Decimal(t["cy"]), width=Decimal(t["width"]), W=t["W"], H=t["H"],
                     max_iter=t["max_iter"], fractal_type=t["fractal_type"], julia_cx=t["julia_cx"],
                     julia_cy=t["julia_cy"], gen_n=t["gen_n"], gen_kr=t["gen_kr"], gen_ki=t["gen_ki"],
-                    bla=True, strict_glitch=True) for t in wl["tiles"]]
+                    bla=True, strict_glitch=True, rebase=rebase and t["fractal_type"] in (0, 1, 4))
+            for t in wl["tiles"]]
 
 
 def config_of(wl, n_gpus):
@@ -760,18 +763,22 @@ def frame_arm(args, wl, rank, world, local_rank, steps, headline):
 
 
 # -------------------------------------------------------------- batch arm
-def step_flops(fractal_type, gen_n, strict, bla):
+def step_flops(fractal_type, gen_n, strict, bla, rebase=False):
     """(stage-1 step, BLA leap, stage-2 step) FP64 operations of coarse_pixel per formula
     (reference-CPU arithmetic, no fused ops): z = Z + dz and |dz|^2 (5), the
     Pauldelbrot test (4 when on), the radius test (3 when BLA is on), then the step:
     z^2 + c 13; Burning Ship 19 (the sign folds); Multibrot 22 per power beyond the
-    first plus 10 for K dz + dc.  Stage 2 iterates z directly: 8, 9, 3 + 6 (n - 1) + 10."""
+    first plus 10 for K dz + dc.  Stage 2 iterates z directly: 8, 9, 3 + 6 (n - 1) + 10.
+    One-pass rebasing (rebase_advance): z and |dz|^2 (5), |z|^2 (3), the step; leaps 22;
+    no stage 2."""
     if fractal_type in (1, 3):
         step, direct = 19.0, 9.0
     elif fractal_type == 4:
         step, direct = 22.0 * (gen_n - 1) + 10.0, 3.0 + 6.0 * (gen_n - 1) + 10.0
     else:
         step, direct = 13.0, 8.0
+    if rebase:
+        return 8.0 + step, FLOPS_LEAP_REBASE, 0.0
     return 5.0 + (4.0 if strict else 0.0) + (3.0 if bla else 0.0) + step, FLOPS_LEAP, direct
 
 
@@ -796,7 +803,8 @@ def batch_flops(torch, _lib, b, cfg):
     total = 0.0
     for slot, c in counters:
         p = arr[slot].p
-        f1, fl, f2 = step_flops(p.fractal_type, p.gen_n, p.strict_glitch > 0, p.bla_levels > 1)
+        f1, fl, f2 = step_flops(p.fractal_type, p.gen_n, p.strict_glitch > 0, p.bla_levels > 1,
+                                bool(p.flags & abi.AP_FLAG_REBASE))
         s = c.view(-1, 4).sum(dim=0, dtype=torch.int64).cpu().numpy()
         total += f1 * float(s[0]) + fl * float(s[1]) + f2 * float(s[2])
     return total

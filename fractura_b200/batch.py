@@ -47,6 +47,7 @@ class Tile:
     gen_ki: float = 1.0
     bla: bool = True           # chained-BLA leaps (Mandelbrot, Julia, Multibrot)
     strict_glitch: bool = True  # Pauldelbrot glitch flags
+    rebase: bool = False       # one-pass rebasing (Mandelbrot, Burning Ship, Multibrot): no glitch flags
 
 
 @dataclass(frozen=True)
@@ -170,6 +171,11 @@ def _tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch):
         stream.synchronize()  # the table scratch is reused by the next tile
     flags = abi.AP_FLAG_NO_RGB | ((abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem
                                   else abi.AP_FLAG_NAN_GUARD)
+    rebase = bool(t.rebase)
+    if rebase and t.fractal_type in (2, 3):
+        raise NotImplementedError("one-pass rebasing serves Mandelbrot, Burning Ship and Multibrot tiles")
+    if rebase:
+        flags |= abi.AP_FLAG_REBASE
     p = abi.new_params(width=t.W, height=t.H, factor=1, max_iter=int(t.max_iter),
                        fractal_type=int(t.fractal_type), tier=abi.AP_TIER_PERTURB,
                        arith=abi.AP_ARITH_REF_CPU if cpu_sem else abi.AP_ARITH_REF_CUDA,
@@ -178,7 +184,7 @@ def _tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch):
                        ref_px=ref_px, ref_py=ref_py, ref_cx=float(bcx), ref_cy=float(bcy),
                        julia_cx_hi=float(t.julia_cx), julia_cy_hi=float(t.julia_cy), ref_len=int(rl),
                        bla_levels=BLA_LEVELS if use_bla else 0,
-                       strict_glitch=1 if t.strict_glitch else 0)
+                       strict_glitch=1 if (t.strict_glitch and not rebase) else 0)
     out = dict(iter=torch.empty((t.H, t.W), dtype=torch.float32, device="cuda"),
                kmap=torch.empty((t.H, t.W), dtype=torch.int32, device="cuda"),
                glitch=torch.empty((t.H, t.W), dtype=torch.uint8, device="cuda"))

@@ -2,7 +2,8 @@
 // persistent kernel.
 //
 // A tile is one coarse perturbation pass (AP_TIER_PERTURB, packed orbit and
-// BLA rows, no in-kernel colour) with its own parameters and outputs.  Each
+// BLA rows, no in-kernel colour) with its own parameters and outputs, in the
+// single-reference form or in one-pass rebasing (AP_FLAG_REBASE).  Each
 // tile is cut into patches of patch_w x patch_h = 256 pixels; patches are
 // numbered tile after tile (the host orders tiles by estimated cost, largest
 // first).  The grid holds blocks_per_sm blocks per SM for the whole batch.  The
@@ -54,9 +55,29 @@ __device__ __noinline__ void tile_advance(const ApTileDesc* __restrict__ t, Pixe
     pixel_advance<ARITH, FT, BLA, true>(t->p, tile_buffers(t), s, kQuantum);
 }
 
+// The same for tiles in one-pass rebasing (AP_FLAG_REBASE; formula types 0, 1, 4).
+template <int ARITH, int FT, bool BLA>
+__device__ __noinline__ void tile_rebase_advance(const ApTileDesc* __restrict__ t, PixelRun& s) {
+    rebase_advance<ARITH, FT, BLA, true>(t->p, tile_buffers(t), s, kQuantum);
+}
+
 template <int ARITH>
 __device__ __forceinline__ void batch_advance(const ApTileDesc* t, PixelRun& s) {
     const bool bla = t->p.bla_levels > 1 && t->bla_packed != nullptr;
+    if (t->p.flags & AP_FLAG_REBASE) {
+        switch (t->p.fractal_type) {
+        case 1: tile_rebase_advance<ARITH, kFtShip, false>(t, s); break;
+        case 4:
+            if (bla) tile_rebase_advance<ARITH, kFtMulti, true>(t, s);
+            else tile_rebase_advance<ARITH, kFtMulti, false>(t, s);
+            break;
+        default:
+            if (bla) tile_rebase_advance<ARITH, kFtQuad, true>(t, s);
+            else tile_rebase_advance<ARITH, kFtQuad, false>(t, s);
+            break;
+        }
+        return;
+    }
     switch (t->p.fractal_type) {
     case 1:
     case 3: tile_advance<ARITH, kFtShip, false>(t, s); break;
@@ -170,7 +191,8 @@ extern "C" int ap_batch_plan(const ApTileDesc* tiles, int32_t n, int32_t patch_w
             (p.fractal_type == 4 && (p.gen_n < 1 || p.gen_n > 64)) || !t.orbit_packed ||
             !t.iter_map || (p.bla_levels > 1 && !t.bla_packed) ||
             (t.counters && (reinterpret_cast<uintptr_t>(t.counters) & 15u)) ||
-            (long long)p.width * p.height >= (1LL << 31)) {
+            (long long)p.width * p.height >= (1LL << 31) ||
+            ((p.flags & AP_FLAG_REBASE) && (p.fractal_type == 2 || p.fractal_type == 3 || p.ref_len < 1))) {
             ap::set_error("ap_batch_plan: tile %d is not a coarse AP_TIER_PERTURB pass on packed "
                           "inputs without in-kernel colour", q);
             return AP_E_INVALID;

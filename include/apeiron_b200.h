@@ -130,7 +130,8 @@ typedef struct ApFrameBuffers {
 
 /* One tile of a batch (ap_render_batch): a coarse AP_TIER_PERTURB pass on packed
  * inputs, without in-kernel colour (p.flags has AP_FLAG_NO_RGB), with its own
- * parameters, reference orbit and outputs.  448 bytes. */
+ * parameters, reference orbit and outputs; single-reference, or one-pass rebasing
+ * (p.flags has AP_FLAG_REBASE; fractal types 0, 1, 4).  448 bytes. */
 typedef struct ApTileDesc {
     ApFrameParams p;
     const double* orbit_packed; /* ap_pack_orbit records of the tile's reference */

@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 PS, PMETA = load_golden("pert_samples.npz")
 
 
-def _tiles():
+def _tiles(rebase=False):
     m = {x["name"]: x for x in PMETA}
     out = []
     sizes = [(160, 90), (37, 23), (64, 64), (200, 50), (16, 16), (96, 54)]
@@ -31,7 +31,7 @@ def _tiles():
                            max_iter=min(c["max_iter"], 20000), fractal_type=c["fractal_type"],
                            julia_cx=c["julia_cx"], julia_cy=c["julia_cy"], gen_n=c["gen_n"],
                            gen_kr=c["gen_kr"], gen_ki=c["gen_ki"], bla=(q % 2 == 0),
-                           strict_glitch=False))
+                           strict_glitch=False, rebase=rebase and c["fractal_type"] in (0, 1, 4)))
     return out
 
 
@@ -43,7 +43,8 @@ def _engine_tile(t, arith, bla_form):
     engine.render_frame_ssaa(t.W, t.H, t.max_iter, t.cx, t.cy, t.width, None, color_scheme_id=0,
                              precision_mode="1e-300 (Perturbation)", fractal_type=t.fractal_type,
                              julia_cx=t.julia_cx, julia_cy=t.julia_cy, bbsa_tol=1e-6,
-                             bbsa_order=32 if t.bla else 0, glitch_mode="Off (Single-Ref)",
+                             bbsa_order=32 if t.bla else 0,
+                             glitch_mode="One-Pass Rebasing" if t.rebase else "Off (Single-Ref)",
                              gen_n=t.gen_n, gen_kr=t.gen_kr, gen_ki=t.gen_ki, h_iter_buf=it,
                              arith=arith, bla_form=bla_form, _extra_out=(kmap, s64))
     return it, kmap.cpu().numpy()
@@ -51,10 +52,13 @@ def _engine_tile(t, arith, bla_form):
 
 @pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda"])
 @pytest.mark.parametrize("bla_form", ["reference", "accurate"])
-def test_batch_matches_per_tile_frames(arith, bla_form):
+@pytest.mark.parametrize("rebase", [False, True])
+def test_batch_matches_per_tile_frames(arith, bla_form, rebase):
+    """Single-reference tiles, and one-pass rebasing tiles (Mandelbrot, Burning Ship,
+    Multibrot) mixed with single-reference Julia tiles."""
     import torch
     hp.clear_reference_orbit_cache()
-    tiles = _tiles()
+    tiles = _tiles(rebase)
     s = torch.cuda.Stream()
     b = fb.prepare_batch(tiles, arith=arith, bla_form=bla_form, stream=s)
     b.render(fb.BatchConfig())
@@ -67,11 +71,12 @@ def test_batch_matches_per_tile_frames(arith, bla_form):
     assert b.nominal_iterations() > 0
 
 
-def test_graph_replay_and_every_launch_shape_agree():
+@pytest.mark.parametrize("rebase", [False, True])
+def test_graph_replay_and_every_launch_shape_agree(rebase):
     import torch
     hp.clear_reference_orbit_cache()
     s = torch.cuda.Stream()
-    b = fb.prepare_batch(_tiles(), stream=s)
+    b = fb.prepare_batch(_tiles(rebase), stream=s)
     b.render(fb.BatchConfig())
     torch.cuda.synchronize()
     ref = [o["iter"].clone() for o in b.tiles_out]
@@ -90,7 +95,8 @@ def test_graph_replay_and_every_launch_shape_agree():
         torch.cuda.synchronize()
         for o, r in zip(b.tiles_out, ref):
             assert torch.equal(o["iter"], r)
-    cfg = fb.tune(b)
-    assert cfg in fb.CANDIDATES
-    assert len(fb.tuned_timings(b)) == len(fb.CANDIDATES)
-    assert fb.tune(b) is cfg   # cached
+    if not rebase:
+        cfg = fb.tune(b)
+        assert cfg in fb.CANDIDATES
+        assert len(fb.tuned_timings(b)) == len(fb.CANDIDATES)
+        assert fb.tune(b) is cfg   # cached
