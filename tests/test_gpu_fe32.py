@@ -3,10 +3,10 @@
 * Packing: the FP32 orbit copy holds each Z rounded to float and the close-approach
   marks; every BLA entry's (mantissa, exponent) pairs give back the FP64 coefficient to
   float precision; the radius rows are r^2 2^600.
-* Width 1e-1000 (config 3b, 1920x1080): every value of the reference's FloatExp frame
-  (fexp_samples.npz, the reference's FP64-mantissa FloatExp tier with BLA) is reproduced:
-  identical escape steps and smooth values within 1e-4 (the whole view escapes in a few
-  leaps, so 24-bit deltas carry it).
+* Width 1e-1000 (config 3b, 1920x1080): the FP64-mantissa FloatExp frame (same BLA
+  form) is reproduced: identical escape steps and smooth values within 1e-4 (the whole
+  view escapes in a few leaps, so 24-bit deltas carry it); the reference's own FloatExp
+  samples (fexp_samples.npz) agree on the escape step.
 * Width 1e-160 (config 3, 1920x1080): the error against the 700-bit ground truth stays at
   the level this form is documented at -- it cannot meet the 1e-4 bound there: the view's
   values need about 40 bits of delta precision (a one-ulp change of dc in float32 alone
