@@ -864,6 +864,25 @@ def batch_arm(args, wl, rank, world, local_rank, steps, headline):
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     barrier(world)
     e2e = iters * e2e_steps * world / e2e_s / 1e9
+    forms = {}
+    if rank == 0 and "One-Pass" in wl.get("glitch_mode", ""):
+        # the single-reference comparator: every tile on one reference with Pauldelbrot
+        # flags; pixels that outlive their tile's reference are flagged and iterated on
+        # directly in FP64 from the reference's end (values not to be trusted)
+        hp.clear_reference_orbit_cache()
+        sw = dict(wl, glitch_mode="Off (Single-Ref)")
+        b1 = fb.prepare_batch(batch_tiles(sw), arith=wl["arith"], bla_form=wl["bla_form"], stream=stream)
+        b1.render(cfg)
+        torch.cuda.synchronize()
+        ms1 = timed_loop(torch, stream, flush, max(3, steps // 5), lambda: b1.render(cfg))
+        it1 = b1.nominal_iterations()
+        glitched = sum(int(o["glitch"].count_nonzero().item()) for o in b1.tiles_out)
+        pixels = sum(t.W * t.H for t in b1.tiles)
+        forms["single_reference"] = {
+            "form": "every tile on one reference with Pauldelbrot flags, no rebasing",
+            "value": it1 / (float(np.median(ms1)) * 1e-3) / 1e9, "unit": "G iter/s",
+            "ms_per_batch": float(np.median(ms1)), "glitched_pixels": glitched,
+            "glitched_fraction": glitched / pixels}
     if rank != 0:
         return None
     flops = batch_flops(torch, _lib, b, cfg)
@@ -885,6 +904,7 @@ def batch_arm(args, wl, rank, world, local_rank, steps, headline):
         "e2e": {"value": e2e, "unit": "G iter/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
                 "path": "batch.prepare_batch (host orbits, device tables) + render + download of every tile"},
+        "forms": forms,
         "autotuner": {"chosen": vars(cfg) if hasattr(cfg, "__dict__") else repr(cfg),
                       "candidates_ms": [[round(ms, 4), repr(c)] for ms, c in fb.tuned_timings(b)]},
         "clocks": clocks.summary(),

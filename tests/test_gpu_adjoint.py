@@ -108,7 +108,7 @@ def test_forward_smooth_value_matches_oracle_fp64(name):
     direct sample (cpu_compute_fp64_sample restated, CUDA-source profile) at the same
     pixel c: the escape step is identical on >= 99.9 % of the pixels and, where it is,
     the smooth values agree to 1e-9 relative (the two differ only in which multiply-adds
-    are fused)."""
+    are fused, and for Multibrot in the reference's float32 1/ln n)."""
     import oracle
     from fractura_b200 import abi
     c = CASES[name]
@@ -128,4 +128,8 @@ def test_forward_smooth_value_matches_oracle_fp64(name):
     assert same.mean() >= 0.999, same.mean()
     esc = same & (k >= 0)
     assert esc.sum() > 1000
-    assert np.allclose(s[esc], s_o[esc], rtol=1e-9, atol=0)
+    # Multibrot: the reference rounds 1/ln n to float32 in its smooth term (the oracle too);
+    # the adjoint differentiates the smooth value with 1/ln n in float64, so the two differ
+    # by up to |nu| 2^-24 (nu <= 2 here) on top of the 1e-9 of differently fused steps
+    atol = 2.0 * 2.0 ** -24 if c["fractal_type"] == 4 else 0.0
+    assert np.allclose(s[esc], s_o[esc], rtol=1e-9, atol=atol)
