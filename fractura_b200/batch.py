@@ -48,6 +48,7 @@ class Tile:
     bla: bool = True           # chained-BLA leaps (Mandelbrot, Julia, Multibrot)
     strict_glitch: bool = True  # Pauldelbrot glitch flags
     rebase: bool = False       # one-pass rebasing (Mandelbrot, Burning Ship, Multibrot): no glitch flags
+    bla_tol: float = 1e-6      # merge tolerance of the reference's BLA table (bla_form "reference")
 
 
 @dataclass(frozen=True)
@@ -162,7 +163,7 @@ def _tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch):
                                          ACCURATE_BLA_EPS, float(dcm), BLA_LEVELS, int(t.gen_n),
                                          float(t.gen_kr), float(t.gen_ki), _ptr(table), s), "ap_build_bla_dc")
         else:
-            _lib.check(L.ap_build_bla(_ptr(d_re), _ptr(d_im), int(rl), int(t.fractal_type), 1e-6,
+            _lib.check(L.ap_build_bla(_ptr(d_re), _ptr(d_im), int(rl), int(t.fractal_type), float(t.bla_tol),
                                       BLA_LEVELS, int(t.gen_n), float(t.gen_kr), float(t.gen_ki),
                                       _ptr(table), s), "ap_build_bla")
         bla_packed = torch.empty(80 * rl, dtype=torch.float64, device="cuda")

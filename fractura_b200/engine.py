@@ -425,9 +425,9 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
                 fp32_deltas=(delta_form == "fp32"),
                 bla_eps=ACCURATE_BLA_EPS if bla_form == "accurate" else None, rows=_rows, orbit=_orbit)
 
-        out = _copy_to_host(fr.rgb, h_rgb_buf, st)
+        out = _copy_to_host(fr.rgb, h_rgb_buf, st, non_blocking=not sync_stream)
         if h_iter_buf is not None:
-            _copy_to_host(fr.iter, h_iter_buf, st)
+            _copy_to_host(fr.iter, h_iter_buf, st, non_blocking=not sync_stream)
     if sync_stream:
         st.synchronize()
     return out
@@ -524,8 +524,10 @@ def eval_glitched_pixels_fallback_cuda(d_out_rgb, d_glitch_out, d_lut, glitched_
         st.synchronize()
 
 
-def _copy_to_host(dev, host, st):
-    """Device -> host copy on stream ``st`` into ``host`` (or a new array)."""
+def _copy_to_host(dev, host, st, non_blocking=False):
+    """Device -> host copy on stream ``st`` into ``host`` (or a new array).  With
+    non_blocking and a pinned ``host`` the copy is only queued on ``st``; the caller
+    synchronises the stream before reading it (sync_stream=False)."""
     torch = _torch()
     np_dt = {torch.uint8: np.uint8, torch.uint16: np.uint16, torch.float32: np.float32}[dev.dtype]
     if host is None or tuple(host.shape) != tuple(dev.shape) or host.dtype != np_dt:
@@ -536,7 +538,7 @@ def _copy_to_host(dev, host, st):
         host[...] = tmp
         return host
     with torch.cuda.stream(st):
-        ht.copy_(dev, non_blocking=False)
+        ht.copy_(dev, non_blocking=bool(non_blocking) and ht.is_pinned())
     return host
 
 
