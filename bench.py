@@ -153,14 +153,15 @@ def workload_cfg4():
     if not tiles:
         raise SystemExit("workloads.json holds no config4_tiles (python tests/golden/make_golden.py config4)")
     return dict(name="batch64_mixed_formulas_w1e-60_1e-12", kind="batch", tiles=tiles,
-                arith="ref_cuda", bla_form="accurate", dtype="f64", W=0, H=0, factor=1,
+                arith="fast", bla_form="accurate", dtype="f64", W=0, H=0, factor=1,
                 max_iter=max(t["max_iter"] for t in tiles), width="1e-60..1e-12",
                 bbsa_order=32, glitch_mode="One-Pass Rebasing", precision_mode="1e-300 (Perturbation)",
                 scheme=0, fractal_type=-1,
-                form="one persistent work-stealing kernel over 64 tiles (FP64 deltas, dc-aware "
-                     "chained BLA, one reference per tile: one-pass rebasing for the Mandelbrot, "
-                     "Burning Ship and Multibrot tiles, Pauldelbrot flags for the Julia tiles), "
-                     "CUDA-graph replay, autotuned launch shape")
+                form="one persistent work-stealing kernel over 64 tiles, the unfinished pixels of "
+                     "each block compacted between quanta (FP64 deltas, dc-aware chained BLA, one "
+                     "reference per tile: one-pass rebasing with the fused step for the Mandelbrot, "
+                     "Burning Ship and Multibrot tiles, Pauldelbrot flags in the CUDA-source "
+                     "profile for the Julia tiles), CUDA-graph replay, autotuned launch shape")
 
 
 def workload_cfg5():
@@ -544,6 +545,7 @@ def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla, direct_flop
     f1 = 18.0 + (4.0 if strict else 0.0) + (3.0 if has_bla else 0.0)
     total = 0.0
     launches = 0
+    work = np.zeros(4, np.int64)  # steps, leaps, stage-2 steps, rebases (one-pass)
     with torch.cuda.stream(stream):
         for fn, args, what in ops:
             if args is None:
@@ -556,6 +558,7 @@ def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla, direct_flop
                 q.counters = C.c_void_p(counters.data_ptr())
                 _lib.check(fn(args[0], C.byref(q), args[2]), what)
                 c = counters.view(-1, 4).sum(dim=0, dtype=torch.int64).cpu().numpy()
+                work += c.astype(np.int64)
                 p = args[0]._obj
                 if p.tier in (abi.AP_TIER_FP64, abi.AP_TIER_DD):
                     total += direct_flops * float(c[0])
@@ -570,7 +573,7 @@ def pass_flops(torch, _lib, abi, ops, stream, H, W, strict, has_bla, direct_flop
             else:
                 _lib.check(fn(*args), what)
     torch.cuda.synchronize()
-    return total, launches
+    return total, launches, work
 
 
 def truth_errors(kmap, s64):
@@ -742,8 +745,14 @@ def frame_arm(args, wl, rank, world, local_rank, steps, headline):
         line["forms"] = {"fp32_floatexp": s}
 
     strict = "Pauldelbrot" in wl["glitch_mode"] or "Strict" in wl["glitch_mode"]
-    flops, n_pass = pass_flops(torch, _lib, abi, chosen.ops, stream, H, W, strict, wl["bbsa_order"] == 32,
-                               wl.get("flops_per_iter", FLOPS_DIRECT))
+    flops, n_pass, work = pass_flops(torch, _lib, abi, chosen.ops, stream, H, W, strict,
+                                     wl["bbsa_order"] == 32, wl.get("flops_per_iter", FLOPS_DIRECT))
+    if perturb:
+        # what the render passes executed per frame (work counters): steps taken one at a
+        # time, BLA leaps, direct stage-2 steps, one-pass restarts
+        line["work_per_frame"] = {"steps": int(work[0]), "leaps": int(work[1]), "stage2_steps": int(work[2]),
+                                  "rebases": int(work[3]),
+                                  "nominal_iterations": line.get("nominal_iterations_per_frame")}
     pass_ms = float(np.sum([a.elapsed_time(b) for a, b in pass_ev])) / steps
     peak64 = fma_peak_tflops(64, torch)
     achieved = flops / (pass_ms * 1e-3) / 1e12 if pass_ms > 0 else None
@@ -871,7 +880,8 @@ def batch_arm(args, wl, rank, world, local_rank, steps, headline):
         # directly in FP64 from the reference's end (values not to be trusted)
         hp.clear_reference_orbit_cache()
         sw = dict(wl, glitch_mode="Off (Single-Ref)")
-        b1 = fb.prepare_batch(batch_tiles(sw), arith=wl["arith"], bla_form=wl["bla_form"], stream=stream)
+        b1 = fb.prepare_batch(batch_tiles(sw), arith="ref_cuda" if wl["arith"] == "fast" else wl["arith"],
+                              bla_form=wl["bla_form"], stream=stream)
         b1.render(cfg)
         torch.cuda.synchronize()
         ms1 = timed_loop(torch, stream, flush, max(3, steps // 5), lambda: b1.render(cfg))
@@ -1055,7 +1065,7 @@ def cpu_budget(wl, headline):
 SUB_KEYS = ("metric", "value", "unit", "steps", "ms_per_step", "config", "form", "arith", "bla_form",
             "roofline", "e2e", "cpu_baseline", "forms", "clocks", "gpu_launches", "kernel_ms",
             "flops_per_step", "autotuner", "nominal_iterations_per_frame", "nominal_iterations_per_batch",
-            "nominal_iterations_per_step", "rebase_passes")
+            "nominal_iterations_per_step", "rebase_passes", "work_per_frame")
 
 
 def main():

@@ -74,7 +74,7 @@ def load():
     L.ap_smooth_adjoint_blocks.restype = i32
     L.ap_smooth_adjoint.argtypes = [vp, vp, vp, vp, i32, vp, vp, vp]
     L.ap_smooth_tangent.argtypes = [vp, vp, vp]
-    L.ap_render_batch.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, vp, vp]
+    L.ap_render_batch.argtypes = [vp, vp, i32, i32, i32, i32, i32, i32, i32, vp, vp]
     L.ap_fma_peak_launch.argtypes = [i32, i32, i32, vp, C.POINTER(C.c_double), vp]
     L.ap_histogram_cdf_noalloc.argtypes = [vp, i32, i32, i32, i32, vp, vp]
     L.ap_launch_counter.restype = C.c_uint64

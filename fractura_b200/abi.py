@@ -5,7 +5,7 @@ compares the sizes against the library's own ``sizeof`` report.
 """
 import ctypes as C
 
-AP_ABI_VERSION = 6
+AP_ABI_VERSION = 7
 
 AP_OK = 0
 AP_E_INVALID = -1

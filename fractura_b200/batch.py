@@ -4,9 +4,11 @@ The reference renders tiles one call at a time (its mosaic exporter,
 workers/image_workers.py:428-601, calls render_frame_ssaa per tile).  Here a
 batch of tiles of any size, formula and max_iter is prepared on the host
 (reference orbit, device BLA table, packed inputs, one descriptor per tile) and
-rendered by a single persistent kernel whose blocks take 256-pixel patches from
-a shared counter.  Each tile's values equal the per-frame coarse pass
-(ap_render_pass) for the same parameters.
+rendered by a single persistent kernel whose blocks take consecutive pixels from
+a shared counter, run them a quantum of loop steps at a time and compact the
+unfinished ones between quanta.  Each tile's values equal the per-frame coarse
+pass (ap_render_pass) for the same parameters.  arith="fast" gives one-pass tiles
+the fused step (the batch's single-reference tiles run "ref_cuda").
 
     tiles = [Tile(cx, cy, width, W, H, max_iter, fractal_type=...), ...]
     batch = prepare_batch(tiles)            # orbits, tables, descriptors
@@ -54,16 +56,19 @@ class Tile:
 @dataclass(frozen=True)
 class BatchConfig:
     """Launch shape of the persistent kernel: patch_w x patch_h = 256 pixels per work
-    item, blocks_per_sm resident blocks, min_blocks = the register budget (4 or 6)."""
+    item, blocks_per_sm resident blocks, min_blocks = the register budget (4 or 6),
+    quantum = loop steps per pixel between two compactions of a block's pixels."""
     patch_w: int = 16
     patch_h: int = 16
     blocks_per_sm: int = 4
     min_blocks: int = 4
+    quantum: int = 64
 
 
-CANDIDATES = tuple(BatchConfig(pw, 256 // pw, bps, mb)
-                   for pw in (16, 32, 64, 8)
-                   for (bps, mb) in ((4, 4), (8, 4), (6, 6)))
+CANDIDATES = tuple(BatchConfig(pw, 256 // pw, bps, mb, qu)
+                   for pw in (16, 32, 8)
+                   for (bps, mb) in ((4, 4), (6, 6))
+                   for qu in (64, 128))
 
 
 def _ptr(t):
@@ -106,7 +111,7 @@ class PreparedBatch:
         L = _lib.load()
         with torch.cuda.stream(self.stream):
             _lib.launch(L.ap_render_batch, _ptr(self.desc_dev), _ptr(first), self.n, self.arith,
-                        cfg.patch_w, cfg.patch_h, cfg.blocks_per_sm, cfg.min_blocks,
+                        cfg.patch_w, cfg.patch_h, cfg.blocks_per_sm, cfg.min_blocks, cfg.quantum,
                         _ptr(self.head), C.c_void_p(self.stream.cuda_stream), what="ap_render_batch")
 
     def capture(self, cfg=BatchConfig()):
@@ -122,7 +127,7 @@ class PreparedBatch:
             L = _lib.load()
             _lib.check(L.ap_render_batch(_ptr(self.desc_dev), _ptr(first), self.n, self.arith,
                                          cfg.patch_w, cfg.patch_h, cfg.blocks_per_sm, cfg.min_blocks,
-                                         _ptr(self.head), C.c_void_p(self.stream.cuda_stream)),
+                                         cfg.quantum, _ptr(self.head), C.c_void_p(self.stream.cuda_stream)),
                        "ap_render_batch")
         return g
 
@@ -135,11 +140,12 @@ class PreparedBatch:
         return tot
 
 
-def _tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch):
+def _tile_inputs(t, ref, arith, bla_form, torch, stream, L, scratch):
     """Packed records, BLA rows, outputs and parameters of one tile around its
     reference `ref` (find_optimal_reference_orbit's result), as the coarse pass of
     render_perturbation_frame sets them (factor 1, one reference)."""
     from .perturbation import max_delta_c
+    cpu_sem = arith == "ref_cpu"
     pw = Decimal(t.width)
     with localcontext(decimal_context(pw)):
         ph = pw * (Decimal(t.H) / Decimal(t.W))
@@ -179,7 +185,8 @@ def _tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch):
         flags |= abi.AP_FLAG_REBASE
     p = abi.new_params(width=t.W, height=t.H, factor=1, max_iter=int(t.max_iter),
                        fractal_type=int(t.fractal_type), tier=abi.AP_TIER_PERTURB,
-                       arith=abi.AP_ARITH_REF_CPU if cpu_sem else abi.AP_ARITH_REF_CUDA,
+                       arith=(abi.AP_ARITH_REF_CPU if cpu_sem else
+                              abi.AP_ARITH_FAST if (arith == "fast" and rebase) else abi.AP_ARITH_REF_CUDA),
                        mode=abi.AP_MODE_COARSE, flags=flags, gen_n=int(t.gen_n),
                        gen_kr=float(t.gen_kr), gen_ki=float(t.gen_ki), dx_hi=dx, dy_hi=dy,
                        ref_px=ref_px, ref_py=ref_py, ref_cx=float(bcx), ref_cy=float(bcy),
@@ -199,14 +206,15 @@ def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, wor
     import torch
     if bla_form not in ("reference", "accurate"):
         raise ValueError("bla_form must be 'reference' or 'accurate'")
-    cpu_sem = arith == "ref_cpu"
-    if arith not in ("ref_cpu", "ref_cuda"):
-        raise ValueError("arith must be 'ref_cpu' or 'ref_cuda'")
+    if arith not in ("ref_cpu", "ref_cuda", "fast"):
+        raise ValueError("arith must be 'ref_cpu', 'ref_cuda' or 'fast' (the fused step of one-pass tiles; "
+                         "the batch's single-reference tiles then run 'ref_cuda')")
     if not tiles:
         raise ValueError("a batch needs at least one tile")
     L = _lib.load()
     stream = stream or torch.cuda.current_stream()
-    b = PreparedBatch(list(tiles), abi.AP_ARITH_REF_CPU if cpu_sem else abi.AP_ARITH_REF_CUDA, stream)
+    b = PreparedBatch(list(tiles), {"ref_cpu": abi.AP_ARITH_REF_CPU, "ref_cuda": abi.AP_ARITH_REF_CUDA,
+                                    "fast": abi.AP_ARITH_FAST}[arith], stream)
     # the orbits first, concurrently (host work), each once: a batch can hold more
     # tiles than the orbit cache keeps
     with ThreadPoolExecutor(max_workers=max(1, workers or os.cpu_count() or 8)) as ex:
@@ -224,7 +232,7 @@ def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, wor
     recs = []
     with torch.cuda.stream(stream):
         for t, ref in zip(b.tiles, refs):
-            recs.append(_tile_inputs(t, ref, cpu_sem, bla_form, torch, stream, L, scratch))
+            recs.append(_tile_inputs(t, ref, arith, bla_form, torch, stream, L, scratch))
     stream.synchronize()
     cost = [t.W * t.H * max(1, r[5]) for t, r in zip(b.tiles, recs)]
     b.order = sorted(range(len(b.tiles)), key=lambda q: -cost[q])

@@ -327,14 +327,18 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
     const double4* __restrict__ AB = reinterpret_cast<const double4*>(b.bla_packed + (size_t)ref_len * 16);
     const int max_level = p.bla_levels - 1;
     const double dcpx = s.dcx, dcpy = s.dcy;
-    int k = s.k, m = s.m, glitch = s.glitch, leaps = s.leaps, skipped = s.skipped, rebases = s.rebases;
+    // k (the pixel's iterations) is not kept: a step or a leap moves k and m alike and a
+    // restart moves only m, so k = m + (max_iter - lim) with lim moved at each restart,
+    // and the loop runs while m < lim (k < max_iter).
+    int m = s.m, lim = max_iter - s.k + s.m;
+    int glitch = s.glitch, leaps = s.leaps, skipped = s.skipped, rebases = s.rebases;
     double dzx = s.dzx, dzy = s.dzy;
     SampleOut o = s.o;
     bool paused = false;
 #if AP_REBASE_PREFETCH
     double4 Znext = ldg4(orb + m);
 #endif
-    while (k < max_iter) {
+    while (m < lim) {
         if (BUDGET && --budget < 0) {
             paused = true;
             break;
@@ -368,6 +372,7 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                 }
                 const double mag2 = kFast ? fma(zx, zx, zy * zy) : zx * zx + zy * zy;
                 if (!(mag2 <= kBailout)) {
+                    const int k = m + (max_iter - lim);
                     if (isnan(mag2)) {
                         o = interior_sample();
                         o.s = (float)k;
@@ -383,6 +388,7 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                 if (mag2 < dz_mag2 || (m == ref_len && m > 0)) {
                     dzx = zx;
                     dzy = zy;
+                    lim -= m;
                     m = 0;
                     ++rebases;
 #if AP_REBASE_PREFETCH
@@ -395,7 +401,7 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                 const double* row = R + (size_t)m * 16;
                 int hi = max_level;
                 if (dz_mag2 == 0.0 && (dzx != 0.0 || dzy != 0.0)) hi = min(hi, 8);
-                hi = min(hi, 31 - __clz(max_iter - k));  // k + 2^lo <= max_iter
+                hi = min(hi, 31 - __clz(lim - m));  // k + 2^lo <= max_iter
                 int q = 0;
 #pragma unroll
                 for (int t = 1; t <= 3; ++t)
@@ -418,6 +424,7 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                 dzx = nx;
                 dzy = ny;
                 if (isnan(dzx) || isnan(dzy) || isinf(dzx) || isinf(dzy)) {
+                    const int k = m + (max_iter - lim);
                     o = interior_sample();
                     o.s = (float)k;
                     o.s64 = (double)k;
@@ -427,7 +434,6 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                     break;
                 }
                 m += 1 << lo;
-                k += 1 << lo;
                 ++leaps;
                 skipped += 1 << lo;
 #if AP_REBASE_PREFETCH
@@ -476,12 +482,11 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
             dzy = pi + kzi + dcpy;
         }
         ++m;
-        ++k;
     }
     if (!paused) s.stage = 3;
     s.dzx = dzx;
     s.dzy = dzy;
-    s.k = k;
+    s.k = m + (max_iter - lim);
     s.m = m;
     s.glitch = glitch;
     s.leaps = leaps;

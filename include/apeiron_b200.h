@@ -26,7 +26,7 @@ extern "C" {
 #define AP_API
 #endif
 
-#define AP_ABI_VERSION 6
+#define AP_ABI_VERSION 7
 
 /* Return codes. */
 #define AP_OK 0
@@ -389,17 +389,20 @@ AP_API int ap_decimal_arith(int32_t op, const int64_t* a_meta, const uint64_t* a
  * the number of each tile's first 256-pixel patch (patch_w x patch_h == 256) and the total;
  * tiles should come in decreasing order of expected cost.
  * ap_render_batch: renders all tiles with one persistent kernel of blocks_per_sm blocks per
- * SM whose lanes take pixels from a shared counter (device word *queue_head, reset here):
- * each lane keeps one pixel, runs it 128 steps at a time, and a warp with 16 or more idle
- * lanes refills them with consecutive pixels;
+ * SM that take pixels from a shared counter (device word *queue_head, reset here).  A block
+ * works in rounds: each thread runs one pixel for `quantum` loop steps; the unfinished
+ * pixels are compacted into the block's first slots (shared memory) and the slots left
+ * over take the next consecutive pixels of the queue with one atomicAdd.
  * tiles and first_patch are device copies of the planned arrays.  min_blocks (4 or 6) picks
- * the register budget the kernel is compiled for; arith is the tiles' common profile.
- * Values equal ap_render_pass's for each tile. */
+ * the register budget the kernel is compiled for; arith is the tiles' common profile
+ * (AP_ARITH_FAST when the plan holds AP_ARITH_FAST tiles: one-pass tiles only, the others
+ * then carry AP_ARITH_REF_CUDA).  Values equal ap_render_pass's for each tile. */
 AP_API int ap_batch_plan(const ApTileDesc* host_tiles, int32_t n, int32_t patch_w, int32_t patch_h,
                          int64_t* first_patch);
 AP_API int ap_render_batch(const ApTileDesc* tiles, const int64_t* first_patch, int32_t n,
                            int32_t arith, int32_t patch_w, int32_t patch_h, int32_t blocks_per_sm,
-                           int32_t min_blocks, unsigned long long* queue_head, void* stream);
+                           int32_t min_blocks, int32_t quantum, unsigned long long* queue_head,
+                           void* stream);
 
 /* Derivatives of the smooth escape value (no counterpart in the reference).
  * theta = (cx, cy, ln w, Re P, Im P).

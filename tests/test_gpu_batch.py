@@ -2,8 +2,9 @@
 
 Every tile of a mixed batch (formulas, sizes, depths) equals the per-tile
 coarse render of the engine, value for value; a captured CUDA graph replays
-to the same values; every launch shape the autotuner may pick gives the same
-values.
+to the same values; every launch shape the autotuner may pick (patch shape,
+blocks per SM, register budget, quantum) gives the same values, and so does a
+quantum of one step, where every pixel is compacted after every step.
 """
 from decimal import Decimal
 
@@ -50,12 +51,13 @@ def _engine_tile(t, arith, bla_form):
     return it, kmap.cpu().numpy()
 
 
-@pytest.mark.parametrize("arith", ["ref_cpu", "ref_cuda"])
+@pytest.mark.parametrize("arith,rebase", [("ref_cpu", False), ("ref_cuda", False), ("ref_cpu", True),
+                                          ("ref_cuda", True), ("fast", True)])
 @pytest.mark.parametrize("bla_form", ["reference", "accurate"])
-@pytest.mark.parametrize("rebase", [False, True])
 def test_batch_matches_per_tile_frames(arith, bla_form, rebase):
     """Single-reference tiles, and one-pass rebasing tiles (Mandelbrot, Burning Ship,
-    Multibrot) mixed with single-reference Julia tiles."""
+    Multibrot) mixed with single-reference Julia tiles; in a 'fast' batch the one-pass
+    tiles take the fused step and the Julia tiles the CUDA-source profile."""
     import torch
     hp.clear_reference_orbit_cache()
     tiles = _tiles(rebase)
@@ -64,7 +66,7 @@ def test_batch_matches_per_tile_frames(arith, bla_form, rebase):
     b.render(fb.BatchConfig())
     torch.cuda.synchronize()
     for t, out in zip(tiles, b.tiles_out):
-        it, k = _engine_tile(t, arith, bla_form)
+        it, k = _engine_tile(t, "ref_cuda" if (arith == "fast" and not t.rebase) else arith, bla_form)
         got = out["iter"].cpu().numpy()
         assert np.array_equal(got.view(np.uint32), it.view(np.uint32)), int((got != it).sum())
         assert np.array_equal(out["kmap"].cpu().numpy(), k)
@@ -76,11 +78,18 @@ def test_graph_replay_and_every_launch_shape_agree(rebase):
     import torch
     hp.clear_reference_orbit_cache()
     s = torch.cuda.Stream()
-    b = fb.prepare_batch(_tiles(rebase), stream=s)
+    b = fb.prepare_batch(_tiles(rebase), arith="fast" if rebase else "ref_cpu", stream=s)
     b.render(fb.BatchConfig())
     torch.cuda.synchronize()
     ref = [o["iter"].clone() for o in b.tiles_out]
     for cfg in fb.CANDIDATES:
+        for o in b.tiles_out:
+            o["iter"].fill_(-7.0)
+        b.render(cfg)
+        torch.cuda.synchronize()
+        for o, r in zip(b.tiles_out, ref):
+            assert torch.equal(o["iter"], r), cfg
+    for cfg in (fb.BatchConfig(quantum=1), fb.BatchConfig(quantum=7, blocks_per_sm=1)):
         for o in b.tiles_out:
             o["iter"].fill_(-7.0)
         b.render(cfg)
