@@ -313,8 +313,9 @@ __device__ __forceinline__ void pixel_advance(const ApFrameParams& p, const ApFr
 // iteration, so one pass serves every pixel.  The packed safe radius also rules
 // out the rebase test (|dz| < |Z|/2), so the common path is the same single branch
 // as pixel_advance's.  Leaps are capped so that k never passes max_iter.  ARITH may
-// also be AP_ARITH_FAST: |dz|^2, |z|^2 and the Mandelbrot step as fused multiply-adds
-// (about 10 FP64 instructions per step on the common path), leaps as the CUDA profile.
+// also be AP_ARITH_FAST: |dz|^2, |z|^2 and every formula's step as fused multiply-adds
+// (about 10 FP64 instructions per Mandelbrot step on the common path; a Multibrot
+// power costs 14 instead of 22), leaps as the CUDA profile.
 template <int ARITH, int FT, bool BLA, bool BUDGET>
 __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApFrameBuffers& b, PixelRun& s,
                                                int budget) {
@@ -458,12 +459,38 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
             dzx = nx;
             dzy = ny;
         } else if (FT == kFtShip) {
-            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
             const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
-            const double ddx = zx * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
-            const double ddy = zy * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
-            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcpy;
-            dzx = nx;
+            if (kFast) {  // 2Z + dz rounded once (2Z is exact); products fused into the sums
+                const double ax = fma(2.0, rx, dzx), ay = fma(2.0, ry, dzy);
+                const double nx = fma(ax, dzx, fma(-ay, dzy, dcpx));
+                const double ddx = zx * sx >= 0.0 ? sx * dzx : -sx * ax;
+                const double ddy = zy * sy >= 0.0 ? sy * dzy : -sy * ay;
+                dzy = fma(2.0, fma(fabs(rx), ddy, fma(fabs(ry), ddx, ddx * ddy)), -dcpy);
+                dzx = nx;
+            } else {
+                const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcpx;
+                const double ddx = zx * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+                const double ddy = zy * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+                dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcpy;
+                dzx = nx;
+            }
+        } else if (kFast) {
+            // (Z + dz)^n - Z^n by P_{j+1} = P_j Z + (P_j + Z^j) dz, each complex product
+            // sum as one chain of fused multiply-adds, then + k dz + dc
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p.gen_n - 1; ++t) {
+                const double sr = pr + qr, si = pi + qi;
+                const double npr = fma(pr, rx, fma(-pi, ry, fma(sr, dzx, -si * dzy)));
+                const double npi = fma(pr, ry, fma(pi, rx, fma(sr, dzy, si * dzx)));
+                const double nqr = fma(qr, rx, -qi * ry), nqi = fma(qr, ry, qi * rx);
+                pr = npr;
+                pi = npi;
+                qr = nqr;
+                qi = nqi;
+            }
+            const double ox = dzx, oy = dzy;
+            dzx = fma(p.gen_kr, ox, fma(-p.gen_ki, oy, pr + dcpx));
+            dzy = fma(p.gen_kr, oy, fma(p.gen_ki, ox, pi + dcpy));
         } else {
             double pr = dzx, pi = dzy, qr = rx, qi = ry;
             for (int t = 0; t < p.gen_n - 1; ++t) {

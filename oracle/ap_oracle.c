@@ -798,8 +798,9 @@ static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, do
 /*   and |dz|^2 < r_d^2 (levels 0..8 only for an underflowed |dz|^2);         */
 /*   else one perturbation step.  Interior after max_iter.                    */
 /*   AP_ARITH_FAST (this form only): |dz|^2, |z|^2 as fma(x, x, y*y); the     */
-/*   Mandelbrot step a = fma(2, Z, dz), dz' = fma(a, dz, ...) + dc fused;       */
-/*   leaps in the CUDA profile's form.                                        */
+/*   Mandelbrot step a = fma(2, Z, dz), dz' = fma(a, dz, ...) + dc fused; the  */
+/*   Burning Ship and Multibrot steps with their products fused into the sums */
+/*   (as written below); leaps in the CUDA profile's form.                    */
 /* ------------------------------------------------------------------------- */
 static int floor_log2(int v) {
     int r = 0;
@@ -890,12 +891,38 @@ static Sample rebase_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, 
             dzx = nx;
             dzy = ny;
         } else if (ft == 1) {
-            const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
             const double sx = rx >= 0.0 ? 1.0 : -1.0, sy = ry >= 0.0 ? 1.0 : -1.0;
-            const double ddx = (rx + dzx) * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
-            const double ddy = (ry + dzy) * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
-            dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcy;
-            dzx = nx;
+            if (fast) { /* 2Z + dz rounded once; products fused into the sums */
+                const double ax = fma(2.0, rx, dzx), ay = fma(2.0, ry, dzy);
+                const double nx = fma(ax, dzx, fma(-ay, dzy, dcx));
+                const double ddx = (rx + dzx) * sx >= 0.0 ? sx * dzx : -sx * ax;
+                const double ddy = (ry + dzy) * sy >= 0.0 ? sy * dzy : -sy * ay;
+                dzy = fma(2.0, fma(fabs(rx), ddy, fma(fabs(ry), ddx, ddx * ddy)), -dcy);
+                dzx = nx;
+            } else {
+                const double nx = (2.0 * rx + dzx) * dzx - (2.0 * ry + dzy) * dzy + dcx;
+                const double ddx = (rx + dzx) * sx >= 0.0 ? sx * dzx : -sx * (2.0 * rx + dzx);
+                const double ddy = (ry + dzy) * sy >= 0.0 ? sy * dzy : -sy * (2.0 * ry + dzy);
+                dzy = 2.0 * (fabs(rx) * ddy + fabs(ry) * ddx + ddx * ddy) - dcy;
+                dzx = nx;
+            }
+        } else if (fast) {
+            /* (Z + dz)^n - Z^n by P_{j+1} = P_j Z + (P_j + Z^j) dz, each complex product
+               sum as one chain of fused multiply-adds, then + k dz + dc */
+            double pr = dzx, pi = dzy, qr = rx, qi = ry;
+            for (int t = 0; t < p->gen_n - 1; t++) {
+                const double sr = pr + qr, si = pi + qi;
+                const double npr = fma(pr, rx, fma(-pi, ry, fma(sr, dzx, -si * dzy)));
+                const double npi = fma(pr, ry, fma(pi, rx, fma(sr, dzy, si * dzx)));
+                const double nqr = fma(qr, rx, -qi * ry), nqi = fma(qr, ry, qi * rx);
+                pr = npr;
+                pi = npi;
+                qr = nqr;
+                qi = nqi;
+            }
+            const double ox = dzx, oy = dzy;
+            dzx = fma(p->gen_kr, ox, fma(-p->gen_ki, oy, pr + dcx));
+            dzy = fma(p->gen_kr, oy, fma(p->gen_ki, ox, pi + dcy));
         } else {
             double pr = dzx, pi = dzy, qr = rx, qi = ry;
             for (int t = 0; t < p->gen_n - 1; t++) {
