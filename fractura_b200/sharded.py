@@ -22,7 +22,11 @@ whole frame's glitch map on one host.  Rows are balanced by a per-row cost estim
 (uniform unless given).
 
 shard_tiles() shares a batch of tiles out by estimated cost (longest processing time
-first), for ranks that each run the persistent batch kernel on their own tiles.
+first), for ranks that each run the persistent batch kernel on their own tiles.  Costs
+come from pixels x max_iter (tile_cost) or from a small probe of each tile
+(probe_tile_costs); a frame's bands can follow a probe of the frame (balance="probe"):
+the probe is the adaptive max-iter probe's pass (math_core/engine.py:1063-1281), and a
+pixel's cost is its escape step (max_iter when it stays bounded).
 
 The steps of a split frame go through a backend object -- find_reference, render_band,
 band_histogram, cdf_from_histogram, colour_band -- so the same orchestration drives the
@@ -81,6 +85,44 @@ def tile_cost(tile):
     return float(tile.W) * float(tile.H) * float(tile.max_iter)
 
 
+# ------------------------------------------------------------------ probe-estimated costs
+def costs_from_probe(iters, max_iter):
+    """Per-pixel cost estimate from a probe's smooth values: the escape step, or
+    max_iter for a pixel that stays bounded (value < 0)."""
+    it = np.asarray(iters, np.float64)
+    return np.where(it < 0.0, float(max_iter), np.maximum(it, 1.0))
+
+
+def row_weights(probe_costs, H):
+    """Per-row costs of an H-row frame from a probe's [h, w] cost map of the same view
+    (probe row q samples frame row q (H - 1) / (h - 1)): each frame row takes the cost
+    of the probe row nearest to it."""
+    pc = np.asarray(probe_costs, np.float64)
+    h = pc.shape[0]
+    per_row = pc.sum(axis=1)
+    if h == 1 or H == 1:
+        return np.full(int(H), per_row.mean())
+    q = np.rint(np.arange(int(H), dtype=np.float64) * (h - 1) / (H - 1)).astype(np.int64)
+    return per_row[q]
+
+
+def probe_row_weights(view, probe, probe_w=128, probe_h=72):
+    """Row costs of a view for band_bounds, from probe(view, probe_w, probe_h) -> the
+    probe's smooth values [probe_h, probe_w] (a DeviceBackend's probe_map: the adaptive
+    max-iter probe's pass, math_core/engine.py:1063-1281, at the view's max_iter)."""
+    return row_weights(costs_from_probe(probe(view, probe_w, probe_h), view["max_iter"]), view["H"])
+
+
+def probe_tile_costs(tiles, probe, probe_w=32, probe_h=32):
+    """Estimated cost of each tile: its probe's mean per-pixel cost x its pixels, with
+    probe(tile, probe_w, probe_h) -> smooth values (a DeviceBackend's probe_tile)."""
+    out = []
+    for t in tiles:
+        c = costs_from_probe(probe(t, probe_w, probe_h), t.max_iter)
+        out.append(float(c.mean()) * float(t.W) * float(t.H))
+    return out
+
+
 # ------------------------------------------------------------------ collectives
 def _group_info(group):
     import torch.distributed as dist
@@ -122,13 +164,22 @@ def gather_bands(band, bands, group=None):
     return torch.cat([parts[q][:bands[q][1] - bands[q][0]] for q in range(world)], dim=0)
 
 
-def render_split(view, backend, group=None, weights=None):
+def render_split(view, backend, group=None, weights=None, balance=None):
     """One frame (a view dict: W, H, max_iter, cx, cy, width, scheme, num_bins, ...) split
     over the ranks of `group` by row bands.  Returns (rgb, iteration map) of the whole
-    frame on every rank, as tensors on the backend's device."""
+    frame on every rank, as tensors on the backend's device.  Bands are even, or follow
+    the per-row `weights`, or with balance="probe" rank 0's probe of the view
+    (backend.probe_map, broadcast with the reference)."""
+    import torch.distributed as dist
     rank, world = _group_info(group)
-    bands = band_bounds(view["H"], world, weights)
     orbit = backend.find_reference(view) if rank == 0 else None
+    if balance == "probe":
+        box = [probe_row_weights(view, backend.probe_map) if rank == 0 else None]
+        dist.broadcast_object_list(box, src=0, group=group)
+        weights = box[0]
+    elif balance is not None:
+        raise ValueError("balance must be None or 'probe'")
+    bands = band_bounds(view["H"], world, weights)
     orbit = broadcast_reference(orbit, group)
     r0, r1 = bands[rank]
     it_band = backend.render_band(view, orbit, r0, r1)
@@ -179,6 +230,25 @@ class DeviceBackend:
             stream=self.stream, arith=view.get("arith"), bla_form=view.get("bla_form"), d_iter_buf=it,
             sync_stream=False, _rows=(r0, r1), _orbit=orbit)
         return it[r0:r1]
+
+    def probe_map(self, view, probe_w, probe_h):
+        """The view's probe (engine.probe_iter_map at the view's max_iter)."""
+        from . import engine
+        return engine.probe_iter_map(Decimal(view["cx"]), Decimal(view["cy"]), Decimal(view["width"]),
+                                     int(view["max_iter"]), probe_w, probe_h,
+                                     fractal_type=view.get("fractal_type", 0), gen_n=view.get("gen_n", 3),
+                                     gen_kr=view.get("gen_kr", 0.25), gen_ki=view.get("gen_ki", 1.0),
+                                     precision_mode=view.get("precision_mode", "1e-300 (Perturbation)"),
+                                     bbsa_order=0, stream=self.stream)
+
+    @staticmethod
+    def probe_tile(tile, probe_w, probe_h):
+        """A batch tile's probe (engine.probe_iter_map at the tile's max_iter)."""
+        from . import engine
+        return engine.probe_iter_map(Decimal(tile.cx), Decimal(tile.cy), Decimal(tile.width), int(tile.max_iter),
+                                     probe_w, probe_h, fractal_type=tile.fractal_type, julia_cx=tile.julia_cx,
+                                     julia_cy=tile.julia_cy, gen_n=tile.gen_n, gen_kr=tile.gen_kr,
+                                     gen_ki=tile.gen_ki, bbsa_order=0)
 
     def band_histogram(self, view, it_band):
         import torch

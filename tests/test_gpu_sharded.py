@@ -93,9 +93,26 @@ def test_render_split_one_rank_nccl_group():
     dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
                             timeout=datetime.timedelta(seconds=60))
     try:
-        rgb, it = sharded.render_split(v, sharded.DeviceBackend())
-        torch.cuda.synchronize()
-        assert np.array_equal(it.cpu().numpy().view(np.uint32), it_want.view(np.uint32))
-        assert np.array_equal(rgb.cpu().numpy(), rgb_want)
+        for balance in (None, "probe"):
+            rgb, it = sharded.render_split(v, sharded.DeviceBackend(), balance=balance)
+            torch.cuda.synchronize()
+            assert np.array_equal(it.cpu().numpy().view(np.uint32), it_want.view(np.uint32))
+            assert np.array_equal(rgb.cpu().numpy(), rgb_want)
     finally:
         dist.destroy_process_group()
+
+
+def test_device_probe_costs():
+    """The device probe behind probe balancing: row weights of a view (one per frame row,
+    every probe pixel costing at least one step) and per-tile costs of a batch."""
+    from fractura_b200 import batch as fb
+    v = view(0)
+    be = sharded.DeviceBackend()
+    w = sharded.probe_row_weights(v, be.probe_map, 64, 36)
+    assert w.shape == (v["H"],) and np.all(w >= 64)
+    bands = sharded.band_bounds(v["H"], 3, w)
+    assert bands[0][0] == 0 and bands[-1][1] == v["H"]
+    tiles = [fb.Tile(cx=Decimal(v["cx"]), cy=Decimal(v["cy"]), width=Decimal(v["width"]) * f, W=64, H=48,
+                     max_iter=v["max_iter"]) for f in (1, 4)]
+    cost = sharded.probe_tile_costs(tiles, be.probe_tile, 16, 16)
+    assert len(cost) == 2 and all(c >= 64 * 48 for c in cost)

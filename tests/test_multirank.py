@@ -158,6 +158,13 @@ class OracleBackend:
                                    np.arange(r0, r1, dtype=np.float64))
         return torch.from_numpy(s)
 
+    def probe_map(self, view, probe_w, probe_h):
+        """A stand-in probe whose cost falls row by row (the upper rows four times dearer
+        than the lower ones), so that probe balancing moves the band edge."""
+        import numpy as np
+        rows = np.linspace(4000.0, 1000.0, probe_h)[:, None]
+        return np.repeat(rows, probe_w, axis=1).astype(np.float32)
+
     def band_histogram(self, view, it_band):
         import torch
         import oracle
@@ -193,7 +200,7 @@ class OracleBackend:
         return torch.from_numpy(fr.rgb.copy())
 
 
-def _split_worker(rank, world, port, outdir):
+def _split_worker(rank, world, port, outdir, balance=None):
     import datetime
 
     import torch.distributed as dist
@@ -205,7 +212,7 @@ def _split_worker(rank, world, port, outdir):
         import oracle
         from fractura_b200 import sharded
         oracle.set_threads(1)
-        rgb, it = sharded.render_split(_split_view(), OracleBackend())
+        rgb, it = sharded.render_split(_split_view(), OracleBackend(), balance=balance)
         import numpy as np
         np.savez(os.path.join(outdir, f"rank{rank}.npz"), rgb=rgb.numpy(), it=it.numpy())
         dist.barrier()
@@ -213,17 +220,20 @@ def _split_worker(rank, world, port, outdir):
         dist.destroy_process_group()
 
 
-def test_split_frame_world2_equals_single_frame(tmp_path):
+@pytest.mark.parametrize("balance", [None, "probe"])
+def test_split_frame_world2_equals_single_frame(tmp_path, balance):
     """One frame shared out over two gloo ranks by row bands (orbit broadcast from rank 0,
-    band histograms all-reduced before the CDF, bands all-gathered) equals the frame the
-    oracle renders in one process, bit for bit, on both ranks."""
+    band histograms all-reduced before the CDF, bands all-gathered; even bands or bands
+    balanced by rank 0's probe) equals the frame the oracle renders in one process, bit
+    for bit, on both ranks."""
     import numpy as np
     for d in ("oracle", "tests"):
         sys.path.insert(0, os.path.join(ROOT, d))
     import frames
     from fractura_b200 import abi
     port = _free_port()
-    mp.start_processes(_split_worker, args=(2, port, str(tmp_path)), nprocs=2, join=True, start_method="spawn")
+    mp.start_processes(_split_worker, args=(2, port, str(tmp_path), balance), nprocs=2, join=True,
+                       start_method="spawn")
     got = []
     for rank in range(2):
         d = np.load(tmp_path / f"rank{rank}.npz")
@@ -234,3 +244,31 @@ def test_split_frame_world2_equals_single_frame(tmp_path):
     for rank, rgb, it in got:
         assert np.array_equal(it.view(np.uint32), fr.iter_map.view(np.uint32)), rank
         assert np.array_equal(rgb, fr.rgb), rank
+
+
+def test_probe_costs_and_row_weights():
+    """Probe costs (escape step; max_iter when bounded) and their mapping to frame rows,
+    and the bands and tile costs they give."""
+    import numpy as np
+    from fractura_b200 import sharded
+    c = sharded.costs_from_probe(np.array([[-1.0, 0.0, 10.5]]), 100)
+    assert np.array_equal(c, [[100.0, 1.0, 10.5]])
+    pc = np.array([[1.0, 1.0], [2.0, 2.0], [3.0, 3.0]])
+    w = sharded.row_weights(pc, 5)   # probe rows at frame rows 0, 2, 4
+    assert np.array_equal(w, [2.0, 2.0, 4.0, 6.0, 6.0])
+    assert np.array_equal(sharded.row_weights(pc, 1), [4.0])
+    view = {"H": 90, "max_iter": 1000}
+    wt = sharded.probe_row_weights(view, OracleBackend().probe_map)
+    bands = sharded.band_bounds(90, 2, wt)
+    assert bands[0][1] < 45 and bands[0][0] == 0 and bands[1][1] == 90   # the dear upper rows go to rank 0
+    lo, hi = wt[:bands[0][1]].sum(), wt[bands[0][1]:].sum()
+    assert abs(lo - hi) <= wt.max()
+
+    class T:
+        def __init__(self, W, H, mi):
+            self.W, self.H, self.max_iter = W, H, mi
+    tiles = [T(64, 64, 1000), T(32, 32, 1000), T(64, 64, 50)]
+    probe = lambda t, w, h: np.full((h, w), -1.0 if t.max_iter == 50 else 10.0, np.float32)
+    cost = sharded.probe_tile_costs(tiles, probe, 8, 8)
+    assert cost == [10.0 * 64 * 64, 10.0 * 32 * 32, 50.0 * 64 * 64]
+    assert sharded.shard_tiles(cost, 2) == [[2], [0, 1]]   # the bounded tile is the dearest
