@@ -14,8 +14,8 @@
 //   ap_smooth_adjoint: per pixel, for the upstream gradient g = dL/ds, sweeps the
 //     orbit backwards one checkpoint segment at a time, recomputing the segment's
 //     z from its checkpoint (first every 16th z, then each 16-step sub-segment into
-//     shared memory; no orbit is stored), and accumulates dL/dtheta; per-block sums
-//     (deterministic, summed by the caller);
+//     shared memory; no orbit is stored), and accumulates dL/dtheta; one row of sums
+//     per warp of 8 x 4 pixels (deterministic, summed by the caller);
 //   ap_smooth_tangent: forward mode (one tangent per parameter carried beside z),
 //     per-pixel ds/dtheta, the independent check of the adjoint.
 // Holomorphic steps make both sweeps complex multiplications: the adjoint
@@ -84,11 +84,14 @@ __device__ __forceinline__ double inv_ln_of(const ApGradView& v) {
     return (v.fractal_type == 4 && v.gen_n > 1) ? 1.0 / log((double)v.gen_n) : kInvLn2;
 }
 
-__global__ void __launch_bounds__(256) smooth_forward_kernel(const ApGradView v, double* __restrict__ s64,
-                                                             int32_t* __restrict__ kmap,
-                                                             double2* __restrict__ ckpt, int n_ck) {
-    const int i = blockIdx.x * 16 + (threadIdx.x & 15);
-    const int j = blockIdx.y * 16 + (threadIdx.x >> 4);
+// Blocks of 8 x 8 pixels (two warps of 8 x 4): a block lives as long as its slowest
+// pixel, so small blocks let the SMs refill as blocks finish, and the grid of a 512 x 512
+// view (4096 blocks) is resident at once (32 blocks of 64 threads per SM: 4736).
+__global__ void __launch_bounds__(64) smooth_forward_kernel(const ApGradView v, double* __restrict__ s64,
+                                                            int32_t* __restrict__ kmap,
+                                                            double2* __restrict__ ckpt, int n_ck) {
+    const int i = blockIdx.x * 8 + (threadIdx.x & 7);
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 3);
     if (i >= v.width || j >= v.height) return;
     const size_t idx = (size_t)j * v.width + i;
     C2d z, c, d;
@@ -129,18 +132,29 @@ __device__ __forceinline__ C2d ds_dzK(const ApGradView& v, C2d zK) {
     return {f * zK.r, f * zK.i};
 }
 
-__global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
-                                                             const double* __restrict__ grad_s,
-                                                             const int32_t* __restrict__ kmap,
-                                                             const double2* __restrict__ ckpt, int n_ck,
-                                                             double* __restrict__ pix_grads,
-                                                             double* __restrict__ block_sums) {
-    __shared__ double red[5][128];
-    __shared__ double2 buf[kSub][128];  // one sub-segment of z per thread (32 KiB)
-    const int tpr = (v.width + 15) / 16;  // blocks of 128 threads cover 16 x 8 pixels
-    const int bx = blockIdx.x % tpr, by = blockIdx.x / tpr;
-    const int i = bx * 16 + (threadIdx.x & 15);
-    const int j = by * 8 + (threadIdx.x >> 4);
+// Each warp takes 8 x 4 pixels and writes its own row of sums (shuffles, no block
+// barrier); a block of kAdjWarps warps holds its shared sub-segment buffer until its
+// slowest pixel is done, so small blocks keep the SMs filling up behind long-lived pixels.
+#ifndef AP_ADJ_WARPS
+#define AP_ADJ_WARPS 4
+#endif
+constexpr int kAdjWarps = AP_ADJ_WARPS;
+
+__global__ void __launch_bounds__(32 * kAdjWarps) smooth_adjoint_kernel(const ApGradView v,
+                                                                        const double* __restrict__ grad_s,
+                                                                        const int32_t* __restrict__ kmap,
+                                                                        const double2* __restrict__ ckpt,
+                                                                        int n_ck, double* __restrict__ pix_grads,
+                                                                        double* __restrict__ block_sums,
+                                                                        int n_tiles) {
+    __shared__ double2 buf[kSub][32 * kAdjWarps];  // one sub-segment of z per thread (8 KiB per warp)
+    const int tile = blockIdx.x * kAdjWarps + (threadIdx.x >> 5);
+    if (tile >= n_tiles) return;  // whole warps only: the shuffles below stay full
+    const int lane = threadIdx.x & 31;
+    const int tpr = (v.width + 7) / 8;
+    const int bx = tile % tpr, by = tile / tpr;
+    const int i = bx * 8 + (lane & 7);
+    const int j = by * 4 + (lane >> 3);
     double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // cx, cy, ln w, Re P, Im P
     if (i < v.width && j < v.height) {
         const size_t idx = (size_t)j * v.width + i;
@@ -210,14 +224,11 @@ __global__ void __launch_bounds__(128) smooth_adjoint_kernel(const ApGradView v,
             for (int q = 0; q < 5; ++q) pix_grads[idx * 5 + q] = g[q];
         }
     }
-    for (int q = 0; q < 5; ++q) red[q][threadIdx.x] = g[q];
-    __syncthreads();
-    for (int o = 64; o > 0; o >>= 1) {
-        if (threadIdx.x < o)
-            for (int q = 0; q < 5; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x < 5) block_sums[(size_t)blockIdx.x * 5 + threadIdx.x] = red[threadIdx.x][0];
+    // the warp's sums, by halves (a fixed order: the result does not depend on timing)
+    for (int o = 16; o > 0; o >>= 1)
+        for (int q = 0; q < 5; ++q) g[q] += __shfl_down_sync(0xffffffffu, g[q], o);
+    if (lane == 0)
+        for (int q = 0; q < 5; ++q) block_sums[(size_t)tile * 5 + q] = g[q];
 }
 
 __global__ void __launch_bounds__(256) smooth_tangent_kernel(const ApGradView v, double* __restrict__ ds) {
@@ -285,14 +296,14 @@ extern "C" int ap_smooth_forward(const ApGradView* v, double* s64, int32_t* kmap
         ap::set_error("ap_smooth_forward: s64 required; ckpt needs ceil(max_iter / ckpt_every) + 1 slots");
         return AP_E_INVALID;
     }
-    dim3 grid((v->width + 15) / 16, (v->height + 15) / 16);
-    ap::smooth_forward_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+    dim3 grid((v->width + 7) / 8, (v->height + 7) / 8);
+    ap::smooth_forward_kernel<<<grid, 64, 0, static_cast<cudaStream_t>(stream)>>>(
         *v, s64, kmap, reinterpret_cast<double2*>(ckpt), n_ck);
     return ap::check_launch("smooth_forward_kernel");
 }
 
 extern "C" int32_t ap_smooth_adjoint_blocks(int32_t width, int32_t height) {
-    return ((width + 15) / 16) * ((height + 7) / 8);
+    return ((width + 7) / 8) * ((height + 3) / 4);
 }
 
 extern "C" int ap_smooth_adjoint(const ApGradView* v, const double* grad_s, const int32_t* kmap,
@@ -307,8 +318,9 @@ extern "C" int ap_smooth_adjoint(const ApGradView* v, const double* grad_s, cons
         return AP_E_INVALID;
     }
     const int blocks = ap_smooth_adjoint_blocks(v->width, v->height);
-    ap::smooth_adjoint_kernel<<<blocks, 128, 0, static_cast<cudaStream_t>(stream)>>>(
-        *v, grad_s, kmap, reinterpret_cast<const double2*>(ckpt), n_ck, pix_grads, block_sums);
+    ap::smooth_adjoint_kernel<<<(blocks + ap::kAdjWarps - 1) / ap::kAdjWarps, 32 * ap::kAdjWarps, 0,
+                                static_cast<cudaStream_t>(stream)>>>(
+        *v, grad_s, kmap, reinterpret_cast<const double2*>(ckpt), n_ck, pix_grads, block_sums, blocks);
     return ap::check_launch("smooth_adjoint_kernel");
 }
 

@@ -409,8 +409,8 @@ AP_API int ap_render_batch(const ApTileDesc* tiles, const int64_t* first_patch, 
  * ap_smooth_forward: s64[H, W] float64 smooth values (-1 interior), kmap[H, W] escape
  *   steps (-1 bounded, -2 cardioid/bulb), and, when ckpt is given, the orbit at every
  *   ckpt_every-th step: ckpt[H, W, n_ck] complex float64, n_ck >= ceil(max_iter/ckpt_every)+1.
- * ap_smooth_adjoint: for grad_s[H, W] = dL/ds, dL/dtheta summed per block of pixels into
- *   block_sums[ap_smooth_adjoint_blocks(W, H), 5] (the caller sums the rows); the orbit
+ * ap_smooth_adjoint: for grad_s[H, W] = dL/ds, dL/dtheta summed per tile of 8 x 4 pixels
+ *   into block_sums[ap_smooth_adjoint_blocks(W, H), 5] (the caller sums the rows); the orbit
  *   is recomputed segment by segment from ckpt, never stored; pix_grads[H, W, 5]
  *   (optional) receives each pixel's term.
  * ap_smooth_tangent: forward mode, ds[H, W, 5] = ds/dtheta per pixel. */
