@@ -12,7 +12,10 @@
 
 namespace ap {
 
-constexpr int kTile = 16;
+// Blocks of kTile x kTile pixels (warps of 8 x 4).  A block lives as long as its slowest
+// pixel; small blocks let an SM refill as each one ends, instead of holding 8 warps for the
+// one long-lived pixel of a 16 x 16 tile.
+constexpr int kTile = 8;
 
 template <int TIER, int ARITH>
 __device__ __forceinline__ SampleOut sample_at(const ApFrameParams& p, const ApFrameBuffers& b,
@@ -41,7 +44,7 @@ __device__ __forceinline__ SampleOut sample_at(const ApFrameParams& p, const ApF
 // hist_resolve = 1: ssaa_resolve_hist_*_kernel semantics
 //   (math_core/cuda_kernels.py:2038-2234).
 template <int TIER, int ARITH>
-__global__ void __launch_bounds__(256) render_pass_kernel(const ApFrameParams p,
+__global__ void __launch_bounds__(kTile * kTile) render_pass_kernel(const ApFrameParams p,
                                                           const ApFrameBuffers b,
                                                           const int hist_resolve) {
     const int i = blockIdx.x * kTile + (threadIdx.x & (kTile - 1));
