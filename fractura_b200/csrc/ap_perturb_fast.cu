@@ -1,5 +1,5 @@
 // ap_perturb_fast.cu -- the per-frame coarse-pass kernel over coarse_pixel
-// (ap_coarse.cuh): one thread per pixel on 16 x 16 tiles, 8 x 4 pixels per warp.  Picked by
+// (ap_coarse.cuh): one thread per pixel on square tiles, 8 x 4 pixels per warp.  Picked by
 // ap_render_pass for AP_TIER_PERTURB coarse passes without in-kernel colour
 // when the buffers carry the packed orbit and, with BLA, the packed table.
 #include "ap_coarse.cuh"
@@ -9,35 +9,43 @@ namespace ap {
 #ifndef AP_REBASE_MIN_BLOCKS
 #define AP_REBASE_MIN_BLOCKS 4
 #endif
+// Tiles of kCoarseTile x kCoarseTile pixels per block (16 or 8), warps of 8 x 4 pixels.
+#ifndef AP_COARSE_TILE
+#define AP_COARSE_TILE 8
+#endif
+constexpr int kCoarseTile = AP_COARSE_TILE;
+constexpr int kCoarseThreads = kCoarseTile * kCoarseTile;
+constexpr int kCoarseScale = 256 / kCoarseThreads;  // blocks per 256-thread register budget
 
 template <int ARITH, int FT, bool BLA, bool REBASE>
-__global__ void __launch_bounds__(256, REBASE ? AP_REBASE_MIN_BLOCKS : 4) perturb_coarse_kernel(const ApFrameParams p,
-                                                                const ApFrameBuffers b, int row0,
-                                                                int row_end) {
-    // each warp takes an 8 x 4 patch of its block's 16 x 16 pixels: neighbours
-    // follow similar paths through the loop, so compact warps diverge less; rows
-    // [row0, row_end) of the frame (a whole frame, or one band of a split frame)
+__global__ void __launch_bounds__(kCoarseThreads, (REBASE ? AP_REBASE_MIN_BLOCKS : 4) * kCoarseScale)
+    perturb_coarse_kernel(const ApFrameParams p, const ApFrameBuffers b, int row0, int row_end) {
+    // each warp takes an 8 x 4 patch of its block's pixels: neighbours follow similar
+    // paths through the loop, so compact warps diverge less; rows [row0, row_end) of
+    // the frame (a whole frame, or one band of a split frame)
+    constexpr int kWarpsPerRow = kCoarseTile / 8;
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-    const int i = blockIdx.x * 16 + (w & 1) * 8 + (l & 7);
-    const int j = row0 + blockIdx.y * 16 + (w >> 1) * 4 + (l >> 3);
+    const int i = blockIdx.x * kCoarseTile + (w % kWarpsPerRow) * 8 + (l & 7);
+    const int j = row0 + blockIdx.y * kCoarseTile + (w / kWarpsPerRow) * 4 + (l >> 3);
     if (i >= p.width || j >= row_end) return;
     coarse_pixel<ARITH, FT, BLA, REBASE>(p, b, i, j);
 }
 
 template <int ARITH, int FT>
 static void launch_ft(const ApFrameParams& p, const ApFrameBuffers& b, int r0, int r1, cudaStream_t st) {
-    dim3 grid((p.width + 15) / 16, (r1 - r0 + 15) / 16);
+    dim3 grid((p.width + kCoarseTile - 1) / kCoarseTile, (r1 - r0 + kCoarseTile - 1) / kCoarseTile);
     if (grid.y == 0) return;
     const bool rebase = (p.flags & AP_FLAG_REBASE) != 0;
+    constexpr int T = kCoarseThreads;
     if constexpr (ARITH == AP_ARITH_FAST) {  // validated: AP_ARITH_FAST passes are rebasing passes
-        if (p.bla_levels > 1) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
-        else perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
+        if (p.bla_levels > 1) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, T, 0, st>>>(p, b, r0, r1);
+        else perturb_coarse_kernel<ARITH, FT, false, true><<<grid, T, 0, st>>>(p, b, r0, r1);
     } else if (p.bla_levels > 1) {
-        if (rebase) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
-        else perturb_coarse_kernel<ARITH, FT, true, false><<<grid, 256, 0, st>>>(p, b, r0, r1);
+        if (rebase) perturb_coarse_kernel<ARITH, FT, true, true><<<grid, T, 0, st>>>(p, b, r0, r1);
+        else perturb_coarse_kernel<ARITH, FT, true, false><<<grid, T, 0, st>>>(p, b, r0, r1);
     } else {
-        if (rebase) perturb_coarse_kernel<ARITH, FT, false, true><<<grid, 256, 0, st>>>(p, b, r0, r1);
-        else perturb_coarse_kernel<ARITH, FT, false, false><<<grid, 256, 0, st>>>(p, b, r0, r1);
+        if (rebase) perturb_coarse_kernel<ARITH, FT, false, true><<<grid, T, 0, st>>>(p, b, r0, r1);
+        else perturb_coarse_kernel<ARITH, FT, false, false><<<grid, T, 0, st>>>(p, b, r0, r1);
     }
 }
 
