@@ -56,19 +56,20 @@ class Tile:
 @dataclass(frozen=True)
 class BatchConfig:
     """Launch shape of the persistent kernel: patch_w x patch_h = 256 pixels per work
-    item, blocks_per_sm resident blocks, min_blocks = the register budget (4 or 6),
-    quantum = loop steps per pixel between two compactions of a block's pixels."""
+    item, blocks_per_sm resident blocks of 512 threads, min_blocks = the register
+    budget (4: 64 registers, 6: 42), quantum = loop steps per pixel between two
+    compactions of a block's pixels."""
     patch_w: int = 16
     patch_h: int = 16
-    blocks_per_sm: int = 4
+    blocks_per_sm: int = 2
     min_blocks: int = 4
-    quantum: int = 64
+    quantum: int = 256
 
 
 CANDIDATES = tuple(BatchConfig(pw, 256 // pw, bps, mb, qu)
-                   for pw in (16, 32, 8)
-                   for (bps, mb) in ((4, 4), (6, 6))
-                   for qu in (64, 128))
+                   for pw in (16, 8)
+                   for (bps, mb) in ((2, 4), (3, 6))
+                   for qu in (128, 256))
 
 
 def _ptr(t):

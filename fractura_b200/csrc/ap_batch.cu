@@ -26,7 +26,13 @@ namespace ap {
 
 static_assert(sizeof(ApTileDesc) % 16 == 0, "tile descriptors are 16-byte aligned records");
 
-constexpr int kBatchThreads = 256;
+// Threads (pixel slots) per block.  A larger block packs its unfinished pixels into
+// fuller warps at each compaction: 512 slots took config 4 from 230 to 214 ms against
+// 256 (with a 256-step quantum), 128 slots to 250 ms.
+#ifndef AP_BATCH_THREADS
+#define AP_BATCH_THREADS 512
+#endif
+constexpr int kBatchThreads = AP_BATCH_THREADS;
 
 inline __device__ ApFrameBuffers tile_buffers(const ApTileDesc* t) {
     ApFrameBuffers b{};
@@ -45,7 +51,7 @@ inline __device__ ApFrameBuffers tile_buffers(const ApTileDesc* t) {
 // A stage-2 pixel keeps z itself where a stage-1 pixel keeps its delta; a one-pass
 // pixel keeps its reference index m where a single-reference pixel keeps the step
 // at which it entered stage 2.  The finished sample is not kept: a pixel that has
-// not finished holds the interior sample.  16 KiB per block.
+// not finished holds the interior sample.  64 bytes a slot (32 KiB for 512 slots).
 struct BatchSlots {
     double zx[kBatchThreads], zy[kBatchThreads];
     double dcx[kBatchThreads], dcy[kBatchThreads];
@@ -197,7 +203,7 @@ __device__ __forceinline__ bool batch_pixel_at(const ApTileDesc* __restrict__ ti
 }
 
 template <int ARITH, int MINB>
-__global__ void __launch_bounds__(kBatchThreads, MINB) batch_kernel(const ApTileDesc* __restrict__ tiles,
+__global__ void __launch_bounds__(kBatchThreads, MINB * 256 / kBatchThreads) batch_kernel(const ApTileDesc* __restrict__ tiles,
                                                                     const int64_t* __restrict__ first,
                                                                     int n, int patch_w, int patch_h,
                                                                     int quantum,
