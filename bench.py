@@ -865,11 +865,12 @@ def batch_arm(args, wl, rank, world, local_rank, steps, headline):
     h2d = d2h = 0
     for _ in range(e2e_steps):
         hp.clear_reference_orbit_cache()
-        bb = fb.prepare_batch(tiles, arith=wl["arith"], bla_form=wl["bla_form"], stream=stream)
-        bb.render(cfg)
-        maps = [o["iter"].cpu() for o in bb.tiles_out]
+        # the tiles whose references are ready render while the host searches the others
+        sb = fb.render_streamed(tiles, arith=wl["arith"], bla_form=wl["bla_form"], stream=stream, cfg=cfg)
+        stream.synchronize()  # the maps are read once the batch stream has finished
+        maps = [o["iter"].cpu() for o in sb.tiles_out]
         d2h = sum(m.numel() * 4 for m in maps)
-        h2d = sum(16 * (p.ref_len + 1) for p in bb.params) + len(bb.desc_dev)
+        h2d = sum(sum(16 * (p.ref_len + 1) for p in part.params) + len(part.desc_dev) for part in sb.parts)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     barrier(world)
     e2e = iters * e2e_steps * world / e2e_s / 1e9
@@ -913,7 +914,9 @@ def batch_arm(args, wl, rank, world, local_rank, steps, headline):
                      "kernel_ms_per_step": kernel_ms, "traffic": None},
         "e2e": {"value": e2e, "unit": "G iter/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
-                "path": "batch.prepare_batch (host orbits, device tables) + render + download of every tile"},
+                "path": "batch.render_streamed (host orbits; each time the device is idle, the tiles ready so "
+                        "far get their tables and go to one launch) + download of every tile",
+                "launches_per_step": len(sb.parts)},
         "forms": forms,
         "autotuner": {"chosen": vars(cfg) if hasattr(cfg, "__dict__") else repr(cfg),
                       "candidates_ms": [[round(ms, 4), repr(c)] for ms, c in fb.tuned_timings(b)]},

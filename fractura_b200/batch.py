@@ -15,6 +15,7 @@ the fused step (the batch's single-reference tiles run "ref_cuda").
     cfg = tune(batch)                       # autotuned patch shape and occupancy
     batch.render(cfg)                       # or: g = batch.capture(cfg); g.replay()
     batch.tiles_out[t]["iter"]              # [H, W] float32 smooth values on the device
+    sb = render_streamed(tiles, cfg=cfg)    # or: launches while the references still arrive
 """
 import ctypes as C
 import os
@@ -200,26 +201,40 @@ def _tile_inputs(t, ref, arith, bla_form, torch, stream, L, scratch):
     return p, orbit, bla_packed, out, (d_re, d_im), rl
 
 
+_ARITH_CODES = {"ref_cpu": abi.AP_ARITH_REF_CPU, "ref_cuda": abi.AP_ARITH_REF_CUDA, "fast": abi.AP_ARITH_FAST}
+
+
+def _check_batch(tiles, arith, bla_form):
+    if bla_form not in ("reference", "accurate"):
+        raise ValueError("bla_form must be 'reference' or 'accurate'")
+    if arith not in _ARITH_CODES:
+        raise ValueError("arith must be 'ref_cpu', 'ref_cuda' or 'fast' (the fused step of one-pass tiles; "
+                         "the batch's single-reference tiles then run 'ref_cuda')")
+    if not tiles:
+        raise ValueError("a batch needs at least one tile")
+
+
 def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, workers=None):
     """Host and device preparation of a batch: reference orbits (in parallel threads;
     the native orbit code releases the GIL), device BLA tables, packed records,
     outputs and the descriptor array, ordered by estimated cost (pixels x ref_len)."""
     import torch
-    if bla_form not in ("reference", "accurate"):
-        raise ValueError("bla_form must be 'reference' or 'accurate'")
-    if arith not in ("ref_cpu", "ref_cuda", "fast"):
-        raise ValueError("arith must be 'ref_cpu', 'ref_cuda' or 'fast' (the fused step of one-pass tiles; "
-                         "the batch's single-reference tiles then run 'ref_cuda')")
-    if not tiles:
-        raise ValueError("a batch needs at least one tile")
-    L = _lib.load()
+    _check_batch(tiles, arith, bla_form)
     stream = stream or torch.cuda.current_stream()
-    b = PreparedBatch(list(tiles), {"ref_cpu": abi.AP_ARITH_REF_CPU, "ref_cuda": abi.AP_ARITH_REF_CUDA,
-                                    "fast": abi.AP_ARITH_FAST}[arith], stream)
+    tiles = list(tiles)
     # the orbits first, concurrently (host work), each once: a batch can hold more
     # tiles than the orbit cache keeps
     with ThreadPoolExecutor(max_workers=max(1, workers or os.cpu_count() or 8)) as ex:
-        refs = list(ex.map(_warm_orbit, b.tiles))
+        refs = list(ex.map(_warm_orbit, tiles))
+    return _assemble(tiles, refs, arith, bla_form, stream, stream)
+
+
+def _assemble(tiles, refs, arith, bla_form, stream, prep):
+    """A PreparedBatch of tiles around their references refs: device tables, records,
+    outputs and descriptors, built on stream prep; the batch renders on stream."""
+    import torch
+    L = _lib.load()
+    b = PreparedBatch(list(tiles), _ARITH_CODES[arith], stream)
     scratch_box = {}
     lock = threading.Lock()
 
@@ -231,10 +246,10 @@ def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, wor
             return scratch_box["t"]
 
     recs = []
-    with torch.cuda.stream(stream):
+    with torch.cuda.stream(prep):
         for t, ref in zip(b.tiles, refs):
-            recs.append(_tile_inputs(t, ref, arith, bla_form, torch, stream, L, scratch))
-    stream.synchronize()
+            recs.append(_tile_inputs(t, ref, arith, bla_form, torch, prep, L, scratch))
+    prep.synchronize()
     cost = [t.W * t.H * max(1, r[5]) for t, r in zip(b.tiles, recs)]
     b.order = sorted(range(len(b.tiles)), key=lambda q: -cost[q])
     arr = (abi.ApTileDesc * len(b.tiles))()
@@ -250,9 +265,79 @@ def prepare_batch(tiles, arith="ref_cpu", bla_form="reference", stream=None, wor
     b.params = [recs[q][0] for q in range(len(b.tiles))]
     b.desc_host = arr
     raw = np.frombuffer(bytes(arr), dtype=np.uint8)
-    b.desc_dev = torch.from_numpy(raw.copy()).cuda()
-    b.head = torch.zeros(1, dtype=torch.int64, device="cuda")
+    with torch.cuda.stream(prep):
+        b.desc_dev = torch.from_numpy(raw.copy()).cuda()
+        b.head = torch.zeros(1, dtype=torch.int64, device="cuda")
+    prep.synchronize()
     return b
+
+
+def _search_cost(t):
+    """Estimated host cost of a tile's reference search: max_iter x the formula's degree."""
+    return float(t.max_iter) * (float(t.gen_n) if t.fractal_type == 4 else 2.0)
+
+
+class StreamedBatch:
+    """The parts of a streamed batch (PreparedBatch each) and every tile's outputs, in the
+    order of the tiles given."""
+
+    def __init__(self, tiles):
+        self.tiles = list(tiles)
+        self.parts = []
+        self.tiles_out = [None] * len(self.tiles)
+
+    def nominal_iterations(self):
+        """Sum over tiles of their escape steps (max_iter for pixels that never escape)."""
+        tot = 0
+        for t, out in zip(self.tiles, self.tiles_out):
+            k = out["kmap"].cpu().numpy()
+            tot += int(k[k >= 0].astype(np.int64).sum()) + t.max_iter * int(np.count_nonzero(k == -1))
+        return tot
+
+
+def render_streamed(tiles, arith="ref_cpu", bla_form="reference", stream=None, cfg=BatchConfig(), workers=None,
+                    poll_s=0.002):
+    """Render a batch while its reference searches are still running.  The searches run
+    in host threads; whenever the device has finished the last launch, the tiles whose
+    references have arrived get their tables and records (on a preparation stream of
+    their own, so that its synchronisations never wait for a running launch) and go to
+    one persistent launch on `stream`, and the host goes on searching the others.  Values
+    equal prepare_batch + render of the whole batch, tile for tile.  Returns a
+    StreamedBatch; the caller synchronises `stream` before reading the outputs."""
+    import torch
+    from concurrent.futures import FIRST_COMPLETED, wait
+    _check_batch(tiles, arith, bla_form)
+    stream = stream or torch.cuda.current_stream()
+    prep = torch.cuda.Stream()
+    res = StreamedBatch(tiles)
+    last = None  # the event after the latest launch
+    # the longest searches start first (a reference costs about max_iter steps of the
+    # formula's degree), so that their tiles, which tend to cost the most on the device too,
+    # do not all wait for the last launch
+    order = sorted(range(len(res.tiles)), key=lambda q: -_search_cost(res.tiles[q]))
+    with ThreadPoolExecutor(max_workers=max(1, workers or os.cpu_count() or 8)) as ex:
+        futs = {ex.submit(_warm_orbit, res.tiles[q]): q for q in order}
+        ready = []
+        while futs or ready:
+            if futs:
+                done, _ = wait(list(futs), timeout=poll_s if ready else None, return_when=FIRST_COMPLETED)
+                for f in done:
+                    ready.append((futs.pop(f), f.result()))
+            if ready and (not futs or last is None or last.query()):
+                idx = [q for q, _ in ready]
+                part = _assemble([res.tiles[q] for q in idx], [r for _, r in ready], arith, bla_form,
+                                 stream, prep)
+                ready = []
+                with torch.cuda.stream(prep):
+                    part._plan(cfg)
+                prep.synchronize()
+                part.render(cfg)
+                last = torch.cuda.Event()
+                last.record(stream)
+                for q, o in zip(idx, part.tiles_out):
+                    res.tiles_out[q] = o
+                res.parts.append(part)
+    return res
 
 
 def _warm_orbit(t):

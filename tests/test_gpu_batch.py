@@ -109,3 +109,23 @@ def test_graph_replay_and_every_launch_shape_agree(rebase):
         assert cfg in fb.CANDIDATES
         assert len(fb.tuned_timings(b)) == len(fb.CANDIDATES)
         assert fb.tune(b) is cfg   # cached
+
+
+@pytest.mark.parametrize("arith,rebase", [("ref_cpu", False), ("fast", True)])
+def test_streamed_batch_equals_the_whole_batch(arith, rebase):
+    """render_streamed (launches while references still arrive, several parts) gives every
+    tile the values of prepare_batch + render of the whole batch."""
+    import torch
+    tiles = _tiles(rebase)
+    s = torch.cuda.Stream()
+    hp.clear_reference_orbit_cache()
+    b = fb.prepare_batch(tiles, arith=arith, bla_form="accurate", stream=s)
+    b.render(fb.BatchConfig())
+    torch.cuda.synchronize()
+    hp.clear_reference_orbit_cache()
+    sb = fb.render_streamed(tiles, arith=arith, bla_form="accurate", stream=s, workers=2)
+    s.synchronize()
+    assert len(sb.parts) >= 1 and sum(p.n for p in sb.parts) == len(tiles)
+    for want, got in zip(b.tiles_out, sb.tiles_out):
+        assert torch.equal(want["iter"], got["iter"]) and torch.equal(want["kmap"], got["kmap"])
+    assert sb.nominal_iterations() == b.nominal_iterations()
