@@ -30,7 +30,7 @@ pixel's cost is its escape step (max_iter when it stays bounded).
 
 The steps of a split frame go through a backend object -- find_reference, render_band,
 band_histogram, cdf_from_histogram, colour_band -- so the same orchestration drives the
-engine's device code (DeviceBackend) and, in the multi-process CPU tests, the checker.
+engine's device code (DeviceBackend) and, in the multi-process CPU tests, the oracle.
 """
 import ctypes as C
 from decimal import Decimal

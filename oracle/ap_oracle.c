@@ -1,7 +1,7 @@
 /*
  * ap_oracle.c -- CPU restatement of the reference escape-time path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine:
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle for the CUDA engine:
  * the parity tests, __graft_entry__.smoke() and the CPU-baseline leg of
  * bench.py call it; the product path never does.  It is written from the
  * reference's Python/Numba sources line by line, in plain C, and shares no

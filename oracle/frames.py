@@ -1,6 +1,6 @@
 """Perturbation-tier frames through the oracle, pass for pass.
 
-TEST INFRASTRUCTURE ONLY (the checker and bench.py's CPU baseline / reference arm):
+TEST INFRASTRUCTURE ONLY (the oracle's frames and bench.py's CPU baseline / reference arm):
 the frame driver of the reference's perturbation path restated around the C oracle
 (ap_oracle.c), in the order the engine issues its passes -- reference orbit search
 (ref_orbit.py), chained-BLA table, the render pass, histogram and colour, the SSAA edge

@@ -1,6 +1,6 @@
 """Reference orbits for the oracle, in Python's decimal module.
 
-TEST INFRASTRUCTURE ONLY: the checker's own reference-orbit search, so that oracle
+TEST INFRASTRUCTURE ONLY: the oracle's own reference-orbit search, so that oracle
 frames and bench.py's CPU baseline share no code with the engine (whose orbits come
 from its native fixed-point code).  It restates the reference's Decimal branch, which
 is the reference's path wherever gmpy2 is absent (as here):

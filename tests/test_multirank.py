@@ -120,7 +120,7 @@ def _split_view():
 
 
 class OracleBackend:
-    """The split frame's per-rank steps through the checker (CPU): each rank evaluates
+    """The split frame's per-rank steps through the oracle (CPU): each rank evaluates
     only its own rows, at their global row indices (one-pass rebasing, dc-aware BLA)."""
 
     def __init__(self, arith=1, eps=1e-14):
