@@ -1,13 +1,23 @@
 // ap_fe32.cu -- FP32-mantissa FloatExp perturbation (AP_TIER_FLOATEXP32).
 //
-// The engine's fast form of the perturbation tiers.  The delta is held as
+// The engine's fast form of the perturbation tiers, for all five formulas.  The
+// delta is held as
 //   dz = w * 2^e,  w a complex float32 with max(|w_re|, |w_im|) in [1, 2)
 // after renormalisation, e an int32 exponent; delta_c = dcm * 2^-E with dcm a
-// complex float32 and E the frame's exponent scale.  One Mandelbrot/Julia step
-//   w' = 2 Z w + S w^2 + D,   S = 2^e (float, 0 below 2^-149),  D = dcm 2^(-E-e)
-// runs in FP32; the exponent changes only when |w| leaves [2^-16, 2^16]
-// (exact power-of-two rescaling, as the FP64 FloatExp tier of the reference
-// does with its 2^16 steps, math_core/cuda_kernels.py:913-923).
+// complex float32 and E the frame's exponent scale.  With S = 2^e (float, 0 below
+// 2^-126) and D = dcm 2^(-E-e) (0 for the Julia sets), one step runs in FP32:
+//   Mandelbrot, Julia:   w' = 2 Z w + S w^2 + D
+//   Burning Ship and its Julia set (y' = 2 |x| |y| - c_y):
+//     w'_x = 2 (Z_x w_x - Z_y w_y) + S (w_x^2 - w_y^2) + D_x
+//     w'_y = 2 (|Z_x| d_y + |Z_y| d_x + S d_x d_y) - D_y,
+//     d_x = (|Z_x + dz_x| - |Z_x|) 2^-e = s w_x when Z_x + dz_x keeps the sign s of
+//     Z_x, else -s (2 Z_x 2^-e + w_x) (and d_y alike);
+//   Multibrot z^n + k z + c:  P_1 = w, P_{j+1} = P_j Z + (S P_j + Z^j) w (P_j the
+//     scaled (Z + dz)^j - Z^j), w' = P_n + k w + D.
+// The exponent changes only when |w| leaves [2^-16, 2^16] (exact power-of-two
+// rescaling, as the FP64 FloatExp tier of the reference does with its 2^16 steps,
+// math_core/cuda_kernels.py:913-923; its Burning Ship and Multibrot delta steps are
+// :927-1010).
 //
 // What stays FP64 (and how):
 //   * the reference orbit: FP64 records (ap_pack_orbit) feed every FP64
@@ -15,13 +25,19 @@
 //   * BLA validity radii: r^2 * 2^B in FP64 (B a power-of-two bias so that
 //     |dz|^2 * 2^B does not underflow near any radius), compared with
 //     (double)|w|^2 * 2^(2e + B);
-//   * the Pauldelbrot glitch test |Z + dz|^2 < 1e-6 |Z|^2 and the escape test:
-//     an FP32 screen decides whether they can trigger at this step; when it
-//     can, they are evaluated in FP64 on Z and the exactly converted delta;
+//   * the Pauldelbrot glitch test |Z + dz|^2 < 1e-6 |Z|^2, the escape test, the
+//     Burning Ship sign tests and the one-pass rebase test |Z + dz| < |dz|: an FP32
+//     screen decides whether each can fire at this step (a sign can change only when
+//     |dz_x| >= |Z_x| / 2, a rebase only when |dz| > |Z| / 2); when it can, the test
+//     is evaluated in FP64 on Z and the exactly converted delta;
 //   * the smooth value at escape and the stage-2 direct iteration (after the
 //     reference escapes) run in FP64.
 // BLA leaps: A = am 2^ea, B = bm 2^eb with float mantissas (ap_pack_fe32);
 // dz' = A dz + B dc keeps exponent e + ea.
+//
+// One-pass rebasing (AP_FLAG_REBASE, fractal types 0, 1, 4) as in the FP64-delta
+// form: when |Z_m + dz| < |dz| or the reference has ended, dz <- Z_m + dz (formed in
+// FP64, then renormalised) and m <- 0; no pixel is glitched and there is no stage 2.
 //
 // FP64 slow path.  Two cases leave the FP32 range and take one step (or leap)
 // in FP64 on the same normalised quantities, renormalised in FP64 before the
@@ -34,6 +50,7 @@
 // stays finite and normal, and |dz|^2 2^600 only saturates (to 0 or inf) where
 // it is far from every radius -- where the comparison's outcome is certain.
 #include "ap_common.cuh"
+#include "ap_coarse.cuh"
 
 namespace ap {
 
@@ -118,12 +135,128 @@ __device__ __forceinline__ void renorm_to_float(double x, double y, float& wx, f
     e += ex;
 }
 
-template <bool BLA>
-__global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams p,
+// One FP64 step of the slow path on the normalised delta (x, y) 2^e around the FP64
+// orbit value Z: the float step's formulas with se = 2^e, the dc term (cx, cy) already
+// in units of 2^e.  The result is in units of 2^e.
+template <int FT>
+__device__ __forceinline__ void fe32_step_fp64(const ApFrameParams& p, double Zx, double Zy, double x,
+                                               double y, int e, double cx, double cy, double& nx,
+                                               double& ny) {
+    const double se = ldexp(1.0, e);
+    if (FT == kFtQuad) {
+        nx = 2.0 * (Zx * x - Zy * y) + se * (x - y) * (x + y) + cx;
+        ny = 2.0 * (Zx * y + Zy * x) + se * 2.0 * x * y + cy;
+    } else if (FT == kFtShip) {
+        const double sx = Zx >= 0.0 ? 1.0 : -1.0, sy = Zy >= 0.0 ? 1.0 : -1.0;
+        const double ddx = (Zx + x * se) * sx >= 0.0 ? sx * x : -sx * (ldexp(2.0 * Zx, -e) + x);
+        const double ddy = (Zy + y * se) * sy >= 0.0 ? sy * y : -sy * (ldexp(2.0 * Zy, -e) + y);
+        nx = 2.0 * (Zx * x - Zy * y) + se * (x - y) * (x + y) + cx;
+        ny = 2.0 * (fabs(Zx) * ddy + fabs(Zy) * ddx + se * ddx * ddy) - cy;
+    } else {
+        double pr = x, pi = y, qr = Zx, qi = Zy;
+        for (int t = 0; t < p.gen_n - 1; ++t) {
+            const double sr = se * pr + qr, si = se * pi + qi;
+            const double npr = (pr * Zx - pi * Zy) + (sr * x - si * y);
+            const double npi = (pr * Zy + pi * Zx) + (sr * y + si * x);
+            const double nqr = qr * Zx - qi * Zy, nqi = qr * Zy + qi * Zx;
+            pr = npr;
+            pi = npi;
+            qr = nqr;
+            qi = nqi;
+        }
+        nx = pr + (p.gen_kr * x - p.gen_ki * y) + cx;
+        ny = pi + (p.gen_kr * y + p.gen_ki * x) + cy;
+    }
+}
+
+// One FP32 step (the fast path): Z the float copy of the orbit value, (Dx, Dy) the dc
+// term in units of 2^e, (kr, ki) Multibrot's k.  A Burning Ship sign test that the float
+// screen cannot decide (|dz_x| >= |Z_x| / 2) reads the FP64 orbit value at orb_k.
+template <int FT>
+__device__ __forceinline__ void fe32_step(const ApFrameParams& p, const float4 Z, const double4* orb_k,
+                                          float& wx, float& wy, int e, float S, float Dx, float Dy,
+                                          float kr, float ki) {
+    if (FT == kFtQuad) {
+        const float tx = fmaf(Z.x, wx, -Z.y * wy);
+        const float ty = fmaf(Z.x, wy, Z.y * wx);
+        const float sq_x = (wx - wy) * (wx + wy);
+        const float sq_y = 2.0f * wx * wy;
+        const float nx = fmaf(2.0f, tx, fmaf(S, sq_x, Dx));
+        const float ny = fmaf(2.0f, ty, fmaf(S, sq_y, Dy));
+        wx = nx;
+        wy = ny;
+    } else if (FT == kFtShip) {
+        const float sx = Z.x >= 0.0f ? 1.0f : -1.0f, sy = Z.y >= 0.0f ? 1.0f : -1.0f;
+        float ddx = sx * wx, ddy = sy * wy;
+        const bool ux = !(fabsf(wx * S) < 0.5f * fabsf(Z.x));
+        const bool uy = !(fabsf(wy * S) < 0.5f * fabsf(Z.y));
+        if (ux || uy) {
+            const double2 Z64 = __ldg(reinterpret_cast<const double2*>(orb_k));
+            const double se = ldexp(1.0, e);
+            if (ux) {
+                const double x = wx, s = Z64.x >= 0.0 ? 1.0 : -1.0;
+                ddx = (Z64.x + x * se) * s >= 0.0 ? (float)(s * x) : (float)(-s * (ldexp(2.0 * Z64.x, -e) + x));
+            }
+            if (uy) {
+                const double y = wy, s = Z64.y >= 0.0 ? 1.0 : -1.0;
+                ddy = (Z64.y + y * se) * s >= 0.0 ? (float)(s * y) : (float)(-s * (ldexp(2.0 * Z64.y, -e) + y));
+            }
+        }
+        const float nx = fmaf(2.0f, fmaf(Z.x, wx, -Z.y * wy), fmaf(S, (wx - wy) * (wx + wy), Dx));
+        const float ny = fmaf(2.0f, fmaf(fabsf(Z.x), ddy, fmaf(fabsf(Z.y), ddx, S * (ddx * ddy))), -Dy);
+        wx = nx;
+        wy = ny;
+    } else {
+        float pr = wx, pi = wy, qr = Z.x, qi = Z.y;
+        for (int t = 0; t < p.gen_n - 1; ++t) {
+            const float sr = fmaf(S, pr, qr), si = fmaf(S, pi, qi);
+            const float npr = fmaf(pr, Z.x, fmaf(-pi, Z.y, fmaf(sr, wx, -si * wy)));
+            const float npi = fmaf(pr, Z.y, fmaf(pi, Z.x, fmaf(sr, wy, si * wx)));
+            const float nqr = fmaf(qr, Z.x, -qi * Z.y), nqi = fmaf(qr, Z.y, qi * Z.x);
+            pr = npr;
+            pi = npi;
+            qr = nqr;
+            qi = nqi;
+        }
+        const float nx = fmaf(kr, wx, fmaf(-ki, wy, pr + Dx));
+        const float ny = fmaf(kr, wy, fmaf(ki, wx, pi + Dy));
+        wx = nx;
+        wy = ny;
+    }
+}
+
+// One FP64 direct step z <- f(z) + c of stage 2 (zx2, zy2 the squares already formed).
+template <int FT>
+__device__ __forceinline__ void fe32_direct_step(const ApFrameParams& p, double& zx, double& zy, double zx2,
+                                                 double zy2, double cx, double cy) {
+    if (FT == kFtQuad) {
+        zy = 2.0 * zx * zy + cy;
+        zx = zx2 - zy2 + cx;
+    } else if (FT == kFtShip) {
+        zy = 2.0 * fabs(zx) * fabs(zy) - cy;
+        zx = zx2 - zy2 + cx;
+    } else {
+        double zr = zx, zi = zy;
+        for (int t = 0; t < p.gen_n - 1; ++t) {
+            const double nr = zr * zx - zi * zy, ni = zr * zy + zi * zx;
+            zr = nr;
+            zi = ni;
+        }
+        const double kzr = p.gen_kr * zx - p.gen_ki * zy;
+        const double kzi = p.gen_kr * zy + p.gen_ki * zx;
+        zx = zr + kzr + cx;
+        zy = zi + kzi + cy;
+    }
+}
+
+// One pixel per thread, blocks of 8x8 pixels (warps of 8x4): a block lives as long as
+// its slowest pixel, so small blocks let an SM start new ones as each ends.
+template <int FT, bool BLA, bool REBASE>
+__global__ void __launch_bounds__(64, 16) fe32_coarse_kernel(const ApFrameParams p,
                                                              const ApFrameBuffers b) {
     constexpr int bias = kRadiusBias;
-    const int i = blockIdx.x * 16 + (threadIdx.x & 15);
-    const int j = blockIdx.y * 16 + (threadIdx.x >> 4);
+    const int i = blockIdx.x * 8 + (threadIdx.x & 7);
+    const int j = blockIdx.y * 8 + (threadIdx.x >> 3);
     if (i >= p.width || j >= p.height) return;
     const int idx = j * p.width + i;
     if (p.rebase_pass > 0 && b.glitch_in[idx] == 0) return;
@@ -142,10 +275,11 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
     const double sub_j = (double)(j * p.factor) + sub_offset;
     const double dcy_n = (p.ref_py - sub_j) * p.dy_hi;
     const double dcx_n = (sub_i - p.ref_px) * p.dx_hi;
-    const bool julia = (p.fractal_type == 2);
+    const bool julia = (p.fractal_type == 2 || p.fractal_type == 3);
     const int ec = -p.e_scale;
     const float dcmx = (float)dcx_n, dcmy = (float)dcy_n;
     const float pdx = julia ? 0.0f : dcmx, pdy = julia ? 0.0f : dcmy;
+    const float kr = (float)p.gen_kr, ki = (float)p.gen_ki;
 
     float wx = julia ? dcmx : 0.0f, wy = julia ? dcmy : 0.0f;
     int e = ec;
@@ -170,18 +304,62 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
     };
     rescale();
 
-    const bool strict = p.strict_glitch > 0;
-    int k = 0, glitch = 0, leaps = 0, skipped = 0, k2 = -1;
+    const bool strict = !REBASE && p.strict_glitch > 0;
+    // k: the reference index (and, without rebasing, the pixel's iterations).  With
+    // rebasing the pixel's iterations are k + (max_iter - lim): a restart moves lim.
+    int k = 0, lim = max_iter, glitch = 0, leaps = 0, skipped = 0, k2 = -1, rebases = 0;
     const int max_level = p.bla_levels - 1;
     SampleOut o = interior_sample();
     bool finished = false;
     const double inv_ln = inv_ln_for(p.fractal_type, p.gen_n);
 
-    while (k < ref_len) {
+    while (REBASE ? (k < lim) : (k < ref_len)) {
         const float4 Z = __ldg(orb32 + k);
         const float wm2 = wx * wx + wy * wy;
-        // Escape and Pauldelbrot tests can only fire once the delta is not negligible.
-        if (e >= -40 || (strict && k > 15 && e >= -75)) {
+        if (REBASE) {
+            // z is formed in FP64 where a test can fire: at the end of the reference, at a
+            // close approach, near escape, or where |dz| > |Z| / 2 (|Z + dz| < |dz| needs it)
+            bool test = k == ref_len || Z.w != 0.0f || (e >= -53 && wm2 * (S * S) > 0.2f * Z.z);
+            if (!test && e >= -40) {
+                const float zx = Z.x + wx * S, zy = Z.y + wy * S;
+                test = zx * zx + zy * zy > 65535.0f;
+            }
+            if (test) {
+                const double2 Z64 = __ldg(reinterpret_cast<const double2*>(orb + k));
+                const double sc = ldexp(1.0, e), x = wx, y = wy;
+                const double ax = Z64.x + x * sc, ay = Z64.y + y * sc;
+                const double mag2 = ax * ax + ay * ay;
+                if (!(mag2 <= kBailout)) {
+                    const int kk = k + (max_iter - lim);
+                    if (isnan(mag2)) {
+                        o.s = (float)kk;
+                        o.s64 = (double)kk;
+                        o.k = kk;
+                        glitch = 1;
+                    } else {
+                        o = escaped_sample(kk, mag2, inv_ln);
+                    }
+                    finished = true;
+                    break;
+                }
+                // |z| < |dz| compared in units of 2^e, so that neither side underflows
+                double bx = ldexp(Z64.x, -e) + x, by = ldexp(Z64.y, -e) + y;
+                if ((k == ref_len && k > 0) || bx * bx + by * by < x * x + y * y) {
+                    if (!(fabs(bx) + fabs(by) < 1e300)) {  // a reference that ended far above the delta
+                        bx = ax;
+                        by = ay;
+                        e = 0;
+                    }
+                    renorm_to_float(bx, by, wx, wy, e);
+                    rescale();
+                    lim -= k;
+                    k = 0;
+                    ++rebases;
+                    continue;
+                }
+            }
+        } else if (e >= -40 || (strict && k > 15 && e >= -75)) {
+            // Escape and Pauldelbrot tests can only fire once the delta is not negligible.
             const float zx = Z.x + wx * S, zy = Z.y + wy * S;
             const float zm2 = zx * zx + zy * zy;
             const bool near_escape = e >= -40 && zm2 > 65535.0f;
@@ -208,6 +386,7 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
             const double* row = Rs + (size_t)k * 16;
             if (dzs < __ldg(row)) {
                 int lo = 0, hi = max_level;
+                if (REBASE) hi = min(hi, 31 - __clz(lim - k));  // the leap ends at or before max_iter
 #pragma unroll 4
                 for (int it = 0; it < 4; ++it) {
                     if (lo < hi) {
@@ -229,9 +408,8 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
                     wy = ny;
                     e += c.ea;
                 } else {  // FP64 slow path: the dc term's scale leaves the float range
-                    const double f = ldexp(1.0, fe);
-                    const double bx = ((double)c.br * pdx - (double)c.bi * pdy) * f;
-                    const double by = ((double)c.br * pdy + (double)c.bi * pdx) * f;
+                    const double bx = ldexp((double)c.br * pdx - (double)c.bi * pdy, fe);
+                    const double by = ldexp((double)c.br * pdy + (double)c.bi * pdx, fe);
                     const double nx = (double)c.ar * wx - (double)c.ai * wy + bx;
                     const double ny = (double)c.ar * wy + (double)c.ai * wx + by;
                     e += c.ea;
@@ -245,32 +423,26 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
             }
         }
         if (Z.w != 0.0f || ec - e > 120) {
-            // FP64 slow path: w' = 2 Z w + 2^e w^2 + dcm 2^(ec - e) on the FP64 orbit.
+            // FP64 slow path: the same step on the FP64 orbit, dc term dcm 2^(ec - e).
             const double2 Z64 = __ldg(reinterpret_cast<const double2*>(orb + k));
-            const double x = wx, y = wy;
-            const double se = ldexp(1.0, e), sd = ldexp(1.0, ec - e);
-            const double nx = 2.0 * (Z64.x * x - Z64.y * y) + se * (x - y) * (x + y) + (double)pdx * sd;
-            const double ny = 2.0 * (Z64.x * y + Z64.y * x) + se * 2.0 * x * y + (double)pdy * sd;
+            double nx, ny;
+            fe32_step_fp64<FT>(p, Z64.x, Z64.y, wx, wy, e, ldexp((double)pdx, ec - e),
+                               ldexp((double)pdy, ec - e), nx, ny);
             renorm_to_float(nx, ny, wx, wy, e);
             rescale();
             ++k;
             continue;
         }
-        // w' = 2 Z w + S w^2 + D
-        const float tx = fmaf(Z.x, wx, -Z.y * wy);
-        const float ty = fmaf(Z.x, wy, Z.y * wx);
-        const float sq_x = (wx - wy) * (wx + wy);
-        const float sq_y = 2.0f * wx * wy;
-        const float nx = fmaf(2.0f, tx, fmaf(S, sq_x, Dx));
-        const float ny = fmaf(2.0f, ty, fmaf(S, sq_y, Dy));
-        wx = nx;
-        wy = ny;
+        fe32_step<FT>(p, Z, orb + k, wx, wy, e, S, Dx, Dy, kr, ki);
         const float mx = fmaxf(fabsf(wx), fabsf(wy));
         if (mx > 65536.0f || (mx < 1.52587890625e-05f && mx > 0.0f)) rescale();
         ++k;
     }
 
-    if (!finished) {
+    if (REBASE) {
+        if (!finished) k = max_iter;  // k + (max_iter - lim) with k == lim
+        else k = o.k;
+    } else if (!finished) {
         // Stage 2: FP64 direct iteration from Z_ref_len + dz, c = ref_c + dc.
         const double2 Zend = __ldg(reinterpret_cast<const double2*>(orb + ref_len));
         const double sc = ldexp(1.0, e);
@@ -278,7 +450,8 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
         const double dct_x = dcx_n * ldexp(1.0, ec), dct_y = dcy_n * ldexp(1.0, ec);
         const double cx = julia ? p.julia_cx_hi : p.ref_cx + dct_x;
         const double cy = julia ? p.julia_cy_hi : p.ref_cy + dct_y;
-        if (ref_len < max_iter) glitch = 1;
+        // a pixel that escapes together with the reference (at k = ref_len) is not glitched
+        if (!(zx * zx + zy * zy > kBailout) && ref_len < max_iter) glitch = 1;
         k2 = k;
         const bool nan_guard = (p.flags & AP_FLAG_NAN_GUARD) != 0;
         while (k < max_iter) {
@@ -295,8 +468,7 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
                 o = escaped_sample(k, mag2, inv_ln);
                 break;
             }
-            zy = 2.0 * zx * zy + cy;
-            zx = zx2 - zy2 + cx;
+            fe32_direct_step<FT>(p, zx, zy, zx2, zy2, cx, cy);
             ++k;
         }
     }
@@ -308,8 +480,22 @@ __global__ void __launch_bounds__(256, 4) fe32_coarse_kernel(const ApFrameParams
     if (b.counters) {
         const int it1 = (k2 < 0 ? k_end : k2) - skipped;
         const int it2 = k2 < 0 ? 0 : k_end - k2;
-        reinterpret_cast<int4*>(b.counters)[idx] = make_int4(it1, leaps, it2, 0);
+        reinterpret_cast<int4*>(b.counters)[idx] = make_int4(it1, leaps, it2, rebases);
     }
+}
+
+template <int FT>
+static void launch_fe32_ft(const ApFrameParams& p, const ApFrameBuffers& b, bool bla, bool rebase,
+                           cudaStream_t st) {
+    const dim3 grid((p.width + 7) / 8, (p.height + 7) / 8);
+    if (bla && rebase)
+        fe32_coarse_kernel<FT, true, true><<<grid, 64, 0, st>>>(p, b);
+    else if (bla)
+        fe32_coarse_kernel<FT, true, false><<<grid, 64, 0, st>>>(p, b);
+    else if (rebase)
+        fe32_coarse_kernel<FT, false, true><<<grid, 64, 0, st>>>(p, b);
+    else
+        fe32_coarse_kernel<FT, false, false><<<grid, 64, 0, st>>>(p, b);
 }
 
 int launch_fe32(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st) {
@@ -320,19 +506,27 @@ int launch_fe32(const ApFrameParams& p, const ApFrameBuffers& b, cudaStream_t st
         set_error("AP_TIER_FLOATEXP32 serves coarse passes without in-kernel colour (set AP_FLAG_NO_RGB)");
         return AP_E_INVALID;
     }
-    if (p.fractal_type != 0 && p.fractal_type != 2) {
-        set_error("AP_TIER_FLOATEXP32 serves Mandelbrot and Julia (fractal_type 0, 2)");
+    const int ft = p.fractal_type;
+    const bool rebase = (p.flags & AP_FLAG_REBASE) != 0;
+    if (ft < 0 || ft > 4) {
+        set_error("AP_TIER_FLOATEXP32: fractal_type 0..4");
+        return AP_E_INVALID;
+    }
+    if (rebase && (ft == 2 || ft == 3 || p.rebase_pass > 0 || p.ref_len < 1)) {
+        set_error("AP_FLAG_REBASE serves fractal types 0, 1 and 4 in one pass (rebase_pass 0, ref_len >= 1)");
         return AP_E_UNSUPPORTED;
     }
     if (!b.orbit_packed || (bla && !b.bla_packed) || p.bla_levels > 16 || p.bbsa_skip > 0) {
         set_error("AP_TIER_FLOATEXP32 needs ap_pack_fe32 inputs (orbit_packed, bla_packed) and no series start");
         return AP_E_INVALID;
     }
-    dim3 grid((p.width + 15) / 16, (p.height + 15) / 16);
-    if (bla)
-        fe32_coarse_kernel<true><<<grid, 256, 0, st>>>(p, b);
+    // the Burning Ship formulas take no leaps (as the FloatExp tier's reference kernels)
+    if (ft == 0 || ft == 2)
+        launch_fe32_ft<kFtQuad>(p, b, bla, rebase, st);
+    else if (ft == 1 || ft == 3)
+        launch_fe32_ft<kFtShip>(p, b, false, rebase, st);
     else
-        fe32_coarse_kernel<false><<<grid, 256, 0, st>>>(p, b);
+        launch_fe32_ft<kFtMulti>(p, b, bla, rebase, st);
     return check_launch("fe32_coarse_kernel");
 }
 

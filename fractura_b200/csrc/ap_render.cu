@@ -199,8 +199,8 @@ int validate_frame(const ApFrameParams* p, const ApFrameBuffers* b, int hist_res
         return AP_E_INVALID;
     }
     if (p->flags & AP_FLAG_REBASE) {
-        if (p->tier != AP_TIER_PERTURB) {
-            set_error("AP_FLAG_REBASE serves the FP64-delta tier (AP_TIER_PERTURB)");
+        if (p->tier != AP_TIER_PERTURB && p->tier != AP_TIER_FLOATEXP32) {
+            set_error("AP_FLAG_REBASE serves the FP64-delta and FP32 FloatExp tiers (AP_TIER_PERTURB, AP_TIER_FLOATEXP32)");
             return AP_E_UNSUPPORTED;
         }
         if (p->fractal_type == 2 || p->fractal_type == 3) {

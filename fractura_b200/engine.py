@@ -335,8 +335,8 @@ def render_frame_ssaa(target_w, target_h=None, max_iter=None, center_x_dec=None,
     arithmetic profile ("ref_cpu" default, "ref_cuda", or "fast": the engine's own
     fused form, for glitch_mode "One-Pass Rebasing" only), ``delta_form``
     the perturbation delta arithmetic: "fp64" (default, the reference's) or
-    "fp32" (FP32 mantissas with integer exponents on coarse passes of
-    Mandelbrot/Julia frames), ``bla_form`` the chained-BLA table: "reference"
+    "fp32" (FP32 mantissas with integer exponents on the coarse passes of
+    perturbation frames, every formula), ``bla_form`` the chained-BLA table: "reference"
     (default: the reference's merge at ``bbsa_tol``) or "accurate" (the
     dc-aware merge at ``ACCURATE_BLA_EPS``).  The smooth iteration map is left in
     ``d_iter_buf`` (and copied to ``h_iter_buf`` when one is given).

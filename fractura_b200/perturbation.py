@@ -351,7 +351,7 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
             e_scale = 0
         # FP32 FloatExp tier: the same spacing in units of 2^-E (E from config.py:51).
         fe32 = None
-        if fp32_deltas and fractal_type in (0, 2):
+        if fp32_deltas:
             fe_e = compute_floatexp_scale(plot_width_dec)
             fe32 = (float(plot_width_dec * (Decimal(2) ** fe_e) / Decimal(max(1, W - 1))) / float(factor),
                     float(plot_height_dec * (Decimal(2) ** fe_e) / Decimal(max(1, H - 1))) / float(factor),
@@ -359,10 +359,12 @@ def render_perturbation_frame(p, fr, lut, stream_h, st, *, W, H, factor, max_ite
     one_pass = ONE_PASS_REBASING in glitch_mode
     if arith_code == abi.AP_ARITH_FAST and not one_pass:
         raise ValueError(f"arith='fast' serves glitch_mode {ONE_PASS_REBASING!r} only")
-    if one_pass and (tier != abi.AP_TIER_PERTURB or fractal_type in (2, 3) or fp32_deltas):
+    # the FP32 form rebases at every depth; below 1e-300 its SSAA edge pass would need
+    # FP64 FloatExp rebasing, which is not built
+    if one_pass and (fractal_type in (2, 3) or (tier != abi.AP_TIER_PERTURB and (not fp32_deltas or factor > 1))):
         raise NotImplementedError(
-            f"{ONE_PASS_REBASING!r} serves FP64-delta frames (widths 1e-300 .. 1e-12) of "
-            "Mandelbrot, Burning Ship and Multibrot")
+            f"{ONE_PASS_REBASING!r} serves Mandelbrot, Burning Ship and Multibrot frames: FP64 deltas "
+            "(widths 1e-300 .. 1e-12), or delta_form='fp32' (any depth; factor 1 below 1e-300)")
     strict = 0 if one_pass else (1 if ("Auto Rebasing" in glitch_mode or "Strict" in glitch_mode
                                        or "Pauldelbrot" in glitch_mode) else 0)
     LAST_FRAME_STATS.update(h2d_bytes=0, d2h_bytes=0, rebase_passes=0, strict_pixels=0, strict_tier=0)

@@ -39,7 +39,8 @@ extern "C" {
 #define AP_TIER_DD 1        /* direct double-double iteration   (cuda_kernels.py:321) */
 #define AP_TIER_PERTURB 2   /* FP64-delta perturbation (+BLA)   (cuda_kernels.py:422, :594) */
 #define AP_TIER_FLOATEXP 3  /* FP64-mantissa FloatExp deltas    (cuda_kernels.py:819, :1102) */
-#define AP_TIER_FLOATEXP32 4 /* FP32-mantissa FloatExp deltas (this engine's fast form) */
+#define AP_TIER_FLOATEXP32 4 /* FP32-mantissa FloatExp deltas (this engine's fast form; all five
+                                formulas, coarse passes; with or without AP_FLAG_REBASE) */
 
 /* Arithmetic profiles.  The escape step of a boundary pixel depends on which
  * multiply-adds are fused, so the engine can reproduce either reference. */
@@ -61,7 +62,7 @@ extern "C" {
 #define AP_FLAG_ITER_LAST_SUB 8u   /* supersample passes write the last sub-sample to the iter map */
 #define AP_FLAG_MAP_FUSED 16u      /* pixel -> c mapping as fma(i, dx, x_min) */
 #define AP_FLAG_HIST_COLOUR 32u    /* colour through the CDF table (scheme 11 resolve passes) */
-/* One-pass rebasing (AP_TIER_PERTURB, fractal types 0, 1, 4; no counterpart in the
+/* One-pass rebasing (AP_TIER_PERTURB and AP_TIER_FLOATEXP32, fractal types 0, 1, 4; no counterpart in the
  * reference, which rebases by whole re-render passes, math_core/engine.py:1890-2113).
  * Each pixel keeps its own iteration count n and a reference index m.  When
  * |Z_m + dz| < |dz| (the delta has outgrown the value it perturbs) or the reference

@@ -369,6 +369,7 @@ static Sample pert_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, do
                              double sub_j);
 static Sample floatexp_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i,
                                  double sub_j);
+static Sample fe32_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i, double sub_j);
 
 /* Sub-sample coordinates (sub_i, sub_j) -> sample, as each unified kernel maps them. */
 static Sample sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i, double sub_j) {
@@ -388,6 +389,8 @@ static Sample sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double 
         return dd_sample_at(p, sub_i, sub_j);
     case AP_TIER_FLOATEXP:
         return floatexp_sample_at(p, b, sub_i, sub_j);
+    case AP_TIER_FLOATEXP32:
+        return fe32_sample_at(p, b, sub_i, sub_j);
     default:
         return pert_sample_at(p, b, sub_i, sub_j);
     }
@@ -1183,6 +1186,371 @@ static Sample floatexp_sample_at(const ApFrameParams* p, const ApFrameBuffers* b
 }
 
 /* ------------------------------------------------------------------------- */
+/* FP32-mantissa FloatExp form (AP_TIER_FLOATEXP32).  The engine's own form,  */
+/* with no counterpart in the reference: restated here from its definition so */
+/* that device frames can be compared with it bit for bit.                    */
+/*                                                                            */
+/* The delta is w 2^e, w a complex float32 renormalised so that               */
+/* max(|w_re|, |w_im|) is in [1, 2) whenever it leaves [2^-16, 2^16];          */
+/* delta_c = dcm 2^-E with dcm = (float) of the pixel offset in units of 2^-E.*/
+/* A step is evaluated in float32 (products rounded one by one, fmaf where the */
+/* form fuses) from the float copy of Z, with S = 2^e and D = dcm 2^(-E-e) as */
+/* floats; it is evaluated in FP64 on the FP64 orbit value instead where Z is  */
+/* a close approach (|Z|^2 < 2^-100) or the dc term's scale exceeds 2^120.     */
+/* Tests on z = Z + dz (escape, Pauldelbrot, one-pass rebasing, Burning Ship's */
+/* sign of each component) are decided in FP64 at the steps where a float    */
+/* screen says they can fire; the screens are part of the form.  Leaps use    */
+/* the chained-BLA table with each coefficient split into a float mantissa    */
+/* pair and an exponent, and radii compared as r^2 2^600.                     */
+/* ------------------------------------------------------------------------- */
+static float fe_exp2i_f(int n) { /* 2^n as float: 0 below 2^-126, 2^127 above */
+    if (n > 127) n = 127;
+    if (n < -126) return 0.0f;
+    union { uint32_t u; float f; } v;
+    v.u = (uint32_t)(n + 127) << 23;
+    return v.f;
+}
+
+static double fe_exp2i_d(int n) { /* 2^n as double: 0 below 2^-1022, inf above 2^1023 */
+    if (n < -1022) return 0.0;
+    if (n > 1023) return INFINITY;
+    union { uint64_t u; double d; } v;
+    v.u = (uint64_t)(n + 1023) << 52;
+    return v.d;
+}
+
+static int fe_ilogb_max(float x, float y) { /* biased exponent field of max(|x|, |y|), minus 127 */
+    union { float f; uint32_t u; } v;
+    v.f = fmaxf(fabsf(x), fabsf(y));
+    return (int)((v.u >> 23) & 0xff) - 127;
+}
+
+/* A double pair as one float mantissa pair (larger component in [1, 2)) and an exponent. */
+static void fe_split(double re, double im, float* mr, float* mi, int* e) {
+    const double m = fmax(fabs(re), fabs(im));
+    if (!(m > 0.0) || !isfinite(m)) {
+        *mr = *mi = 0.0f;
+        *e = 0;
+        return;
+    }
+    union { double d; uint64_t u; } v;
+    v.d = m;
+    int ex = (int)((v.u >> 52) & 0x7ff) - 1023;
+    if (ex < -1022) ex = ilogb(m);
+    const double s = ldexp(1.0, -ex);
+    *mr = (float)(re * s);
+    *mi = (float)(im * s);
+    *e = ex;
+}
+
+/* (x, y) 2^e renormalised into a float pair; zero and non-finite pairs keep e. */
+static void fe_renorm(double x, double y, float* wx, float* wy, int* e) {
+    const double m = fmax(fabs(x), fabs(y));
+    if (!(m > 0.0) || !isfinite(m)) {
+        *wx = (float)x;
+        *wy = (float)y;
+        return;
+    }
+    const int ex = ilogb(m);
+    const double f = ldexp(1.0, -ex);
+    *wx = (float)(x * f);
+    *wy = (float)(y * f);
+    *e += ex;
+}
+
+typedef struct {
+    float wx, wy, S, Dx, Dy;
+    int e, ec;
+    float pdx, pdy;
+    double P2;
+} FeState;
+
+/* Renormalise w when it is not zero, then refresh S, D and the radius scale 2^(2e + 600). */
+static void fe_rescale(FeState* s) {
+    if (s->wx != 0.0f || s->wy != 0.0f) {
+        const int ex = fe_ilogb_max(s->wx, s->wy);
+        if (ex != 0) {
+            const float f = fe_exp2i_f(-ex);
+            s->wx *= f;
+            s->wy *= f;
+            s->e += ex;
+        }
+    }
+    s->S = fe_exp2i_f(s->e);
+    const float dsc = fe_exp2i_f(s->ec - s->e);
+    s->Dx = s->pdx * dsc;
+    s->Dy = s->pdy * dsc;
+    s->P2 = fe_exp2i_d(2 * s->e + 600);
+}
+
+/* The FP64 step of the slow path, in units of 2^e; (cx, cy) the dc term in those units. */
+static void fe_step_fp64(const ApFrameParams* p, int form, double Zx, double Zy, double x, double y, int e,
+                         double cx, double cy, double* nx, double* ny) {
+    const double se = ldexp(1.0, e);
+    if (form == 0) {
+        *nx = 2.0 * (Zx * x - Zy * y) + se * (x - y) * (x + y) + cx;
+        *ny = 2.0 * (Zx * y + Zy * x) + se * 2.0 * x * y + cy;
+    } else if (form == 1) {
+        const double sx = Zx >= 0.0 ? 1.0 : -1.0, sy = Zy >= 0.0 ? 1.0 : -1.0;
+        const double ddx = (Zx + x * se) * sx >= 0.0 ? sx * x : -sx * (ldexp(2.0 * Zx, -e) + x);
+        const double ddy = (Zy + y * se) * sy >= 0.0 ? sy * y : -sy * (ldexp(2.0 * Zy, -e) + y);
+        *nx = 2.0 * (Zx * x - Zy * y) + se * (x - y) * (x + y) + cx;
+        *ny = 2.0 * (fabs(Zx) * ddy + fabs(Zy) * ddx + se * ddx * ddy) - cy;
+    } else {
+        double pr = x, pi = y, qr = Zx, qi = Zy;
+        for (int t = 0; t < p->gen_n - 1; t++) {
+            const double sr = se * pr + qr, si = se * pi + qi;
+            const double npr = (pr * Zx - pi * Zy) + (sr * x - si * y);
+            const double npi = (pr * Zy + pi * Zx) + (sr * y + si * x);
+            const double nqr = qr * Zx - qi * Zy, nqi = qr * Zy + qi * Zx;
+            pr = npr;
+            pi = npi;
+            qr = nqr;
+            qi = nqi;
+        }
+        *nx = pr + (p->gen_kr * x - p->gen_ki * y) + cx;
+        *ny = pi + (p->gen_kr * y + p->gen_ki * x) + cy;
+    }
+}
+
+/* The float32 step: Zf the float copy of the orbit value, (Zx, Zy) the FP64 one (read
+ * by Burning Ship's sign test where |dz_x| >= |Z_x| / 2 in float). */
+static void fe_step_f32(const ApFrameParams* p, int form, float Zfx, float Zfy, double Zx, double Zy,
+                        FeState* s, float kr, float ki) {
+    const float wx = s->wx, wy = s->wy, S = s->S;
+    if (form == 0) {
+        const float tx = fmaf(Zfx, wx, -Zfy * wy);
+        const float ty = fmaf(Zfx, wy, Zfy * wx);
+        const float sq_x = (wx - wy) * (wx + wy);
+        const float sq_y = 2.0f * wx * wy;
+        s->wx = fmaf(2.0f, tx, fmaf(S, sq_x, s->Dx));
+        s->wy = fmaf(2.0f, ty, fmaf(S, sq_y, s->Dy));
+    } else if (form == 1) {
+        const float sx = Zfx >= 0.0f ? 1.0f : -1.0f, sy = Zfy >= 0.0f ? 1.0f : -1.0f;
+        float ddx = sx * wx, ddy = sy * wy;
+        const int ux = !(fabsf(wx * S) < 0.5f * fabsf(Zfx));
+        const int uy = !(fabsf(wy * S) < 0.5f * fabsf(Zfy));
+        const double se = ldexp(1.0, s->e);
+        if (ux) {
+            const double x = wx, g = Zx >= 0.0 ? 1.0 : -1.0;
+            ddx = (Zx + x * se) * g >= 0.0 ? (float)(g * x) : (float)(-g * (ldexp(2.0 * Zx, -s->e) + x));
+        }
+        if (uy) {
+            const double y = wy, g = Zy >= 0.0 ? 1.0 : -1.0;
+            ddy = (Zy + y * se) * g >= 0.0 ? (float)(g * y) : (float)(-g * (ldexp(2.0 * Zy, -s->e) + y));
+        }
+        s->wx = fmaf(2.0f, fmaf(Zfx, wx, -Zfy * wy), fmaf(S, (wx - wy) * (wx + wy), s->Dx));
+        s->wy = fmaf(2.0f, fmaf(fabsf(Zfx), ddy, fmaf(fabsf(Zfy), ddx, S * (ddx * ddy))), -s->Dy);
+    } else {
+        float pr = wx, pi = wy, qr = Zfx, qi = Zfy;
+        for (int t = 0; t < p->gen_n - 1; t++) {
+            const float sr = fmaf(S, pr, qr), si = fmaf(S, pi, qi);
+            const float npr = fmaf(pr, Zfx, fmaf(-pi, Zfy, fmaf(sr, wx, -si * wy)));
+            const float npi = fmaf(pr, Zfy, fmaf(pi, Zfx, fmaf(sr, wy, si * wx)));
+            const float nqr = fmaf(qr, Zfx, -qi * Zfy), nqi = fmaf(qr, Zfy, qi * Zfx);
+            pr = npr;
+            pi = npi;
+            qr = nqr;
+            qi = nqi;
+        }
+        s->wx = fmaf(kr, wx, fmaf(-ki, wy, pr + s->Dx));
+        s->wy = fmaf(kr, wy, fmaf(ki, wx, pi + s->Dy));
+    }
+}
+
+/* Stage 2's direct FP64 step z <- f(z) + c. */
+static void fe_direct_step(const ApFrameParams* p, int form, double* zx, double* zy, double zx2, double zy2,
+                           double cx, double cy) {
+    if (form == 0) {
+        *zy = 2.0 * *zx * *zy + cy;
+        *zx = zx2 - zy2 + cx;
+    } else if (form == 1) {
+        *zy = 2.0 * fabs(*zx) * fabs(*zy) - cy;
+        *zx = zx2 - zy2 + cx;
+    } else {
+        double zr = *zx, zi = *zy;
+        for (int t = 0; t < p->gen_n - 1; t++) {
+            const double nr = zr * *zx - zi * *zy, ni = zr * *zy + zi * *zx;
+            zr = nr;
+            zi = ni;
+        }
+        const double kzr = p->gen_kr * *zx - p->gen_ki * *zy;
+        const double kzi = p->gen_kr * *zy + p->gen_ki * *zx;
+        *zx = zr + kzr + cx;
+        *zy = zi + kzi + cy;
+    }
+}
+
+/* One sample of the FP32 form.  Without AP_FLAG_REBASE: one reference, Pauldelbrot flags
+ * (strict_glitch), FP64 direct iteration after the reference ends.  With it (fractal types
+ * 0, 1, 4): when |Z_m + dz| < |dz| or the reference has ended, dz <- Z_m + dz and m <- 0. */
+static Sample fe32_sample_at(const ApFrameParams* p, const ApFrameBuffers* b, double sub_i, double sub_j) {
+    const int ft = p->fractal_type;
+    const int form = (ft == 0 || ft == 2) ? 0 : ((ft == 1 || ft == 3) ? 1 : 4);
+    const int rebase = (p->flags & AP_FLAG_REBASE) != 0;
+    const int bla = p->bla_levels > 1 && b->bla != NULL && form != 1;
+    const int ref_len = p->ref_len, max_iter = p->max_iter, levels = p->bla_levels;
+    const double* re = b->ref_re;
+    const double* im = b->ref_im;
+    const double* T = b->bla;
+    const size_t L = (size_t)ref_len;
+    const double dcy_n = (p->ref_py - sub_j) * p->dy_hi;
+    const double dcx_n = (sub_i - p->ref_px) * p->dx_hi;
+    const int julia = ft == 2 || ft == 3;
+    const float dcmx = (float)dcx_n, dcmy = (float)dcy_n;
+    const float kr = (float)p->gen_kr, ki = (float)p->gen_ki;
+    FeState s;
+    s.ec = -p->e_scale;
+    s.e = s.ec;
+    s.pdx = julia ? 0.0f : dcmx;
+    s.pdy = julia ? 0.0f : dcmy;
+    s.wx = julia ? dcmx : 0.0f;
+    s.wy = julia ? dcmy : 0.0f;
+    fe_rescale(&s);
+    const int strict = !rebase && p->strict_glitch > 0;
+    const double inv_ln = inv_ln_for(ft, p->gen_n);
+    int k = 0, lim = max_iter, glitch = 0;
+    while (rebase ? (k < lim) : (k < ref_len)) {
+        const double Zx = re[k], Zy = im[k];
+        const double r2 = Zx * Zx + Zy * Zy;
+        const float Zfx = (float)Zx, Zfy = (float)Zy, Zfr2 = (float)r2;
+        const int close = r2 < 0x1p-100;
+        const float wm2 = s.wx * s.wx + s.wy * s.wy;
+        if (rebase) {
+            int test = k == ref_len || close || (s.e >= -53 && wm2 * (s.S * s.S) > 0.2f * Zfr2);
+            if (!test && s.e >= -40) {
+                const float zx = Zfx + s.wx * s.S, zy = Zfy + s.wy * s.S;
+                test = zx * zx + zy * zy > 65535.0f;
+            }
+            if (test) {
+                const double sc = ldexp(1.0, s.e), x = s.wx, y = s.wy;
+                const double ax = Zx + x * sc, ay = Zy + y * sc;
+                const double mag2 = ax * ax + ay * ay;
+                if (!(mag2 <= BAILOUT)) {
+                    const int kk = k + (max_iter - lim);
+                    if (isnan(mag2)) return glitch_at(kk);
+                    return escaped(kk, mag2, inv_ln);
+                }
+                double bx = ldexp(Zx, -s.e) + x, by = ldexp(Zy, -s.e) + y;
+                if ((k == ref_len && k > 0) || bx * bx + by * by < x * x + y * y) {
+                    if (!(fabs(bx) + fabs(by) < 1e300)) {
+                        bx = ax;
+                        by = ay;
+                        s.e = 0;
+                    }
+                    fe_renorm(bx, by, &s.wx, &s.wy, &s.e);
+                    fe_rescale(&s);
+                    lim -= k;
+                    k = 0;
+                    continue;
+                }
+            }
+        } else if (s.e >= -40 || (strict && k > 15 && s.e >= -75)) {
+            const float zx = Zfx + s.wx * s.S, zy = Zfy + s.wy * s.S;
+            const float zm2 = zx * zx + zy * zy;
+            const int near_escape = s.e >= -40 && zm2 > 65535.0f;
+            const int near_glitch = strict && k > 15 && zm2 < 2e-6f * Zfr2;
+            if (near_escape || near_glitch) {
+                const double sc = ldexp(1.0, s.e);
+                const double ax = Zx + (double)s.wx * sc, ay = Zy + (double)s.wy * sc;
+                const double mag2 = ax * ax + ay * ay;
+                if (mag2 > BAILOUT) {
+                    Sample o = escaped(k, mag2, inv_ln);
+                    o.glitch = glitch;
+                    return o;
+                }
+                if (near_glitch) {
+                    const double thr = r2 > 1e-8 ? 1e-6 * r2 : -1.0;
+                    if (mag2 < thr) glitch = 1;
+                }
+            }
+        }
+        if (bla && k < ref_len - 1) {
+            const double dzs = (double)wm2 * s.P2;
+#define FE_RADIUS(d) ((d) < levels ? ldexp(T[((size_t)(d) * L + k) * 5 + 4], 600) : 0.0)
+            if (dzs < FE_RADIUS(0)) {
+                int lo = 0, hi = levels - 1;
+                if (rebase) {
+                    const int cap = 31 - __builtin_clz((unsigned)(lim - k));
+                    if (hi > cap) hi = cap;
+                }
+                for (int it = 0; it < 4; it++) {
+                    if (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (dzs < FE_RADIUS(mid)) lo = mid;
+                        else hi = mid - 1;
+                    }
+                }
+                const double* c = T + ((size_t)lo * L + k) * 5;
+                float ar, ai, br, bi;
+                int ea, eb;
+                fe_split(c[0], c[1], &ar, &ai, &ea);
+                fe_split(c[2], c[3], &br, &bi, &eb);
+                const int fe = eb + s.ec - s.e - ea;
+                if (fe >= -120 && fe <= 120) {
+                    const float f = fe_exp2i_f(fe);
+                    const float bx = (br * s.pdx - bi * s.pdy) * f;
+                    const float by = (br * s.pdy + bi * s.pdx) * f;
+                    const float nx = fmaf(ar, s.wx, fmaf(-ai, s.wy, bx));
+                    const float ny = fmaf(ar, s.wy, fmaf(ai, s.wx, by));
+                    s.wx = nx;
+                    s.wy = ny;
+                    s.e += ea;
+                } else {
+                    const double bx = ldexp((double)br * s.pdx - (double)bi * s.pdy, fe);
+                    const double by = ldexp((double)br * s.pdy + (double)bi * s.pdx, fe);
+                    const double nx = (double)ar * s.wx - (double)ai * s.wy + bx;
+                    const double ny = (double)ar * s.wy + (double)ai * s.wx + by;
+                    s.e += ea;
+                    fe_renorm(nx, ny, &s.wx, &s.wy, &s.e);
+                }
+                fe_rescale(&s);
+                k += 1 << lo;
+                continue;
+            }
+#undef FE_RADIUS
+        }
+        if (close || s.ec - s.e > 120) {
+            double nx, ny;
+            fe_step_fp64(p, form, Zx, Zy, s.wx, s.wy, s.e, ldexp((double)s.pdx, s.ec - s.e),
+                         ldexp((double)s.pdy, s.ec - s.e), &nx, &ny);
+            fe_renorm(nx, ny, &s.wx, &s.wy, &s.e);
+            fe_rescale(&s);
+            k++;
+            continue;
+        }
+        fe_step_f32(p, form, Zfx, Zfy, Zx, Zy, &s, kr, ki);
+        const float mx = fmaxf(fabsf(s.wx), fabsf(s.wy));
+        if (mx > 65536.0f || (mx < 1.52587890625e-05f && mx > 0.0f)) fe_rescale(&s);
+        k++;
+    }
+    if (rebase) return interior();
+    /* stage 2: FP64 direct iteration from Z_ref_len + dz, c = ref_c + dc */
+    const double sc = ldexp(1.0, s.e);
+    double zx = re[ref_len] + (double)s.wx * sc, zy = im[ref_len] + (double)s.wy * sc;
+    const double dct_x = dcx_n * ldexp(1.0, s.ec), dct_y = dcy_n * ldexp(1.0, s.ec);
+    const double cx = julia ? p->julia_cx_hi : p->ref_cx + dct_x;
+    const double cy = julia ? p->julia_cy_hi : p->ref_cy + dct_y;
+    if (!(zx * zx + zy * zy > BAILOUT) && ref_len < max_iter) glitch = 1;
+    const int nan_guard = (p->flags & AP_FLAG_NAN_GUARD) != 0;
+    while (k < max_iter) {
+        const double zx2 = zx * zx, zy2 = zy * zy;
+        const double mag2 = zx2 + zy2;
+        if (nan_guard && (isnan(mag2) || isinf(mag2))) return glitch_at(k);
+        if (mag2 > BAILOUT) {
+            Sample o = escaped(k, mag2, inv_ln);
+            o.glitch = glitch;
+            return o;
+        }
+        fe_direct_step(p, form, &zx, &zy, zx2, zy2, cx, cy);
+        k++;
+    }
+    Sample o = interior();
+    o.glitch = glitch;
+    return o;
+}
+
+/* ------------------------------------------------------------------------- */
 /* Chained BLA table: _jit_build_bla_table (high_precision.py:1101-1238).     */
 /* The reference builds it with a fastmath Numba kernel; the fused forms      */
 /* below are the ones its compiled x86-64 code evaluates.                     */
@@ -1654,8 +2022,9 @@ typedef struct {
 static void pert_grid_row(void* vctx, int j) {
     const PertGridCtx* c = (const PertGridCtx*)vctx;
     for (int i = 0; i < c->W; i++) {
-        Sample o = c->p->tier == AP_TIER_FLOATEXP ? floatexp_sample_at(c->p, c->b, c->xs[i], c->ys[j])
-                                                  : pert_sample_at(c->p, c->b, c->xs[i], c->ys[j]);
+        Sample o = c->p->tier == AP_TIER_FLOATEXP     ? floatexp_sample_at(c->p, c->b, c->xs[i], c->ys[j])
+                   : c->p->tier == AP_TIER_FLOATEXP32 ? fe32_sample_at(c->p, c->b, c->xs[i], c->ys[j])
+                                                      : pert_sample_at(c->p, c->b, c->xs[i], c->ys[j]);
         size_t idx = (size_t)j * c->W + i;
         c->s32[idx] = o.s;
         if (c->b->s64) c->b->s64[idx] = o.s64;

@@ -99,12 +99,15 @@ class RebaseProgress:
 
 
 def pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max_passes=4,
-                      bla_eps=None):
+                      bla_eps=None, fp32=False):
     """A perturbation-tier frame through the oracle, pass for pass as the engine issues it,
     including the rebase loop.  ``m`` is a view dict (W, H, factor, max_iter, cx, cy,
     width, scheme, fractal_type, julia_cx, julia_cy, gen_n, gen_kr, gen_ki, bbsa_order,
     glitch_mode; optional bbsa_tol, offset, density, contrast).  ``bla_eps`` selects the
-    dc-aware BLA table (the engine's bla_form="accurate").  Returns (frame, rebase passes)."""
+    dc-aware BLA table (the engine's bla_form="accurate"); ``fp32`` the FP32-mantissa
+    FloatExp form on the coarse passes (the engine's delta_form="fp32": pixel offsets in
+    units of 2^-E with E from the view's width at every depth).  Returns (frame, rebase
+    passes)."""
     W, H, f, mi = m["W"], m["H"], m["factor"], m["max_iter"]
     ft, scheme = m["fractal_type"], m["scheme"]
     cpu_sem = arith == abi.AP_ARITH_REF_CPU
@@ -118,6 +121,19 @@ def pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max
         two_e = Decimal(2) ** e_scale
         dx_f = float(pw * two_e / Decimal(max(1, W - 1)))
         dy_f = float(ph * two_e / Decimal(max(1, H - 1)))
+        fe_e = compute_floatexp_scale(pw)
+        fe_dx = float(pw * (Decimal(2) ** fe_e) / Decimal(max(1, W - 1))) / float(f)
+        fe_dy = float(ph * (Decimal(2) ** fe_e) / Decimal(max(1, H - 1))) / float(f)
+
+    def coarse(q):
+        """The params of a coarse pass: the FP32 form's, when selected."""
+        if not fp32:
+            return q
+        c = abi.ApFrameParams.from_buffer_copy(q)
+        c.tier = abi.AP_TIER_FLOATEXP32
+        c.dx_hi, c.dy_hi, c.e_scale = fe_dx, fe_dy, int(fe_e)
+        c.bbsa_skip = 0
+        return c
     # the oracle's own Decimal restatement of the reference's orbit search (oracle/ref_orbit.py)
     bcx, bcy, bu, bv, re, im, rl = ref_orbit.find_reference(
         cxd, cyd, pw, ph, mi, ft=ft, julia_cx=m["julia_cx"], julia_cy=m["julia_cy"],
@@ -187,7 +203,7 @@ def pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max
 
     if scheme == 11:
         p.flags = uf | abi.AP_FLAG_NO_RGB
-        oracle.render_pass(p, fr)
+        oracle.render_pass(coarse(p), fr)
         oracle.histogram_cdf(fr, mi)
         oracle.colour(p, fr)
         if f > 1:
@@ -196,7 +212,7 @@ def pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max
             resolve(q)
     else:
         p.flags = uf
-        oracle.render_pass(p, fr)
+        oracle.render_pass(coarse(p), fr)
         if f > 1:
             oracle.edge_detect(fr, np.float32(edge_threshold))
             p.mode = abi.AP_MODE_EDGE
@@ -234,7 +250,7 @@ def pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max
             resolve(q)
         elif f == 1:
             q.mode, q.flags = abi.AP_MODE_COARSE, uf
-            oracle.render_pass(q, fr)
+            oracle.render_pass(coarse(q), fr)
         elif cpu_sem:
             q.mode, q.flags = abi.AP_MODE_COARSE, uf
             oracle.render_pass(q, fr)

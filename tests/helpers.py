@@ -69,11 +69,11 @@ def rgb_mismatch(a, b):
 
 
 def oracle_pert_frame(m, arith=abi.AP_ARITH_REF_CPU, lut=None, edge_threshold=0.35, max_passes=4,
-                      bla_eps=None):
+                      bla_eps=None, fp32=False):
     """A perturbation-tier frame through the oracle (oracle/frames.py), including the
-    rebase loop: (frame, rebase passes)."""
+    rebase loop: (frame, rebase passes).  ``fp32``: the FP32-mantissa form on coarse passes."""
     return frames.pert_frame(m, arith=arith, lut=lut, edge_threshold=edge_threshold, max_passes=max_passes,
-                             bla_eps=bla_eps)
+                             bla_eps=bla_eps, fp32=fp32)
 
 
 def probe_search(base_iter):
