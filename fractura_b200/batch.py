@@ -8,7 +8,9 @@ rendered by a single persistent kernel whose blocks take consecutive pixels from
 a shared counter, run them a quantum of loop steps at a time and compact the
 unfinished ones between quanta.  Each tile's values equal the per-frame coarse
 pass (ap_render_pass) for the same parameters.  arith="fast" gives one-pass tiles
-the fused step (the batch's single-reference tiles run "ref_cuda").
+the fused step (the batch's single-reference tiles run "ref_cuda"); a tile with
+delta_form="fp32" runs the FP32-mantissa FloatExp form (AP_TIER_FLOATEXP32), as the
+engine's coarse pass with delta_form="fp32" does.
 
     tiles = [Tile(cx, cy, width, W, H, max_iter, fractal_type=...), ...]
     batch = prepare_batch(tiles)            # orbits, tables, descriptors
@@ -28,7 +30,7 @@ import numpy as np
 
 from . import _lib, abi
 from . import high_precision as hp
-from .config import ACCURATE_BLA_EPS, decimal_context
+from .config import ACCURATE_BLA_EPS, compute_floatexp_scale, decimal_context
 
 BLA_LEVELS = 16
 
@@ -52,6 +54,7 @@ class Tile:
     strict_glitch: bool = True  # Pauldelbrot glitch flags
     rebase: bool = False       # one-pass rebasing (Mandelbrot, Burning Ship, Multibrot): no glitch flags
     bla_tol: float = 1e-6      # merge tolerance of the reference's BLA table (bla_form "reference")
+    delta_form: str = "fp64"   # "fp32": the FP32-mantissa FloatExp form (AP_TIER_FLOATEXP32)
 
 
 @dataclass(frozen=True)
@@ -148,11 +151,16 @@ def _tile_inputs(t, ref, arith, bla_form, torch, stream, L, scratch):
     render_perturbation_frame sets them (factor 1, one reference)."""
     from .perturbation import max_delta_c
     cpu_sem = arith == "ref_cpu"
+    fp32 = t.delta_form == "fp32"
     pw = Decimal(t.width)
     with localcontext(decimal_context(pw)):
         ph = pw * (Decimal(t.H) / Decimal(t.W))
         dx = float(pw / Decimal(max(1, t.W - 1)))
         dy = float(ph / Decimal(max(1, t.H - 1)))
+        # the FP32 form's pixel spacing in units of 2^-E (as the engine's coarse pass)
+        fe_e = compute_floatexp_scale(pw)
+        fe_dx = float(pw * (Decimal(2) ** fe_e) / Decimal(max(1, t.W - 1)))
+        fe_dy = float(ph * (Decimal(2) ** fe_e) / Decimal(max(1, t.H - 1)))
     bcx, bcy, bu, bv, re, im, rl = ref
     n = rl + 1
     d_re = torch.from_numpy(np.ascontiguousarray(re[:n])).to("cuda", non_blocking=False)
@@ -175,9 +183,16 @@ def _tile_inputs(t, ref, arith, bla_form, torch, stream, L, scratch):
                                       BLA_LEVELS, int(t.gen_n), float(t.gen_kr), float(t.gen_ki),
                                       _ptr(table), s), "ap_build_bla")
         bla_packed = torch.empty(80 * rl, dtype=torch.float64, device="cuda")
-        _lib.check(L.ap_pack_bla(_ptr(table), BLA_LEVELS, int(rl), _ptr(bla_packed), _ptr(orbit), s),
-                   "ap_pack_bla")
+        if fp32:
+            _lib.check(L.ap_pack_fe32(_ptr(orbit), int(rl), _ptr(table), BLA_LEVELS, _ptr(orbit[4 * n:]),
+                                      _ptr(bla_packed), s), "ap_pack_fe32")
+        else:
+            _lib.check(L.ap_pack_bla(_ptr(table), BLA_LEVELS, int(rl), _ptr(bla_packed), _ptr(orbit), s),
+                       "ap_pack_bla")
         stream.synchronize()  # the table scratch is reused by the next tile
+    elif fp32:
+        _lib.check(L.ap_pack_fe32(_ptr(orbit), int(rl), None, BLA_LEVELS, _ptr(orbit[4 * n:]), None, s),
+                   "ap_pack_fe32")
     flags = abi.AP_FLAG_NO_RGB | ((abi.AP_FLAG_ESCAPE_GLITCH | abi.AP_FLAG_NAN_GUARD) if cpu_sem
                                   else abi.AP_FLAG_NAN_GUARD)
     rebase = bool(t.rebase)
@@ -186,11 +201,13 @@ def _tile_inputs(t, ref, arith, bla_form, torch, stream, L, scratch):
     if rebase:
         flags |= abi.AP_FLAG_REBASE
     p = abi.new_params(width=t.W, height=t.H, factor=1, max_iter=int(t.max_iter),
-                       fractal_type=int(t.fractal_type), tier=abi.AP_TIER_PERTURB,
+                       fractal_type=int(t.fractal_type),
+                       tier=abi.AP_TIER_FLOATEXP32 if fp32 else abi.AP_TIER_PERTURB,
                        arith=(abi.AP_ARITH_REF_CPU if cpu_sem else
                               abi.AP_ARITH_FAST if (arith == "fast" and rebase) else abi.AP_ARITH_REF_CUDA),
                        mode=abi.AP_MODE_COARSE, flags=flags, gen_n=int(t.gen_n),
-                       gen_kr=float(t.gen_kr), gen_ki=float(t.gen_ki), dx_hi=dx, dy_hi=dy,
+                       gen_kr=float(t.gen_kr), gen_ki=float(t.gen_ki), dx_hi=fe_dx if fp32 else dx,
+                       dy_hi=fe_dy if fp32 else dy, e_scale=int(fe_e) if fp32 else 0,
                        ref_px=ref_px, ref_py=ref_py, ref_cx=float(bcx), ref_cy=float(bcy),
                        julia_cx_hi=float(t.julia_cx), julia_cy_hi=float(t.julia_cy), ref_len=int(rl),
                        bla_levels=BLA_LEVELS if use_bla else 0,
@@ -207,6 +224,8 @@ _ARITH_CODES = {"ref_cpu": abi.AP_ARITH_REF_CPU, "ref_cuda": abi.AP_ARITH_REF_CU
 def _check_batch(tiles, arith, bla_form):
     if bla_form not in ("reference", "accurate"):
         raise ValueError("bla_form must be 'reference' or 'accurate'")
+    if any(t.delta_form not in ("fp64", "fp32") for t in tiles):
+        raise ValueError("a tile's delta_form must be 'fp64' or 'fp32'")
     if arith not in _ARITH_CODES:
         raise ValueError("arith must be 'ref_cpu', 'ref_cuda' or 'fast' (the fused step of one-pass tiles; "
                          "the batch's single-reference tiles then run 'ref_cuda')")

@@ -1,9 +1,10 @@
 // ap_batch.cu -- many tiles of uneven size, formula and max_iter in one
 // persistent kernel.
 //
-// A tile is one coarse perturbation pass (AP_TIER_PERTURB, packed orbit and
-// BLA rows, no in-kernel colour) with its own parameters and outputs, in the
-// single-reference form or in one-pass rebasing (AP_FLAG_REBASE).  Each
+// A tile is one coarse perturbation pass (AP_TIER_PERTURB with packed orbit and
+// BLA rows, or AP_TIER_FLOATEXP32 with the FP32 form's packed inputs; no in-kernel
+// colour) with its own parameters and outputs, in the single-reference form or in
+// one-pass rebasing (AP_FLAG_REBASE).  Each
 // tile is cut into patches of patch_w x patch_h = 256 pixels; patches are
 // numbered tile after tile (the host orders tiles by estimated cost, largest
 // first).  The grid holds blocks_per_sm blocks per SM for the whole batch; the
@@ -11,7 +12,8 @@
 //
 // A block works in rounds.  In a round each thread runs one pixel for `quantum`
 // loop steps, resumable (the per-frame kernel's pixel_begin / pixel_advance /
-// rebase_advance / pixel_finish, so values are identical).  A pixel that finishes is
+// rebase_advance / pixel_finish, and fe32_begin / fe32_advance / fe32_finish for FP32
+// tiles, so values are identical).  A pixel that finishes is
 // written out; one that does not leaves its state in the block's shared slots.  At
 // the end of the round the block compacts the unfinished pixels into its first
 // slots, keeping their order, so they run together in as few warps as possible in
@@ -21,6 +23,7 @@
 // anything outside the block: a block whose slots are empty once the queue has run
 // out exits.
 #include "ap_coarse.cuh"
+#include "ap_fe32.cuh"
 
 namespace ap {
 
@@ -137,11 +140,109 @@ __device__ __noinline__ bool slot_run(const ApTileDesc* __restrict__ t, BatchSlo
     return true;
 }
 
+// FP32 tiles (AP_TIER_FLOATEXP32) keep their pixels in the same slots: the delta's
+// mantissa pair (exactly, as doubles) where an FP64 pixel keeps its delta, z in stage 2
+// as there, the offset dc in units of 2^-E, and the delta's exponent where an FP64
+// pixel keeps its first step (an FP32 pixel takes no series start: it starts at 0).
+__device__ __forceinline__ void fe32_slot_store(BatchSlots& S, int q, const Fe32Run& s, int tile, bool rebase) {
+    const bool st2 = s.stage == 2;
+    S.zx[q] = st2 ? s.zx : (double)s.wx;
+    S.zy[q] = st2 ? s.zy : (double)s.wy;
+    S.dcx[q] = s.dcx;
+    S.dcy[q] = s.dcy;
+    S.idx[q] = s.idx;
+    S.k[q] = s.k;
+    S.k0[q] = s.e;
+    S.k2m[q] = rebase ? s.m : s.k2;
+    S.leaps[q] = s.leaps;
+    S.skipped[q] = s.skipped;
+    S.rebases[q] = s.rebases;
+    S.tag[q] = (tile << 3) | (s.stage << 1) | (s.glitch ? 1 : 0);
+}
+
+__device__ __forceinline__ void fe32_slot_load(const BatchSlots& S, int q, Fe32Run& s, bool rebase) {
+    const int tag = S.tag[q];
+    s.stage = (tag >> 1) & 3;
+    s.glitch = tag & 1;
+    const double a = S.zx[q], c = S.zy[q];
+    const bool st2 = s.stage == 2;
+    s.wx = st2 ? 0.0f : (float)a;
+    s.wy = st2 ? 0.0f : (float)c;
+    s.zx = st2 ? a : 0.0;
+    s.zy = st2 ? c : 0.0;
+    s.dcx = S.dcx[q];
+    s.dcy = S.dcy[q];
+    s.idx = 0;
+    s.k = S.k[q];
+    s.e = S.k0[q];
+    s.m = rebase ? S.k2m[q] : 0;
+    s.k2 = rebase ? -1 : S.k2m[q];
+    s.leaps = S.leaps[q];
+    s.skipped = S.skipped[q];
+    s.rebases = S.rebases[q];
+    s.o = interior_sample();
+}
+
+// What a round of an FP32 pixel changes (the tile, dc and the index stay).
+__device__ __forceinline__ void fe32_slot_store_run(BatchSlots& S, int q, const Fe32Run& s, bool rebase) {
+    const bool st2 = s.stage == 2;
+    S.zx[q] = st2 ? s.zx : (double)s.wx;
+    S.zy[q] = st2 ? s.zy : (double)s.wy;
+    S.k[q] = s.k;
+    S.k0[q] = s.e;
+    S.k2m[q] = rebase ? s.m : s.k2;
+    S.leaps[q] = s.leaps;
+    S.skipped[q] = s.skipped;
+    S.rebases[q] = s.rebases;
+    S.tag[q] = (S.tag[q] & ~7) | (s.stage << 1) | (s.glitch ? 1 : 0);
+}
+
+// One round of an FP32 pixel (as slot_run).
+template <int FT, bool BLA, bool REBASE>
+__device__ __noinline__ bool fe32_slot_run(const ApTileDesc* __restrict__ t, BatchSlots& S, int q, int quantum) {
+    const ApFrameBuffers b = tile_buffers(t);
+    Fe32Run s;
+    fe32_slot_load(S, q, s, REBASE);
+    fe32_advance<FT, BLA, REBASE, true>(t->p, b, s, quantum);
+    if (s.stage == 3) {
+        s.idx = S.idx[q];
+        fe32_finish(t->p, b, s);
+        return false;
+    }
+    fe32_slot_store_run(S, q, s, REBASE);
+    return true;
+}
+
+// FP32 formula dispatch (Burning Ship types take no leaps, as in the per-frame pass).
+__device__ __forceinline__ bool fe32_batch_run(const ApTileDesc* t, BatchSlots& S, int q, int quantum) {
+    const bool bla = t->p.bla_levels > 1 && t->bla_packed != nullptr;
+    const bool rebase = (t->p.flags & AP_FLAG_REBASE) != 0;
+    switch (t->p.fractal_type) {
+    case 1:
+    case 3:
+        return rebase ? fe32_slot_run<kFtShip, false, true>(t, S, q, quantum)
+                      : fe32_slot_run<kFtShip, false, false>(t, S, q, quantum);
+    case 4:
+        if (rebase)
+            return bla ? fe32_slot_run<kFtMulti, true, true>(t, S, q, quantum)
+                       : fe32_slot_run<kFtMulti, false, true>(t, S, q, quantum);
+        return bla ? fe32_slot_run<kFtMulti, true, false>(t, S, q, quantum)
+                   : fe32_slot_run<kFtMulti, false, false>(t, S, q, quantum);
+    default:
+        if (rebase)
+            return bla ? fe32_slot_run<kFtQuad, true, true>(t, S, q, quantum)
+                       : fe32_slot_run<kFtQuad, false, true>(t, S, q, quantum);
+        return bla ? fe32_slot_run<kFtQuad, true, false>(t, S, q, quantum)
+                   : fe32_slot_run<kFtQuad, false, false>(t, S, q, quantum);
+    }
+}
+
 // Formula dispatch.  AP_ARITH_FAST serves one-pass tiles only; a FAST batch's
 // single-reference tiles (Julia types) run the CUDA-source profile.
 template <int ARITH>
 __device__ __forceinline__ bool batch_run(const ApTileDesc* t, BatchSlots& S, int q, int quantum) {
     constexpr int kPlain = (ARITH == AP_ARITH_FAST) ? AP_ARITH_REF_CUDA : ARITH;
+    if (t->p.tier == AP_TIER_FLOATEXP32) return fe32_batch_run(t, S, q, quantum);
     const bool bla = t->p.bla_levels > 1 && t->bla_packed != nullptr;
     if (t->p.flags & AP_FLAG_REBASE) {
         switch (t->p.fractal_type) {
@@ -172,11 +273,18 @@ __device__ __forceinline__ bool batch_run(const ApTileDesc* t, BatchSlots& S, in
 template <int ARITH>
 __device__ __noinline__ bool slot_begin(const ApTileDesc* __restrict__ t, int tile, BatchSlots& S, int q, int i,
                                         int j) {
+    const bool rebase = (t->p.flags & AP_FLAG_REBASE) != 0;
+    if (t->p.tier == AP_TIER_FLOATEXP32) {
+        Fe32Run f;
+        const bool ok = fe32_begin(t->p, tile_buffers(t), i, j, f);
+        if (ok) fe32_slot_store(S, q, f, tile, rebase);
+        return ok;
+    }
     PixelRun s;
     const bool ship = t->p.fractal_type == 1 || t->p.fractal_type == 3;
     const bool ok = ship ? pixel_begin<ARITH, kFtShip>(t->p, tile_buffers(t), i, j, s)
                          : pixel_begin<ARITH, kFtQuad>(t->p, tile_buffers(t), i, j, s);
-    if (ok) slot_store(S, q, s, tile, (t->p.flags & AP_FLAG_REBASE) != 0);
+    if (ok) slot_store(S, q, s, tile, rebase);
     return ok;
 }
 
@@ -288,10 +396,17 @@ extern "C" int ap_batch_plan(const ApTileDesc* tiles, int32_t n, int32_t patch_w
         return AP_E_INVALID;
     }
     int64_t acc = 0;
+    // the batch's arithmetic profile: its FP64 tiles'; FP32 tiles have their own form
+    int a0 = -1;
+    for (int q = 0; q < n && a0 < 0; ++q)
+        if (tiles[q].p.tier == AP_TIER_PERTURB)
+            a0 = tiles[q].p.arith == AP_ARITH_FAST ? AP_ARITH_REF_CUDA : tiles[q].p.arith;
     for (int q = 0; q < n; ++q) {
         const ApTileDesc& t = tiles[q];
         const ApFrameParams& p = t.p;
-        if (p.tier != AP_TIER_PERTURB || p.mode != AP_MODE_COARSE || !(p.flags & AP_FLAG_NO_RGB) ||
+        const bool fe32 = p.tier == AP_TIER_FLOATEXP32;
+        if ((p.tier != AP_TIER_PERTURB && !fe32) || (fe32 && p.bbsa_skip > 0) || p.mode != AP_MODE_COARSE ||
+            !(p.flags & AP_FLAG_NO_RGB) ||
             p.rebase_pass != 0 || p.width < 1 || p.height < 1 || p.factor < 1 || p.max_iter < 0 ||
             p.fractal_type < 0 || p.fractal_type > 4 || p.ref_len < 0 || p.bla_levels > 16 ||
             (p.fractal_type == 4 && (p.gen_n < 1 || p.gen_n > 64)) || !t.orbit_packed ||
@@ -299,16 +414,15 @@ extern "C" int ap_batch_plan(const ApTileDesc* tiles, int32_t n, int32_t patch_w
             (t.counters && (reinterpret_cast<uintptr_t>(t.counters) & 15u)) ||
             (long long)p.width * p.height >= (1LL << 31) ||
             ((p.flags & AP_FLAG_REBASE) && (p.fractal_type == 2 || p.fractal_type == 3 || p.ref_len < 1))) {
-            ap::set_error("ap_batch_plan: tile %d is not a coarse AP_TIER_PERTURB pass on packed "
-                          "inputs without in-kernel colour", q);
+            ap::set_error("ap_batch_plan: tile %d is not a coarse AP_TIER_PERTURB or AP_TIER_FLOATEXP32 "
+                          "pass on packed inputs without in-kernel colour", q);
             return AP_E_INVALID;
         }
         // one profile per batch; AP_ARITH_FAST is one-pass rebasing's own step, and a
         // FAST batch's single-reference tiles carry the CUDA-source profile they run in
-        const int a0 = tiles[0].p.arith == AP_ARITH_FAST ? AP_ARITH_REF_CUDA : tiles[0].p.arith;
         const int aq = p.arith == AP_ARITH_FAST ? AP_ARITH_REF_CUDA : p.arith;
-        if (aq != a0 || (p.arith == AP_ARITH_FAST && !(p.flags & AP_FLAG_REBASE)) ||
-            (p.arith != AP_ARITH_REF_CPU && p.arith != AP_ARITH_REF_CUDA && p.arith != AP_ARITH_FAST)) {
+        if (!fe32 && (aq != a0 || (p.arith == AP_ARITH_FAST && !(p.flags & AP_FLAG_REBASE)) ||
+            (p.arith != AP_ARITH_REF_CPU && p.arith != AP_ARITH_REF_CUDA && p.arith != AP_ARITH_FAST))) {
             ap::set_error("ap_batch_plan: every tile of a batch uses one arithmetic profile "
                           "(AP_ARITH_FAST for one-pass tiles only, beside AP_ARITH_REF_CUDA)");
             return AP_E_INVALID;

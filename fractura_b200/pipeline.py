@@ -118,8 +118,8 @@ def batch_serves(tile_w, kw):
     """Whether the persistent batch kernel renders a mosaic tile of width tile_w with the
     render arguments kw exactly as render_frame_ssaa does: the FP64-delta perturbation
     tier, factor 1, a glitch mode with no re-render pass and no Pauldelbrot flags, no
-    series start (orders 4 and 8), the reference arithmetic profiles, FP64 deltas, and no
-    one-pass rebasing of Julia tiles."""
+    series start (orders 4 and 8), the reference arithmetic profiles, FP64 or FP32
+    deltas, and no one-pass rebasing of Julia tiles."""
     from . import engine
     if engine.select_tier(tile_w, kw["precision_mode"]) != abi.AP_TIER_PERTURB:
         return False
@@ -130,7 +130,7 @@ def batch_serves(tile_w, kw):
         return False
     if (kw["arith"] or engine.DEFAULT_ARITH) not in ("ref_cpu", "ref_cuda"):
         return False
-    if kw["delta_form"] not in (None, "fp64"):
+    if kw["delta_form"] not in (None, "fp64", "fp32"):
         return False
     return not ("One-Pass Rebasing" in gm and int(kw["fractal_type"]) in (2, 3))
 
@@ -225,7 +225,7 @@ def _mosaic_batch(views, iters, W, H, n, kw, cmap_name, is_hdr, dt, stitch, on_t
     tiles = [fb.Tile(cx=tcx, cy=tcy, width=tw, W=W, H=H, max_iter=int(it), fractal_type=int(kw["fractal_type"]),
                      julia_cx=float(kw["julia_cx"]), julia_cy=float(kw["julia_cy"]), gen_n=int(kw["gen_n"]),
                      gen_kr=float(kw["gen_kr"]), gen_ki=float(kw["gen_ki"]), bla=bla, strict_glitch=False,
-                     rebase=rebase, bla_tol=float(kw["bbsa_tol"]))
+                     rebase=rebase, bla_tol=float(kw["bbsa_tol"]), delta_form=kw["delta_form"] or "fp64")
              for (_, _, tcx, tcy, tw), it in zip(views, iters)]
     st = stream or torch.cuda.Stream()
     L = _lib.load()

@@ -129,14 +129,16 @@ typedef struct ApFrameBuffers {
     const double* bla_packed;   /* optional, from ap_pack_bla (needs orbit_packed) */
 } ApFrameBuffers;
 
-/* One tile of a batch (ap_render_batch): a coarse AP_TIER_PERTURB pass on packed
- * inputs, without in-kernel colour (p.flags has AP_FLAG_NO_RGB), with its own
- * parameters, reference orbit and outputs; single-reference, or one-pass rebasing
+/* One tile of a batch (ap_render_batch): a coarse AP_TIER_PERTURB or AP_TIER_FLOATEXP32
+ * pass on packed inputs, without in-kernel colour (p.flags has AP_FLAG_NO_RGB), with its
+ * own parameters, reference orbit and outputs; single-reference, or one-pass rebasing
  * (p.flags has AP_FLAG_REBASE; fractal types 0, 1, 4).  448 bytes. */
 typedef struct ApTileDesc {
     ApFrameParams p;
-    const double* orbit_packed; /* ap_pack_orbit records of the tile's reference */
-    const double* bla_packed;   /* ap_pack_bla rows when p.bla_levels > 1, else NULL */
+    const double* orbit_packed; /* ap_pack_orbit records of the tile's reference (AP_TIER_FLOATEXP32:
+                                   followed by ap_pack_fe32's float records, 6 (ref_len + 1) doubles) */
+    const double* bla_packed;   /* when p.bla_levels > 1: ap_pack_bla rows (AP_TIER_FLOATEXP32: ap_pack_fe32's
+                                   bla_out), else NULL */
     float* iter_map;            /* [H, W] smooth values (required) */
     int32_t* kmap;              /* optional [H, W] escape steps */
     double* s64;                /* optional [H, W] float64 smooth values */
@@ -397,7 +399,8 @@ AP_API int ap_decimal_arith(int32_t op, const int64_t* a_meta, const uint64_t* a
  * tiles and first_patch are device copies of the planned arrays.  min_blocks (4 or 6) picks
  * the register budget the kernel is compiled for; arith is the tiles' common profile
  * (AP_ARITH_FAST when the plan holds AP_ARITH_FAST tiles: one-pass tiles only, the others
- * then carry AP_ARITH_REF_CUDA).  Values equal ap_render_pass's for each tile. */
+ * then carry AP_ARITH_REF_CUDA; AP_TIER_FLOATEXP32 tiles compute in the FP32 form whatever
+ * the profile).  Values equal ap_render_pass's for each tile. */
 AP_API int ap_batch_plan(const ApTileDesc* host_tiles, int32_t n, int32_t patch_w, int32_t patch_h,
                          int64_t* first_patch);
 AP_API int ap_render_batch(const ApTileDesc* tiles, const int64_t* first_patch, int32_t n,

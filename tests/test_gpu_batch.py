@@ -6,6 +6,7 @@ to the same values; every launch shape the autotuner may pick (patch shape,
 blocks per SM, register budget, quantum) gives the same values, and so does a
 quantum of one step, where every pixel is compacted after every step.
 """
+import dataclasses
 from decimal import Decimal
 
 import numpy as np
@@ -47,7 +48,7 @@ def _engine_tile(t, arith, bla_form):
                              bbsa_order=32 if t.bla else 0,
                              glitch_mode="One-Pass Rebasing" if t.rebase else "Off (Single-Ref)",
                              gen_n=t.gen_n, gen_kr=t.gen_kr, gen_ki=t.gen_ki, h_iter_buf=it,
-                             arith=arith, bla_form=bla_form, _extra_out=(kmap, s64))
+                             arith=arith, bla_form=bla_form, delta_form=t.delta_form, _extra_out=(kmap, s64))
     return it, kmap.cpu().numpy()
 
 
@@ -129,3 +130,29 @@ def test_streamed_batch_equals_the_whole_batch(arith, rebase):
     for want, got in zip(b.tiles_out, sb.tiles_out):
         assert torch.equal(want["iter"], got["iter"]) and torch.equal(want["kmap"], got["kmap"])
     assert sb.nominal_iterations() == b.nominal_iterations()
+
+
+@pytest.mark.parametrize("rebase", [False, True])
+@pytest.mark.parametrize("bla_form", ["reference", "accurate"])
+def test_fp32_tiles_match_per_tile_frames(rebase, bla_form):
+    """Tiles in the FP32-mantissa form (delta_form='fp32', every formula) beside FP64 tiles
+    in one batch: each equals the engine's coarse render of the tile in its own form, in
+    the default launch shape, the widest candidate, and quanta of 1 and 7 steps (every
+    pixel's state goes through the shared slots at every step)."""
+    import torch
+    hp.clear_reference_orbit_cache()
+    tiles = [dataclasses.replace(t, delta_form="fp32") if q % 3 != 2 else t for q, t in enumerate(_tiles(rebase))]
+    want = [_engine_tile(t, "ref_cuda", bla_form) for t in tiles]
+    s = torch.cuda.Stream()
+    hp.clear_reference_orbit_cache()
+    b = fb.prepare_batch(tiles, arith="ref_cuda", bla_form=bla_form, stream=s)
+    for cfg in (fb.BatchConfig(), fb.CANDIDATES[-1], fb.BatchConfig(quantum=1),
+                fb.BatchConfig(quantum=7, blocks_per_sm=1)):
+        for o in b.tiles_out:
+            o["iter"].fill_(-7.0)
+        b.render(cfg)
+        torch.cuda.synchronize()
+        for t, out, (it, k) in zip(tiles, b.tiles_out, want):
+            got = out["iter"].cpu().numpy()
+            assert np.array_equal(got.view(np.uint32), it.view(np.uint32)), (cfg, t.fractal_type, int((got != it).sum()))
+            assert np.array_equal(out["kmap"].cpu().numpy(), k)

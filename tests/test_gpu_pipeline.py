@@ -65,9 +65,10 @@ def test_mosaic_batch_path_equals_per_tile_frames(glitch_mode, arith, scheme):
     assert img.any()
 
 
-@pytest.mark.parametrize("case", ["pauldelbrot", "ssaa2", "no_batch", "ship_one_pass"])
+@pytest.mark.parametrize("case", ["pauldelbrot", "ssaa2", "no_batch", "ship_one_pass", "fp32_batch",
+                                  "ship_fp32_one_pass"])
 def test_mosaic_pipeline_path_equals_per_tile_frames(case):
-    m = SHIP if case == "ship_one_pass" else CFG3
+    m = SHIP if case.startswith("ship") else CFG3
     n, max_iter = 2, 5000
     width = Decimal(m["width"]) * 20
     kw = dict(precision_mode="1e-300 (Perturbation)", bbsa_order=32, bbsa_tol=1e-6,
@@ -78,6 +79,10 @@ def test_mosaic_pipeline_path_equals_per_tile_frames(case):
         kw["ssaa_factor"] = 2
     elif case == "ship_one_pass":
         kw["glitch_mode"] = "One-Pass Rebasing"
+    elif case == "fp32_batch":
+        kw["delta_form"] = "fp32"
+    elif case == "ship_fp32_one_pass":
+        kw["glitch_mode"], kw["delta_form"] = "One-Pass Rebasing", "fp32"
     hp.clear_reference_orbit_cache()
     img = render_mosaic(n, W, H, max_iter, Decimal(m["cx"]), Decimal(m["cy"]), width,
                         use_batch=(case != "no_batch"), **kw)

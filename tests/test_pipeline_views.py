@@ -48,7 +48,9 @@ def test_mosaic_views_reject_empty_grid():
     ({"bbsa_order": 32, "ssaa_factor": 2}, False),
     ({"bbsa_order": 32, "arith": "ref_cuda"}, True),
     ({"bbsa_order": 32, "arith": "fast", "glitch_mode": "One-Pass Rebasing"}, False),
-    ({"bbsa_order": 32, "delta_form": "fp32"}, False),
+    ({"bbsa_order": 32, "delta_form": "fp32"}, True),
+    ({"bbsa_order": 32, "delta_form": "fp32", "glitch_mode": "One-Pass Rebasing", "fractal_type": 1}, True),
+    ({"bbsa_order": 32, "delta_form": "fp64x"}, False),
 ])
 def test_batch_serves(change, served):
     kw = dict(_DEFAULTS, **change)
