@@ -311,6 +311,45 @@ def batch_tiles(wl):
             for t in wl["tiles"]]
 
 
+def batch_fp32_form(torch, fb, hp, wl, b64, cfg, stream, flush, steps):
+    """Config 4 in the FP32-mantissa FloatExp form: the same tiles (one-pass rebasing where
+    the FP64 batch rebases) with delta_form="fp32", rendered in one persistent launch, and
+    its agreement with the FP64 batch b64: identical escape steps and smooth differences
+    where both escape at the same step, per formula."""
+    import dataclasses
+    hp.clear_reference_orbit_cache()
+    tiles = [dataclasses.replace(t, delta_form="fp32") for t in batch_tiles(wl)]
+    b = fb.prepare_batch(tiles, arith="ref_cuda", bla_form=wl["bla_form"], stream=stream)
+    b.render(cfg)
+    torch.cuda.synchronize()
+    ms = timed_loop(torch, stream, flush, max(3, steps // 5), lambda: b.render(cfg))
+    iters = b.nominal_iterations()
+    per, same_k, pixels, diffs = {}, 0, 0, []
+    for t, o32, o64 in zip(tiles, b.tiles_out, b64.tiles_out):
+        k32, k64 = o32["kmap"].cpu().numpy(), o64["kmap"].cpu().numpy()
+        s32, s64 = o32["iter"].cpu().numpy(), o64["iter"].cpu().numpy()
+        key = {0: "mandelbrot", 1: "burning_ship", 2: "julia", 3: "ship_julia"}.get(
+            t.fractal_type, f"multibrot{t.gen_n}")
+        eq = k32 == k64
+        both = eq & (k64 >= 0)
+        d = np.abs(s32[both].astype(np.float64) - s64[both].astype(np.float64))
+        diffs.append(d)
+        acc = per.setdefault(key, [0, 0])
+        acc[0] += int(eq.sum())
+        acc[1] += eq.size
+        same_k += int(eq.sum())
+        pixels += eq.size
+    d = np.concatenate(diffs) if diffs else np.zeros(1)
+    return {
+        "form": "the same tiles with FP32-mantissa FloatExp deltas (24-bit mantissas, int exponents; FP64 "
+                "escape, rebase and sign tests where a float screen says they can fire), one persistent launch",
+        "value": iters / (float(np.median(ms)) * 1e-3) / 1e9, "unit": "G iter/s",
+        "ms_per_batch": float(np.median(ms)),
+        "vs_fp64_batch": {"identical_k": same_k / max(1, pixels),
+                          "identical_k_by_formula": {k: v[0] / max(1, v[1]) for k, v in sorted(per.items())},
+                          "smooth_p99_where_k_equal": float(np.percentile(d, 99)) if d.size else 0.0}}
+
+
 def config_of(wl, n_gpus):
     """The workload (what is rendered), the same for both arms; the method is "form"."""
     par = f"replicas x{n_gpus}" if n_gpus > 1 else "single"
@@ -720,6 +759,8 @@ def frame_arm(args, wl, rank, world, local_rank, steps, headline):
             Form("fp32_floatexp", dict(delta_form="fp32", glitch_mode="Pauldelbrot", **cuda),
                  "FP32 mantissa + int exponent deltas, dc-aware BLA, Pauldelbrot with up to 4 rebase "
                  "passes"),
+            Form("fp32_floatexp_one_pass", dict(delta_form="fp32", **cuda),
+                 "FP32 mantissa + int exponent deltas, dc-aware BLA, one-pass rebasing"),
         ]
         for f in extra:
             record_form(torch, _lib, engine, wl, stream, f, kmap, s64)
@@ -733,16 +774,19 @@ def frame_arm(args, wl, rank, world, local_rank, steps, headline):
     elif perturb and wl["width"] == "1e-1000":
         # the FP32-mantissa form against the FP64-mantissa FloatExp form of the same view
         n_cmp = max(3, steps // 10)
-        f = record_form(torch, _lib, engine, wl, stream,
-                        Form("fp32_floatexp", dict(delta_form="fp32"),
-                             "FP32 mantissa + int exponent deltas, dc-aware BLA, Pauldelbrot"), kmap, s64)
-        f_ms, _ = timed_replay(torch, _lib, f.ops, stream, n_cmp, flush)
-        s = summarise_form(f, f_ms)
-        s["k_identical_vs_fp64_floatexp"] = float(np.mean(f.kmap == chosen.kmap))
-        d = np.abs(f.s64 - chosen.s64)
-        s["smooth_diff_vs_fp64_floatexp"] = {"p50": float(np.median(d)), "p99": float(np.percentile(d, 99)),
-                                             "max": float(d.max())}
-        line["forms"] = {"fp32_floatexp": s}
+        line["forms"] = {}
+        for form in (Form("fp32_floatexp", dict(delta_form="fp32"),
+                          "FP32 mantissa + int exponent deltas, dc-aware BLA, Pauldelbrot"),
+                     Form("fp32_floatexp_one_pass", dict(delta_form="fp32", glitch_mode="One-Pass Rebasing"),
+                          "FP32 mantissa + int exponent deltas, dc-aware BLA, one-pass rebasing")):
+            f = record_form(torch, _lib, engine, wl, stream, form, kmap, s64)
+            f_ms, _ = timed_replay(torch, _lib, f.ops, stream, n_cmp, flush)
+            s = summarise_form(f, f_ms)
+            s["k_identical_vs_fp64_floatexp"] = float(np.mean(f.kmap == chosen.kmap))
+            d = np.abs(f.s64 - chosen.s64)
+            s["smooth_diff_vs_fp64_floatexp"] = {"p50": float(np.median(d)), "p99": float(np.percentile(d, 99)),
+                                                 "max": float(d.max())}
+            line["forms"][form.name] = s
 
     strict = "Pauldelbrot" in wl["glitch_mode"] or "Strict" in wl["glitch_mode"]
     flops, n_pass, work = pass_flops(torch, _lib, abi, chosen.ops, stream, H, W, strict,
@@ -894,6 +938,8 @@ def batch_arm(args, wl, rank, world, local_rank, steps, headline):
             "value": it1 / (float(np.median(ms1)) * 1e-3) / 1e9, "unit": "G iter/s",
             "ms_per_batch": float(np.median(ms1)), "glitched_pixels": glitched,
             "glitched_fraction": glitched / pixels}
+    if rank == 0:
+        forms["fp32_floatexp"] = batch_fp32_form(torch, fb, hp, wl, b, cfg, stream, flush, steps)
     if rank != 0:
         return None
     flops = batch_flops(torch, _lib, b, cfg)

@@ -18,6 +18,13 @@
  *   AP_ARITH_REF_CUDA  the reference's CUDA sources as written: cuda.fma is
  *                      fused, every other operation is rounded separately.
  *
+ * Two forms have no reference counterpart and are restated from the engine's
+ * own definitions, so that device frames can be pinned bit for bit: the fused
+ * one-pass rebasing step (AP_ARITH_FAST) and the FP32-mantissa FloatExp form
+ * (AP_TIER_FLOATEXP32).  Where their precision carries a view, their values
+ * equal the reference's goldens (tests/test_oracle_rebase.py,
+ * tests/test_oracle_fe32.py).
+ *
  * Parity is pinned by the .npz fixtures in tests/golden, generated by running the reference
  * (tests/golden/make_golden.py).
  */
