@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libapeiron_b200.so")
 
 EXPORTS = (
     "ap_abi_version", "ap_last_error", "ap_render_pass", "ap_resolve_hist_pass",
-    "ap_edge_detect", "ap_histogram_cdf", "ap_colour", "ap_build_bla", "ap_build_bla_dc", "ap_bbsa_coeffs", "ap_reference_orbit", "ap_decimal_escape", "ap_decimal_orbit", "ap_decimal_arith", "ap_decimal_to_double", "ap_glitch_bins", "ap_set_pixels", "ap_strict_eval", "ap_batch_plan", "ap_render_batch", "ap_smooth_forward", "ap_smooth_adjoint_blocks", "ap_smooth_adjoint", "ap_smooth_tangent", "ap_fma_peak_launch",
+    "ap_edge_detect", "ap_histogram_cdf", "ap_colour", "ap_build_bla", "ap_build_bla_dc", "ap_bbsa_coeffs", "ap_reference_orbit", "ap_reference_orbit_cert", "ap_decimal_escape", "ap_decimal_orbit", "ap_decimal_arith", "ap_decimal_to_double", "ap_glitch_bins", "ap_set_pixels", "ap_strict_eval", "ap_batch_plan", "ap_render_batch", "ap_smooth_forward", "ap_smooth_adjoint_blocks", "ap_smooth_adjoint", "ap_smooth_tangent", "ap_fma_peak_launch",
     "ap_histogram_cdf_noalloc", "ap_launch_counter", "ap_pack_orbit", "ap_pack_bla",
     "ap_pack_fe32", "ap_render_rows", "ap_histogram", "ap_cdf_from_histogram",
 )
@@ -61,6 +61,7 @@ def load():
     L.ap_build_bla_dc.argtypes = [vp, vp, i32, i32, f64, f64, i32, i32, f64, f64, vp, vp]
     L.ap_bbsa_coeffs.argtypes = [vp, vp, i32, f64, i32, f64, i32, i32, f64, f64, i32, vp]
     L.ap_reference_orbit.argtypes = [vp, i32, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp]
+    L.ap_reference_orbit_cert.argtypes = [vp, i32, i32, i32, i32, i32, i32, vp, vp, vp, vp, vp]
     L.ap_decimal_escape.argtypes = [vp, vp, i32, i32, i32, i32, i32, vp, vp, vp]
     L.ap_decimal_arith.argtypes = [i32, vp, vp, vp, vp, i32, vp, vp, vp]
     L.ap_decimal_orbit.argtypes = [vp, vp, i32, i32, i32, i32, i32, vp, vp, vp]

@@ -307,13 +307,86 @@ inline bool equal(const Fx& a, const Fx& b, int L) {
     return a.neg == b.neg && cmp_mag(a.m, b.m, L) == 0;
 }
 
+// ---- Certification against the Decimal iteration (quadratic formulas) ----------------
+// The reference iterates the orbit in Decimal with P significant digits; every operation
+// rounds with relative error at most u = 5 10^-P.  The run here is fixed point with F
+// fractional bits; a truncated product is off by less than 1.01 units of 2^-F, a stored
+// seed by 0.5.  Both follow the same map.  In the complex modulus, z^2 moves by at most
+// (2 |z| + E) E when z moves by E, and so does Burning Ship's step, whose fold
+// (x, y) -> (|x|, |y|) moves no point farther; so the two runs' distance obeys
+//   E_{k+1} <= (2 |z| + E_k) E_k + r_dec + r_fix,
+//   r_dec <= u [2 (x^2 + y^2) + |x'| + 4 |x| |y| + |y'|] (with margins),  r_fix = 6.5 2^-F,
+// where |x'| <= x^2 + y^2 + |c_x| and |y'| <= 2 |x| |y| + |c_y|, the magnitudes taken at
+// the fixed-point value plus E.  The two float64 roundings of a component agree wherever
+// E_k is below half its distance to the nearest float64 rounding boundary (half: the
+// boundaries below a power of two are twice as dense), and the bailout decisions agree
+// wherever |Z|^2 is farther from 65536 than its own error bound.  E is held scaled by
+// 2^B (u 2^B in [1, 2)), so it neither underflows nor overflows.
+constexpr int kNoDist = -(1 << 30);
+
+u64 bits_at(const Fx& a, int L, int lo_bit) {  // bits [lo_bit, lo_bit + 63]; zero outside [0, 64 L)
+    if (lo_bit <= -64) return 0;
+    if (lo_bit < 0) return a.m[0] << (-lo_bit);
+    const int li = lo_bit >> 6, sh = lo_bit & 63;
+    if (li >= L) return 0;
+    u64 w = a.m[li] >> sh;
+    if (sh && li + 1 < L) w |= a.m[li + 1] << (64 - sh);
+    return w;
+}
+
+// floor(log2) of a lower bound on the distance from a (in value units) to the nearest
+// float64 rounding boundary; kNoDist when there is none to give (zero, a value near
+// the subnormal range, or 64 bits below the mantissa at the midpoint itself).
+int rounding_distance_exp(const Fx& a, int L, int I) {
+    int top = L - 1;
+    while (top >= 0 && a.m[top] == 0) --top;
+    if (top < 0) return kNoDist;
+    const int p = 64 * top + (63 - __builtin_clzll(a.m[top]));
+    const int F = 64 * (L - I);
+    if (p - F < -1000) return kNoDist;
+    const int lo_bit = p - 116;  // the 64 bits just below the mantissa's last bit
+    const u64 w = bits_at(a, L, lo_bit), half = 1ULL << 63;
+    const u64 d = w < half ? half - w - 1 : w - half;  // the bits below may add up to one unit
+    if (d == 0) return kNoDist;
+    return (63 - __builtin_clzll(d)) + lo_bit - F;
+}
+
+struct Cert {
+    bool ok = false;
+    int B = 0;              // scaled quantities are value * 2^B
+    double u_s = 0.0;       // Decimal unit roundoff, scaled
+    double r_fix_s = 0.0;   // the fixed-point run's error per step, scaled
+    double E = 0.0;         // the bound on |z_Decimal - z_fixed| (max norm), scaled
+    double cx = 0.0, cy = 0.0;
+
+    void start(int dec_digits, int L, int I, double cxd, double cyd, bool julia) {
+        const double l2_10 = 3.3219280948873623478703194294894;
+        ok = dec_digits > 0;
+        B = (int)std::ceil((dec_digits - 1) * l2_10) + 1;
+        u_s = std::exp2((double)(B - 1) - (dec_digits - 1) * l2_10) * (1.0 + 1e-9);
+        const int F = 64 * (L - I);
+        r_fix_s = std::ldexp(6.5, B - F);
+        E = julia ? std::ldexp(0.75, B - F) : 0.0;  // a Julia orbit starts at the rounded pixel
+        cx = std::fabs(cxd);
+        cy = std::fabs(cyd);
+    }
+    // true when the float64 rounding of a is certain: the error bound is below half its
+    // distance to a rounding boundary (scaled error E: E 2^-B < 2^(ilogb(E) + 1 - B))
+    bool rounds_alike(const Fx& a, int L, int I, double Es) const {
+        if (Es == 0.0) return true;
+        if (!(Es < 1e300)) return false;
+        const int dexp = rounding_distance_exp(a, L, I);
+        return dexp != kNoDist && dexp >= std::ilogb(Es) + 3 - B;
+    }
+};
+
 }  // namespace
 
-extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_limbs,
-                                  int32_t fractal_type,
-                                  int32_t gen_n, int32_t max_iter, int32_t escape_only,
-                                  double* ref_re, double* ref_im, int32_t* ref_len,
-                                  double* escape_mag2, uint64_t* trace_hash) {
+static int orbit_impl(const uint64_t* seeds, int32_t limbs, int32_t int_limbs, int32_t fractal_type,
+                      int32_t gen_n, int32_t max_iter, int32_t escape_only, double* ref_re, double* ref_im,
+                      int32_t* ref_len, double* escape_mag2, uint64_t* trace_hash, int32_t dec_digits,
+                      int32_t* certified) {
+    if (certified) *certified = 0;
     if (!seeds || !ref_len || max_iter < 0 || fractal_type < 0 || fractal_type > 4 ||
         (fractal_type == 4 && (gen_n < 1 || gen_n > 64)) || (!escape_only && (!ref_re || !ref_im))) {
         ap::set_error("ap_reference_orbit: bad arguments");
@@ -351,6 +424,9 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
     std::memset(bail.m, 0, sizeof(u64) * L);
     bail.m[L - I] = 65536;
     bail.neg = 0;
+    Cert cert;
+    if (certified && !escape_only && fractal_type <= 3)
+        cert.start(dec_digits, L, I, to_double(cx, L, I), to_double(cy, L, I), fractal_type >= 2);
 
     const bool periodic = (fractal_type == 0 || fractal_type == 2) && !escape_only;
     int check_step = 8, saved_k = 0;
@@ -383,7 +459,28 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
         SQR(zx2, zx);
         SQR(zy2, zy);
         add(mag, zx2, zy2, L);
-        if (!mag.neg && cmp_mag(mag.m, bail.m, L) > 0) {
+        const bool escaped = !mag.neg && cmp_mag(mag.m, bail.m, L) > 0;
+        double Emag_s = 0.0;
+        if (cert.ok) {
+            // the stored values, then the bailout decision (and |Z|^2 at escape)
+            const double xf = to_double(zx, L, I), yf = to_double(zy, L, I);
+            const double Et = std::ldexp(cert.E, -cert.B);
+            const double az = std::hypot(xf, yf) * (1.0 + 0x1p-48);  // |z| of this run, from above
+            const double ax = std::fabs(xf) * (1.0 + 0x1p-50) + Et, ay = std::fabs(yf) * (1.0 + 0x1p-50) + Et;
+            const double m2 = (az + Et) * (az + Et);                  // |z|^2 of either run, from above
+            const double grow = (2.0 * az + Et) * cert.E * (1.0 + 1e-12);
+            Emag_s = (grow + cert.u_s * 2.0001 * m2 + std::ldexp(2.02, cert.B - 64 * (L - I))) * (1.0 + 1e-12);
+            const double magf = xf * xf + yf * yf;
+            const double margin = std::ldexp(Emag_s, -cert.B) + 65536.0 * 0x1p-48;
+            cert.ok = cert.rounds_alike(zx, L, I, cert.E) && cert.rounds_alike(zy, L, I, cert.E) &&
+                      std::fabs(magf - 65536.0) > margin;
+            if (cert.ok && escaped && escape_mag2) cert.ok = cert.rounds_alike(mag, L, I, Emag_s);
+            // the next step's bound
+            const double rdec = 2.0001 * m2 + 1.0001 * (m2 + cert.cx) + 4.0001 * ax * ay +
+                                1.0001 * (2.0 * ax * ay + cert.cy);
+            cert.E = grow + cert.u_s * rdec * (1.0 + 1e-12) + cert.r_fix_s;
+        }
+        if (escaped) {
             len = k;
             if (escape_mag2) *escape_mag2 = to_double(mag, L, I);
             break;
@@ -402,7 +499,7 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
                 }
                 *ref_len = max_iter;
                 if (trace_hash) *trace_hash = hash;
-                return AP_OK;
+                return AP_OK;  // a copied cycle is not certified: the caller compares two runs
             }
         }
         if (fractal_type == 0 || fractal_type == 2) {  // z^2 + c
@@ -449,5 +546,27 @@ extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t 
     }
     *ref_len = len;
     if (trace_hash) *trace_hash = hash;
+    if (certified) *certified = cert.ok ? 1 : 0;
     return AP_OK;
+}
+
+extern "C" int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_limbs,
+                                  int32_t fractal_type,
+                                  int32_t gen_n, int32_t max_iter, int32_t escape_only,
+                                  double* ref_re, double* ref_im, int32_t* ref_len,
+                                  double* escape_mag2, uint64_t* trace_hash) {
+    return orbit_impl(seeds, limbs, int_limbs, fractal_type, gen_n, max_iter, escape_only, ref_re, ref_im,
+                      ref_len, escape_mag2, trace_hash, 0, nullptr);
+}
+
+extern "C" int ap_reference_orbit_cert(const uint64_t* seeds, int32_t limbs, int32_t int_limbs,
+                                       int32_t fractal_type, int32_t gen_n, int32_t max_iter,
+                                       int32_t dec_digits, double* ref_re, double* ref_im, int32_t* ref_len,
+                                       double* escape_mag2, int32_t* certified) {
+    if (!certified || dec_digits < 1) {
+        ap::set_error("ap_reference_orbit_cert: bad arguments");
+        return AP_E_INVALID;
+    }
+    return orbit_impl(seeds, limbs, int_limbs, fractal_type, gen_n, max_iter, 0, ref_re, ref_im, ref_len,
+                      escape_mag2, nullptr, dec_digits, certified);
 }

@@ -51,35 +51,60 @@ def orbit_limbs(prec_bits, int_limbs=1):
     return lo + int_limbs, hi + int_limbs
 
 
-def to_fixed(value, limbs, int_limbs=1):
-    """A Decimal (or a number's str) as two's-complement fixed point,
-    value * 2^(64 (limbs - int_limbs)) rounded half to even, in little-endian uint64 limbs."""
+def _ratio(value):
+    """A Decimal (or a number's str) as the exact fraction (num, den), den > 0."""
     d = value if isinstance(value, Decimal) else Decimal(str(value))
-    sign, digits, exp = d.as_tuple()
-    n = int("".join(map(str, digits))) if digits else 0
+    return d.as_integer_ratio()
+
+
+def _fixed_from_ratio(num, den, limbs, int_limbs=1):
     shift = 64 * (limbs - int_limbs)
-    if exp >= 0:
-        q = (n * 10 ** exp) << shift
-    else:
-        den = 10 ** (-exp)
-        q, r = divmod(n << shift, den)
-        if 2 * r > den or (2 * r == den and q & 1):
-            q += 1
-    if sign:
+    q, r = divmod(abs(num) << shift, den)
+    if 2 * r > den or (2 * r == den and q & 1):
+        q += 1
+    if num < 0:
         q = -q
     if not -(1 << (64 * limbs - 1)) <= q < (1 << (64 * limbs - 1)):
         raise OverflowError("value outside the fixed-point range")
     return np.frombuffer((q % (1 << (64 * limbs))).to_bytes(8 * limbs, "little"), dtype=np.uint64)
 
 
-def _seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki, limbs, int_limbs=1):
+def to_fixed(value, limbs, int_limbs=1):
+    """A Decimal (or a number's str) as two's-complement fixed point,
+    value * 2^(64 (limbs - int_limbs)) rounded half to even, in little-endian uint64 limbs."""
+    return _fixed_from_ratio(*_ratio(value), limbs, int_limbs)
+
+
+def _seed_values(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki):
     """(z0, c, K) of the orbit, as the reference starts it (math_core/high_precision.py:722-735)."""
     if fractal_type in (2, 3):
         z0x, z0y, c_x, c_y = Decimal(cand_cx), Decimal(cand_cy), Decimal(str(julia_cx)), Decimal(str(julia_cy))
     else:
         z0x, z0y, c_x, c_y = Decimal(0), Decimal(0), Decimal(cand_cx), Decimal(cand_cy)
-    vals = (z0x, z0y, c_x, c_y, Decimal(str(gen_kr)), Decimal(str(gen_ki)))
+    return (z0x, z0y, c_x, c_y, Decimal(str(gen_kr)), Decimal(str(gen_ki)))
+
+
+def _seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki, limbs, int_limbs=1):
+    """The seeds of one orbit in fixed point with `limbs` limbs."""
+    vals = _seed_values(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
     return np.ascontiguousarray(np.concatenate([to_fixed(v, limbs, int_limbs) for v in vals]))
+
+
+class _Seeds:
+    """The seeds of one orbit at any limb count: the exact fractions are formed once
+    (on first use, by whichever thread gets there first), then rounded per limb count."""
+
+    def __init__(self, fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki):
+        self.args = (fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
+        self.ratios = None
+        self.lock = threading.Lock()
+
+    def __call__(self, limbs, int_limbs=1):
+        with self.lock:
+            if self.ratios is None:
+                self.ratios = [_ratio(v) for v in _seed_values(*self.args)]
+        return np.ascontiguousarray(np.concatenate([_fixed_from_ratio(n, d, limbs, int_limbs)
+                                                    for n, d in self.ratios]))
 
 
 def _native():
@@ -132,6 +157,33 @@ def _native_orbit(seeds_fn, L, max_iter, fractal_type, gen_n, with_mag2=False):
     return ref_re, ref_im, int(ref_len.value)
 
 
+def _native_orbit_cert(seeds_fn, L, max_iter, fractal_type, gen_n, dec_digits):
+    """The orbit at L limbs with its proof against the Decimal iteration of dec_digits
+    digits (ap_reference_orbit_cert): (ref_re, ref_im, ref_len, |Z|^2 at escape, certified)."""
+    import ctypes as C
+    from . import _lib
+    I = orbit_int_limbs(fractal_type, gen_n)
+    seeds = seeds_fn(L, I)
+    ref_re = np.zeros(max_iter + 1, dtype=np.float64)
+    ref_im = np.zeros(max_iter + 1, dtype=np.float64)
+    ref_len = C.c_int32(0)
+    mag2 = C.c_double(0.0)
+    cert = C.c_int32(0)
+    _lib.check(_native().ap_reference_orbit_cert(
+        seeds.ctypes.data_as(C.c_void_p), L, I, int(fractal_type), int(gen_n), int(max_iter), int(dec_digits),
+        ref_re.ctypes.data_as(C.c_void_p), ref_im.ctypes.data_as(C.c_void_p), C.byref(ref_len),
+        C.byref(mag2), C.byref(cert)), "ap_reference_orbit_cert")
+    return ref_re, ref_im, int(ref_len.value), float(mag2.value), bool(cert.value)
+
+
+def _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits):
+    """The higher-precision run, certified against the Decimal iteration where the
+    formula is quadratic: (ref_re, ref_im, ref_len, |Z|^2 at escape, certified)."""
+    if fractal_type <= 3:
+        return _native_orbit_cert(seeds, hi, max_iter, fractal_type, gen_n, _orbit_digits(prec_bits))
+    return _native_orbit(seeds, hi, max_iter, fractal_type, gen_n, with_mag2=True) + (False,)
+
+
 def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
                                   julia_cx=0.0, julia_cy=0.0, prec_bits=256,
                                   gen_n=3, gen_kr=0.25, gen_ki=1.0):
@@ -142,24 +194,38 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     power-of-two checkpoints and its cycle is copied to the end of the arrays
     (math_core/high_precision.py:706-875).
 
-    The orbit runs natively (ap_reference_orbit) in binary fixed point twice, with
-    64 fractional bits fewer and 64 more than the reference's Decimal digits
-    carry.  When both give the same float64 orbit, the Decimal orbit, whose
-    precision lies between them, gives it too, and that orbit is returned.  When
-    they differ, the orbit has run through the available precision (a bounded
-    chaotic orbit): it is then iterated in Decimal exactly as the reference does.
+    The orbit runs natively in binary fixed point with 64 fractional bits more than
+    the reference's Decimal digits carry.  For the quadratic formulas the run carries
+    a bound on its distance from the Decimal iteration (ap_reference_orbit_cert); where
+    the bound proves every float64 value and bailout decision equal, that orbit is
+    returned.  Otherwise the orbit runs again with 64 fractional bits fewer than the
+    Decimal digits: when both give the same float64 orbit, the Decimal orbit, whose
+    precision lies between them, gives it too.  When they differ, the orbit has run
+    through the available precision (a bounded chaotic orbit): it is then iterated in
+    Decimal exactly as the reference does.
     """
     lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+    seeds = _Seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki)
+    if fractal_type <= 3:
+        a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+        b = None if a[4] else _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
+    else:
+        fa = _pair_pool().submit(_first_run, seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+        b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
+        a = fa.result()
+    return _certified_orbit(a, b, cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,
+                            prec_bits, gen_n, gen_kr, gen_ki)
 
-    def seeds(L, I):
-        return _seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki, L, I)
 
-    fa = _pair_pool().submit(_native_orbit, seeds, hi, max_iter, fractal_type, gen_n)
-    b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
-    a = fa.result()
+def _certified_orbit(a, b, cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
+                     gen_n, gen_kr, gen_ki):
+    """The orbit of the higher-precision run a when it is certified on its own (b None) or
+    the lower one b gives the same float64 orbit, else the exact Decimal orbit."""
+    if b is None:
+        return a[:3]
     n = a[2] + 1  # past ref_len both hold zeros, or the same copied cycle
     if a[2] == b[2] and np.array_equal(a[0][:n], b[0][:n]) and np.array_equal(a[1][:n], b[1][:n]):
-        return a
+        return a[:3]
     return decimal_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,
                          prec_bits, gen_n, gen_kr, gen_ki)
 
@@ -218,18 +284,56 @@ def probe_candidate(cand_cx, cand_cy, max_iter, fractal_type=0, julia_cx=0.0, ju
     returns, from one pair of certified native runs (orbit None when the runs
     disagree; the escape scalar is then the exact Decimal one)."""
     lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+    seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
+    a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+    b = None if a[4] else _native_orbit(seeds, lo, max_iter, fractal_type, gen_n, with_mag2=True)
+    return _certified_probe(a, b, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
+                            gen_n, gen_kr, gen_ki)
 
-    def seeds(L, I):
-        return _seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki, L, I)
 
-    a = _native_orbit(seeds, hi, max_iter, fractal_type, gen_n, with_mag2=True)
-    b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n, with_mag2=True)
+def _certified_probe(a, b, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits, gen_n,
+                     gen_kr, gen_ki):
+    """(escape scalar, orbit) from the higher-precision run a when it is certified on its
+    own (b None) or agrees with the lower one b on the float64 orbit and |Z|^2 at escape,
+    else (the exact Decimal scalar, None)."""
+    if b is None:
+        return _smooth_escape(a[2], a[3], max_iter, fractal_type, gen_n), a[:3]
     n = a[2] + 1
     if (a[2] == b[2] and (a[2] >= max_iter or a[3] == b[3]) and np.array_equal(a[0][:n], b[0][:n])
             and np.array_equal(a[1][:n], b[1][:n])):
         return _smooth_escape(a[2], a[3], max_iter, fractal_type, gen_n), a[:3]
     return decimal_escape_scalar(cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
                                  gen_n, gen_kr, gen_ki), None
+
+
+class _Runs:
+    """The native runs of one orbit on a pool: the higher-precision one at once (certified
+    on its own for the quadratic formulas), the lower one beside it for Multibrot, else
+    only if the first is not certified."""
+
+    def __init__(self, pool, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits, gen_n,
+                 gen_kr, gen_ki):
+        self.lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+        self.seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
+        self.args = (max_iter, fractal_type, gen_n)
+        self.first = pool.submit(_first_run, self.seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+        self.second = (pool.submit(_native_orbit, self.seeds, self.lo, max_iter, fractal_type, gen_n, True)
+                       if fractal_type > 3 else None)
+
+    def result(self):
+        """(first run, second run or None when the first is certified)."""
+        a = self.first.result()
+        if a[4]:
+            if self.second is not None:
+                self.second.cancel()
+            return a, None
+        b = self.second.result() if self.second is not None else _native_orbit(self.seeds, self.lo, *self.args, True)
+        return a, b
+
+    def cancel(self):
+        self.first.cancel()
+        if self.second is not None:
+            self.second.cancel()
 
 
 # Exact Decimal iteration in the reference's operation order: the path for orbits the
@@ -494,9 +598,11 @@ def find_optimal_reference_orbit(cx_dec, cy_dec, pw_dec, ph_dec, max_iter, scree
         # 0.6 max_iter, the usual case deep in a zoom) runs beside the centre's orbit,
         # and each candidate keeps its certified orbit, so the winner is not iterated
         # twice.  Results and choice are those of the sequential reference.
+        # Every orbit is two native runs (two precisions, certified against each
+        # other); each run is a task of its own, so the cores share the 34 runs evenly.
         pool = _probe_pool()
-        centre = pool.submit(compute_single_highprec_orbit, cx_dec, cy_dec, max_iter, fractal_type,
-                             julia_cx, julia_cy, bits, gen_n, gen_kr, gen_ki)
+        args = (max_iter, fractal_type, julia_cx, julia_cy, bits, gen_n, gen_kr, gen_ki)
+        centre = _Runs(pool, cx_dec, cy_dec, *args)
         probes = []
 
         def submit_probes():
@@ -504,14 +610,12 @@ def find_optimal_reference_orbit(cx_dec, cy_dec, pw_dec, ph_dec, max_iter, scree
                 with localcontext(ctx):
                     cand_x = x_min_dec + Decimal(str(u)) * pw_dec
                     cand_y = y_max_dec - Decimal(str(v)) * ph_dec
-                probes.append((pool.submit(probe_candidate, cand_x, cand_y, max_iter, fractal_type,
-                                           julia_cx, julia_cy, bits, gen_n, gen_kr, gen_ki),
-                               cand_x, cand_y, u, v))
+                probes.append((_Runs(pool, cand_x, cand_y, *args), cand_x, cand_y, u, v))
 
         may_probe = pw_dec >= Decimal("1e-10000")
         if may_probe and speculate:
             submit_probes()
-        ref_re, ref_im, ref_len = centre.result()
+        ref_re, ref_im, ref_len = _certified_orbit(*centre.result(), cx_dec, cy_dec, *args)
         best_cx, best_cy, best_u, best_v = cx_dec, cy_dec, 0.5, 0.5
 
         if ref_len < int(max_iter * 0.6) and may_probe:
@@ -519,8 +623,8 @@ def find_optimal_reference_orbit(cx_dec, cy_dec, pw_dec, ph_dec, max_iter, scree
                 submit_probes()
             best_esc = max(int(ref_len * 1.2), ref_len + 32)
             cand, cand_orbit = (cx_dec, cy_dec, 0.5, 0.5), None
-            for fut, cand_x, cand_y, u, v in probes:
-                esc, orbit = fut.result()
+            for runs, cand_x, cand_y, u, v in probes:
+                esc, orbit = _certified_probe(*runs.result(), cand_x, cand_y, *args)
                 if esc > best_esc:
                     best_esc = esc
                     cand, cand_orbit = (cand_x, cand_y, u, v), orbit
@@ -534,8 +638,8 @@ def find_optimal_reference_orbit(cx_dec, cy_dec, pw_dec, ph_dec, max_iter, scree
                     ref_re, ref_im, ref_len = c_re, c_im, c_len
                     best_cx, best_cy, best_u, best_v = cand
         else:
-            for fut, *_ in probes:
-                fut.cancel()  # not needed: drop those not started
+            for runs, *_ in probes:
+                runs.cancel()  # not needed: drop those not started
 
         if can_reuse and best_entry is not None and best_entry["ref_len"] > ref_len:
             u = float((best_entry["cx_dec"] - x_min_dec) / pw_dec)
