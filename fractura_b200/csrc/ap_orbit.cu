@@ -145,16 +145,6 @@ inline void sqr(Fx& r, const Fx& a, int L, int I) {
     r.neg = 0;
 }
 
-inline void twice(Fx& r, const Fx& a, int L) {
-    u64 carry = 0;
-    for (int i = 0; i < L; ++i) {
-        const u64 v = a.m[i];
-        r.m[i] = (v << 1) | carry;
-        carry = v >> 63;
-    }
-    r.neg = a.neg;
-}
-
 // mul and sqr with the limb counts fixed at compile time: the same partial products
 // and column sums as mul / sqr, every column written out by the templates below.  An orbit picks its pair
 // once (pick_products); sizes outside the table use the runtime-bound forms.
@@ -310,8 +300,9 @@ inline bool equal(const Fx& a, const Fx& b, int L) {
 // ---- Certification against the Decimal iteration (quadratic formulas) ----------------
 // The reference iterates the orbit in Decimal with P significant digits; every operation
 // rounds with relative error at most u = 5 10^-P.  The run here is fixed point with F
-// fractional bits; a truncated product is off by less than 1.01 units of 2^-F, a stored
-// seed by 0.5.  Both follow the same map.  In the complex modulus, z^2 moves by at most
+// fractional bits; a truncated square is off by less than 1.01 units of 2^-F (so x^2 - y^2
+// by 2.02 and 2 x y = (x + y)^2 - x^2 - y^2 by 3.03), a stored seed by 0.5.  Both follow the
+// same map.  In the complex modulus, z^2 moves by at most
 // (2 |z| + E) E when z moves by E, and so does Burning Ship's step, whose fold
 // (x, y) -> (|x|, |y|) moves no point farther; so the two runs' distance obeys
 //   E_{k+1} <= (2 |z| + E_k) E_k + r_dec + r_fix,
@@ -503,17 +494,21 @@ static int orbit_impl(const uint64_t* seeds, int32_t limbs, int32_t int_limbs, i
             }
         }
         if (fractal_type == 0 || fractal_type == 2) {  // z^2 + c
-            MUL(t0, zx, zy);
+            // 2 x y = (x + y)^2 - x^2 - y^2: a square costs about half a product
+            add(t2, zx, zy, L);
+            SQR(t0, t2);
+            sub(t0, t0, zx2, L);
+            sub(t0, t0, zy2, L);
             sub(t1, zx2, zy2, L);
             add(zx, t1, cx, L);
-            twice(t0, t0, L);
             add(zy, t0, cy, L);
         } else if (fractal_type == 1 || fractal_type == 3) {  // Burning Ship: 2|x||y| - c_y
-            MUL(t0, zx, zy);
-            t0.neg = 0;  // |x| |y|
+            add_s(t2, zx, 0, zy, 0, L);  // |x| + |y|
+            SQR(t0, t2);
+            sub(t0, t0, zx2, L);
+            sub(t0, t0, zy2, L);
             sub(t1, zx2, zy2, L);
             add(zx, t1, cx, L);
-            twice(t0, t0, L);
             sub(zy, t0, cy, L);
         } else {  // Multibrot z^n + K z + c
             Fx& nr = v[12];  // the checkpoint slots are free: no period detection here
