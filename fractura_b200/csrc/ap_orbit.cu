@@ -311,8 +311,9 @@ inline bool equal(const Fx& a, const Fx& b, int L) {
 // the fixed-point value plus E.  The two float64 roundings of a component agree wherever
 // E_k is below half its distance to the nearest float64 rounding boundary (half: the
 // boundaries below a power of two are twice as dense), and the bailout decisions agree
-// wherever |Z|^2 is farther from 65536 than its own error bound.  E is held scaled by
-// 2^B (u 2^B in [1, 2)), so it neither underflows nor overflows.
+// wherever |Z|^2 is farther from 65536 than its own error bound.  Multibrot z^n + k z + c
+// grows the bound by (|z| + E)^n - |z|^n + |k| E, with the roundings of its power loop.
+// E is held scaled by 2^B (u 2^B in [1, 2)), so it neither underflows nor overflows.
 constexpr int kNoDist = -(1 << 30);
 
 u64 bits_at(const Fx& a, int L, int lo_bit) {  // bits [lo_bit, lo_bit + 63]; zero outside [0, 64 L)
@@ -347,19 +348,23 @@ struct Cert {
     int B = 0;              // scaled quantities are value * 2^B
     double u_s = 0.0;       // Decimal unit roundoff, scaled
     double r_fix_s = 0.0;   // the fixed-point run's error per step, scaled
-    double E = 0.0;         // the bound on |z_Decimal - z_fixed| (max norm), scaled
-    double cx = 0.0, cy = 0.0;
+    double E = 0.0;         // the bound on |z_Decimal - z_fixed| (complex modulus), scaled
+    double cx = 0.0, cy = 0.0, cabs = 0.0, kabs = 0.0;
+    double ulp_s = 0.0;     // 2^-F, scaled
 
-    void start(int dec_digits, int L, int I, double cxd, double cyd, bool julia) {
+    void start(int dec_digits, int L, int I, double cxd, double cyd, double krd, double kid, bool julia) {
         const double l2_10 = 3.3219280948873623478703194294894;
         ok = dec_digits > 0;
         B = (int)std::ceil((dec_digits - 1) * l2_10) + 1;
         u_s = std::exp2((double)(B - 1) - (dec_digits - 1) * l2_10) * (1.0 + 1e-9);
         const int F = 64 * (L - I);
-        r_fix_s = std::ldexp(6.5, B - F);
-        E = julia ? std::ldexp(0.75, B - F) : 0.0;  // a Julia orbit starts at the rounded pixel
+        ulp_s = std::ldexp(1.0, B - F);
+        r_fix_s = 6.5 * ulp_s;
+        E = julia ? 0.75 * ulp_s : 0.0;  // a Julia orbit starts at the rounded pixel
         cx = std::fabs(cxd);
         cy = std::fabs(cyd);
+        cabs = std::hypot(cxd, cyd) * (1.0 + 0x1p-48);
+        kabs = std::hypot(krd, kid) * (1.0 + 0x1p-48);
     }
     // true when the float64 rounding of a is certain: the error bound is below half its
     // distance to a rounding boundary (scaled error E: E 2^-B < 2^(ilogb(E) + 1 - B))
@@ -416,8 +421,9 @@ static int orbit_impl(const uint64_t* seeds, int32_t limbs, int32_t int_limbs, i
     bail.m[L - I] = 65536;
     bail.neg = 0;
     Cert cert;
-    if (certified && !escape_only && fractal_type <= 3)
-        cert.start(dec_digits, L, I, to_double(cx, L, I), to_double(cy, L, I), fractal_type >= 2);
+    if (certified && !escape_only)
+        cert.start(dec_digits, L, I, to_double(cx, L, I), to_double(cy, L, I), to_double(kr, L, I),
+                   to_double(ki, L, I), fractal_type == 2 || fractal_type == 3);
 
     const bool periodic = (fractal_type == 0 || fractal_type == 2) && !escape_only;
     int check_step = 8, saved_k = 0;
@@ -459,17 +465,43 @@ static int orbit_impl(const uint64_t* seeds, int32_t limbs, int32_t int_limbs, i
             const double az = std::hypot(xf, yf) * (1.0 + 0x1p-48);  // |z| of this run, from above
             const double ax = std::fabs(xf) * (1.0 + 0x1p-50) + Et, ay = std::fabs(yf) * (1.0 + 0x1p-50) + Et;
             const double m2 = (az + Et) * (az + Et);                  // |z|^2 of either run, from above
-            const double grow = (2.0 * az + Et) * cert.E * (1.0 + 1e-12);
-            Emag_s = (grow + cert.u_s * 2.0001 * m2 + std::ldexp(2.02, cert.B - 64 * (L - I))) * (1.0 + 1e-12);
+            // |z|^2 moves by at most (2 |z| + E) E
+            const double grow2 = (2.0 * az + Et) * cert.E * (1.0 + 1e-12);
+            Emag_s = (grow2 + cert.u_s * 2.0001 * m2 + 2.02 * cert.ulp_s) * (1.0 + 1e-12);
             const double magf = xf * xf + yf * yf;
             const double margin = std::ldexp(Emag_s, -cert.B) + 65536.0 * 0x1p-48;
             cert.ok = cert.rounds_alike(zx, L, I, cert.E) && cert.rounds_alike(zy, L, I, cert.E) &&
                       std::fabs(magf - 65536.0) > margin;
             if (cert.ok && escaped && escape_mag2) cert.ok = cert.rounds_alike(mag, L, I, Emag_s);
             // the next step's bound
-            const double rdec = 2.0001 * m2 + 1.0001 * (m2 + cert.cx) + 4.0001 * ax * ay +
-                                1.0001 * (2.0 * ax * ay + cert.cy);
-            cert.E = grow + cert.u_s * rdec * (1.0 + 1e-12) + cert.r_fix_s;
+            if (fractal_type <= 3) {
+                const double rdec = 2.0001 * m2 + 1.0001 * (m2 + cert.cx) + 4.0001 * ax * ay +
+                                    1.0001 * (2.0 * ax * ay + cert.cy);
+                cert.E = grow2 + cert.u_s * rdec * (1.0 + 1e-12) + cert.r_fix_s;
+            } else {
+                // z^n + k z + c moves by at most (|z| + E)^n - |z|^n + |k| E, expanded so that
+                // nothing cancels: E sum_{j=1..n} C(n, j) |z|^(n-j) E^(j-1)
+                const int nn = gen_n;
+                double sum = 0.0, c = nn, ep = 1.0, A = az + Et, An = 1.0, geo = 0.0, aj = 1.0;
+                for (int j = 1; j <= nn; ++j) {
+                    sum += c * std::pow(az, nn - j) * ep;
+                    c = c * (nn - j) / (j + 1);
+                    ep *= Et;
+                }
+                for (int j = 0; j < nn; ++j) An *= A;
+                for (int j = 0; j <= nn - 2; ++j) {  // 1 + |z| + ... + |z|^(n-2)
+                    geo += aj;
+                    aj *= az;
+                }
+                const double grow = (sum + cert.kabs) * cert.E * (1.0 + 1e-10);
+                // the Decimal loop rounds 4 products and 2 sums per power, the k z products
+                // and the final sums; the fixed-point run truncates 4 products per power (an
+                // error that the later powers multiply by |z|) and 4 for k z, and carries the
+                // rounded k and c
+                const double rdec = (4.0004 * (nn - 1) + 2.0002) * An + 6.0006 * cert.kabs * A + 2.0002 * cert.cabs;
+                const double rfix = (2.86 * (geo + 1.0) + 0.71 * (az + 1.0)) * cert.ulp_s;
+                cert.E = grow + cert.u_s * rdec * (1.0 + 1e-10) + rfix * (1.0 + 1e-10);
+            }
         }
         if (escaped) {
             len = k;

@@ -112,14 +112,13 @@ def _native():
     return _lib.load()
 
 
-_PAIR_POOL = None
 _PROBE_POOL = None
 _PAIR_LOCK = threading.Lock()
 
 
 def _probe_pool():
     """Threads for the centre orbit and the probe candidates of
-    find_optimal_reference_orbit (one task per orbit pair; the native runs release
+    find_optimal_reference_orbit (one task per native run; the native runs release
     the GIL)."""
     global _PROBE_POOL
     with _PAIR_LOCK:
@@ -127,16 +126,6 @@ def _probe_pool():
             _PROBE_POOL = ThreadPoolExecutor(max_workers=max(2, os.cpu_count() or 4),
                                              thread_name_prefix="probe")
         return _PROBE_POOL
-
-
-def _pair_pool():
-    """Threads that run the higher-precision orbit beside the lower one (the native
-    call releases the GIL)."""
-    global _PAIR_POOL
-    with _PAIR_LOCK:
-        if _PAIR_POOL is None:
-            _PAIR_POOL = ThreadPoolExecutor(max_workers=4, thread_name_prefix="orbit")
-        return _PAIR_POOL
 
 
 def _native_orbit(seeds_fn, L, max_iter, fractal_type, gen_n, with_mag2=False):
@@ -177,11 +166,9 @@ def _native_orbit_cert(seeds_fn, L, max_iter, fractal_type, gen_n, dec_digits):
 
 
 def _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits):
-    """The higher-precision run, certified against the Decimal iteration where the
-    formula is quadratic: (ref_re, ref_im, ref_len, |Z|^2 at escape, certified)."""
-    if fractal_type <= 3:
-        return _native_orbit_cert(seeds, hi, max_iter, fractal_type, gen_n, _orbit_digits(prec_bits))
-    return _native_orbit(seeds, hi, max_iter, fractal_type, gen_n, with_mag2=True) + (False,)
+    """The higher-precision run with its certificate against the Decimal iteration:
+    (ref_re, ref_im, ref_len, |Z|^2 at escape, certified)."""
+    return _native_orbit_cert(seeds, hi, max_iter, fractal_type, gen_n, _orbit_digits(prec_bits))
 
 
 def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
@@ -195,8 +182,8 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     (math_core/high_precision.py:706-875).
 
     The orbit runs natively in binary fixed point with 64 fractional bits more than
-    the reference's Decimal digits carry.  For the quadratic formulas the run carries
-    a bound on its distance from the Decimal iteration (ap_reference_orbit_cert); where
+    the reference's Decimal digits carry.  The run carries a bound on its distance
+    from the Decimal iteration (ap_reference_orbit_cert); where
     the bound proves every float64 value and bailout decision equal, that orbit is
     returned.  Otherwise the orbit runs again with 64 fractional bits fewer than the
     Decimal digits: when both give the same float64 orbit, the Decimal orbit, whose
@@ -206,13 +193,8 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     """
     lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
     seeds = _Seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki)
-    if fractal_type <= 3:
-        a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
-        b = None if a[4] else _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
-    else:
-        fa = _pair_pool().submit(_first_run, seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
-        b = _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
-        a = fa.result()
+    a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+    b = None if a[4] else _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
     return _certified_orbit(a, b, cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,
                             prec_bits, gen_n, gen_kr, gen_ki)
 
@@ -307,9 +289,8 @@ def _certified_probe(a, b, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, j
 
 
 class _Runs:
-    """The native runs of one orbit on a pool: the higher-precision one at once (certified
-    on its own for the quadratic formulas), the lower one beside it for Multibrot, else
-    only if the first is not certified."""
+    """The native runs of one orbit on a pool: the higher-precision one at once, with its
+    certificate; the lower one only if that run is not certified."""
 
     def __init__(self, pool, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits, gen_n,
                  gen_kr, gen_ki):
@@ -317,23 +298,16 @@ class _Runs:
         self.seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
         self.args = (max_iter, fractal_type, gen_n)
         self.first = pool.submit(_first_run, self.seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
-        self.second = (pool.submit(_native_orbit, self.seeds, self.lo, max_iter, fractal_type, gen_n, True)
-                       if fractal_type > 3 else None)
 
     def result(self):
         """(first run, second run or None when the first is certified)."""
         a = self.first.result()
         if a[4]:
-            if self.second is not None:
-                self.second.cancel()
             return a, None
-        b = self.second.result() if self.second is not None else _native_orbit(self.seeds, self.lo, *self.args, True)
-        return a, b
+        return a, _native_orbit(self.seeds, self.lo, *self.args, True)
 
     def cancel(self):
         self.first.cancel()
-        if self.second is not None:
-            self.second.cancel()
 
 
 # Exact Decimal iteration in the reference's operation order: the path for orbits the

@@ -357,8 +357,8 @@ AP_API int ap_reference_orbit(const uint64_t* seeds, int32_t limbs, int32_t int_
  * a running error bound (the Decimal roundings, 5 10^-dec_digits per operation, and this
  * run's truncations, grown by the map) shows that every stored float64 value, every
  * bailout decision and the escape |Z|^2 equal the Decimal iteration's; 0 otherwise (a
- * copied cycle, Multibrot, or a bound too wide somewhere), when the caller compares two
- * precisions instead.  Fractal types 0..3; dec_digits >= 1. */
+ * copied cycle, or a bound too wide somewhere), when the caller compares two precisions
+ * instead.  Every fractal type; dec_digits >= 1. */
 AP_API int ap_reference_orbit_cert(const uint64_t* seeds, int32_t limbs, int32_t int_limbs,
                                    int32_t fractal_type, int32_t gen_n, int32_t max_iter,
                                    int32_t dec_digits, double* ref_re, double* ref_im, int32_t* ref_len,

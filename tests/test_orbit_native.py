@@ -182,7 +182,7 @@ def test_fixed_size_products_at_every_size(fractal_type, gen_n, int_limbs):
 
 
 @pytest.mark.parametrize("prec_bits", [256, 700])
-@pytest.mark.parametrize("formula", FORMULAS[:4], ids=lambda f: f"type{f[0]}")
+@pytest.mark.parametrize("formula", FORMULAS, ids=lambda f: f"type{f[0]}_n{f[2]}")
 def test_certified_runs_equal_decimal(formula, prec_bits):
     """ap_reference_orbit_cert: wherever its error bound certifies a run, the float64 orbit,
     the escape step and |Z|^2 at escape equal the Decimal loop's; and most seeded points
@@ -190,7 +190,7 @@ def test_certified_runs_equal_decimal(formula, prec_bits):
     ft, (jx, jy), n, kr, ki = formula
     lo, hi = hp.orbit_limbs(prec_bits, hp.orbit_int_limbs(ft, n))
     certified = 0
-    pts = _points(prec_bits + 7 * ft + 1, 8, ft)
+    pts = _points(prec_bits + 7 * ft + n, 8, ft)
     for cx, cy in pts:
         seeds = hp._Seeds(ft, cx, cy, jx, jy, kr, ki)
         a = hp._first_run(seeds, hi, 3000, ft, n, prec_bits)
