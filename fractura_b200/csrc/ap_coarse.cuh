@@ -29,6 +29,20 @@ constexpr int kFtQuad = 0;   // Mandelbrot (0) and its Julia set (2)
 constexpr int kFtShip = 1;   // Burning Ship (1) and its Julia set (3)
 constexpr int kFtMulti = 4;  // Multibrot z^n + k z + c
 
+// Calls power() n - 1 times, the common degrees unrolled: the same operations in the
+// same order, and what the last call prepares for a next one is dead and goes.
+template <typename F>
+__device__ __forceinline__ void for_powers(int n, F&& power) {
+    switch (n) {
+    case 2: power(); break;
+    case 3: power(); power(); break;
+    case 4: power(); power(); power(); break;
+    case 5: power(); power(); power(); power(); break;
+    default:
+        for (int t = 0; t < n - 1; ++t) power();
+    }
+}
+
 // 32-byte record through the read-only path (two 16-byte loads).
 __device__ __forceinline__ double4 ldg4(const double4* p) {
     const double2* q = reinterpret_cast<const double2*>(p);
@@ -208,7 +222,7 @@ __device__ __forceinline__ void pixel_advance(const ApFrameParams& p, const ApFr
                 dzx = nx;
             } else {
                 double pr = dzx, pi = dzy, qr = rx, qi = ry;
-                for (int t = 0; t < p.gen_n - 1; ++t) {
+                for_powers(p.gen_n, [&]() {
                     const double t1r = pr * rx - pi * ry, t1i = pr * ry + pi * rx;
                     const double sr = pr + qr, si = pi + qi;
                     const double t2r = sr * dzx - si * dzy, t2i = sr * dzy + si * dzx;
@@ -217,7 +231,7 @@ __device__ __forceinline__ void pixel_advance(const ApFrameParams& p, const ApFr
                     const double nqr = qr * rx - qi * ry, nqi = qr * ry + qi * rx;
                     qr = nqr;
                     qi = nqi;
-                }
+                });
                 const double kzr = p.gen_kr * dzx - p.gen_ki * dzy;
                 const double kzi = p.gen_kr * dzy + p.gen_ki * dzx;
                 dzx = pr + kzr + dcpx;
@@ -280,11 +294,11 @@ __device__ __forceinline__ void pixel_advance(const ApFrameParams& p, const ApFr
                 zx = zx2 - zy2 + cx;
             } else {
                 double zr = zx, zi = zy;
-                for (int t = 0; t < p.gen_n - 1; ++t) {
+                for_powers(p.gen_n, [&]() {
                     const double nr = zr * zx - zi * zy, ni = zr * zy + zi * zx;
                     zr = nr;
                     zi = ni;
-                }
+                });
                 const double kzr = p.gen_kr * zx - p.gen_ki * zy;
                 const double kzi = p.gen_kr * zy + p.gen_ki * zx;
                 zx = zr + kzr + cx;
@@ -478,7 +492,7 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
             // (Z + dz)^n - Z^n by P_{j+1} = P_j Z + (P_j + Z^j) dz, each complex product
             // sum as one chain of fused multiply-adds, then + k dz + dc
             double pr = dzx, pi = dzy, qr = rx, qi = ry;
-            for (int t = 0; t < p.gen_n - 1; ++t) {
+            for_powers(p.gen_n, [&]() {
                 const double sr = pr + qr, si = pi + qi;
                 const double npr = fma(pr, rx, fma(-pi, ry, fma(sr, dzx, -si * dzy)));
                 const double npi = fma(pr, ry, fma(pi, rx, fma(sr, dzy, si * dzx)));
@@ -487,13 +501,13 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                 pi = npi;
                 qr = nqr;
                 qi = nqi;
-            }
+            });
             const double ox = dzx, oy = dzy;
             dzx = fma(p.gen_kr, ox, fma(-p.gen_ki, oy, pr + dcpx));
             dzy = fma(p.gen_kr, oy, fma(p.gen_ki, ox, pi + dcpy));
         } else {
             double pr = dzx, pi = dzy, qr = rx, qi = ry;
-            for (int t = 0; t < p.gen_n - 1; ++t) {
+            for_powers(p.gen_n, [&]() {
                 const double t1r = pr * rx - pi * ry, t1i = pr * ry + pi * rx;
                 const double sr = pr + qr, si = pi + qi;
                 const double t2r = sr * dzx - si * dzy, t2i = sr * dzy + si * dzx;
@@ -502,7 +516,7 @@ __device__ __forceinline__ void rebase_advance(const ApFrameParams& p, const ApF
                 const double nqr = qr * rx - qi * ry, nqi = qr * ry + qi * rx;
                 qr = nqr;
                 qi = nqi;
-            }
+            });
             const double kzr = p.gen_kr * dzx - p.gen_ki * dzy;
             const double kzi = p.gen_kr * dzy + p.gen_ki * dzx;
             dzx = pr + kzr + dcpx;

@@ -114,7 +114,7 @@ __device__ __forceinline__ void fe32_step_fp64(const ApFrameParams& p, double Zx
         ny = 2.0 * (fabs(Zx) * ddy + fabs(Zy) * ddx + se * ddx * ddy) - cy;
     } else {
         double pr = x, pi = y, qr = Zx, qi = Zy;
-        for (int t = 0; t < p.gen_n - 1; ++t) {
+        for_powers(p.gen_n, [&]() {
             const double sr = se * pr + qr, si = se * pi + qi;
             const double npr = (pr * Zx - pi * Zy) + (sr * x - si * y);
             const double npi = (pr * Zy + pi * Zx) + (sr * y + si * x);
@@ -123,7 +123,7 @@ __device__ __forceinline__ void fe32_step_fp64(const ApFrameParams& p, double Zx
             pi = npi;
             qr = nqr;
             qi = nqi;
-        }
+        });
         nx = pr + (p.gen_kr * x - p.gen_ki * y) + cx;
         ny = pi + (p.gen_kr * y + p.gen_ki * x) + cy;
     }
@@ -168,7 +168,7 @@ __device__ __forceinline__ void fe32_step(const ApFrameParams& p, const float4 Z
         wy = ny;
     } else {
         float pr = wx, pi = wy, qr = Z.x, qi = Z.y;
-        for (int t = 0; t < p.gen_n - 1; ++t) {
+        for_powers(p.gen_n, [&]() {
             const float sr = fmaf(S, pr, qr), si = fmaf(S, pi, qi);
             const float npr = fmaf(pr, Z.x, fmaf(-pi, Z.y, fmaf(sr, wx, -si * wy)));
             const float npi = fmaf(pr, Z.y, fmaf(pi, Z.x, fmaf(sr, wy, si * wx)));
@@ -177,7 +177,7 @@ __device__ __forceinline__ void fe32_step(const ApFrameParams& p, const float4 Z
             pi = npi;
             qr = nqr;
             qi = nqi;
-        }
+        });
         const float nx = fmaf(kr, wx, fmaf(-ki, wy, pr + Dx));
         const float ny = fmaf(kr, wy, fmaf(ki, wx, pi + Dy));
         wx = nx;
@@ -197,11 +197,11 @@ __device__ __forceinline__ void fe32_direct_step(const ApFrameParams& p, double&
         zx = zx2 - zy2 + cx;
     } else {
         double zr = zx, zi = zy;
-        for (int t = 0; t < p.gen_n - 1; ++t) {
+        for_powers(p.gen_n, [&]() {
             const double nr = zr * zx - zi * zy, ni = zr * zy + zi * zx;
             zr = nr;
             zi = ni;
-        }
+        });
         const double kzr = p.gen_kr * zx - p.gen_ki * zy;
         const double kzi = p.gen_kr * zy + p.gen_ki * zx;
         zx = zr + kzr + cx;
