@@ -165,10 +165,21 @@ def _native_orbit_cert(seeds_fn, L, max_iter, fractal_type, gen_n, dec_digits):
     return ref_re, ref_im, int(ref_len.value), float(mag2.value), bool(cert.value)
 
 
-def _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits):
-    """The higher-precision run with its certificate against the Decimal iteration:
+def _first_run(seeds, L, max_iter, fractal_type, gen_n, prec_bits):
+    """A run at L limbs with its certificate against the Decimal iteration:
     (ref_re, ref_im, ref_len, |Z|^2 at escape, certified)."""
-    return _native_orbit_cert(seeds, hi, max_iter, fractal_type, gen_n, _orbit_digits(prec_bits))
+    return _native_orbit_cert(seeds, L, max_iter, fractal_type, gen_n, _orbit_digits(prec_bits))
+
+
+def _certify_runs(first, seeds, lo, hi, max_iter, fractal_type, gen_n, prec_bits):
+    """(run, None) for the first certified run -- the lower precision's `first`, else one
+    at the higher precision -- or (higher run, lower run) for the two-run comparison when
+    neither bound certifies.  The bound counts the run's own truncations, so the cheaper
+    run certifies whenever its bits suffice."""
+    if first[4]:
+        return first, None
+    a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+    return (a, None) if a[4] else (a, first)
 
 
 def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
@@ -181,20 +192,20 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     power-of-two checkpoints and its cycle is copied to the end of the arrays
     (math_core/high_precision.py:706-875).
 
-    The orbit runs natively in binary fixed point with 64 fractional bits more than
-    the reference's Decimal digits carry.  The run carries a bound on its distance
-    from the Decimal iteration (ap_reference_orbit_cert); where
-    the bound proves every float64 value and bailout decision equal, that orbit is
-    returned.  Otherwise the orbit runs again with 64 fractional bits fewer than the
-    Decimal digits: when both give the same float64 orbit, the Decimal orbit, whose
+    The orbit runs natively in binary fixed point, first with 64 fractional bits fewer
+    than the reference's Decimal digits carry, then, if needed, with 64 more.  Each
+    run carries a bound on its distance from the Decimal iteration
+    (ap_reference_orbit_cert); where the bound proves every float64 value and bailout
+    decision equal, that orbit is returned.  When neither run is certified, they are
+    compared: when both give the same float64 orbit, the Decimal orbit, whose
     precision lies between them, gives it too.  When they differ, the orbit has run
     through the available precision (a bounded chaotic orbit): it is then iterated in
     Decimal exactly as the reference does.
     """
     lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
     seeds = _Seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki)
-    a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
-    b = None if a[4] else _native_orbit(seeds, lo, max_iter, fractal_type, gen_n)
+    a, b = _certify_runs(_first_run(seeds, lo, max_iter, fractal_type, gen_n, prec_bits), seeds, lo, hi,
+                         max_iter, fractal_type, gen_n, prec_bits)
     return _certified_orbit(a, b, cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,
                             prec_bits, gen_n, gen_kr, gen_ki)
 
@@ -267,8 +278,8 @@ def probe_candidate(cand_cx, cand_cy, max_iter, fractal_type=0, julia_cx=0.0, ju
     disagree; the escape scalar is then the exact Decimal one)."""
     lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
     seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
-    a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
-    b = None if a[4] else _native_orbit(seeds, lo, max_iter, fractal_type, gen_n, with_mag2=True)
+    a, b = _certify_runs(_first_run(seeds, lo, max_iter, fractal_type, gen_n, prec_bits), seeds, lo, hi,
+                         max_iter, fractal_type, gen_n, prec_bits)
     return _certified_probe(a, b, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
                             gen_n, gen_kr, gen_ki)
 
@@ -289,22 +300,19 @@ def _certified_probe(a, b, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, j
 
 
 class _Runs:
-    """The native runs of one orbit on a pool: the higher-precision one at once, with its
-    certificate; the lower one only if that run is not certified."""
+    """The native runs of one orbit on a pool: the lower-precision one at once, with its
+    certificate; the higher one only if that run is not certified."""
 
     def __init__(self, pool, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits, gen_n,
                  gen_kr, gen_ki):
-        self.lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+        self.lo, self.hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
         self.seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
-        self.args = (max_iter, fractal_type, gen_n)
-        self.first = pool.submit(_first_run, self.seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+        self.args = (max_iter, fractal_type, gen_n, prec_bits)
+        self.first = pool.submit(_first_run, self.seeds, self.lo, max_iter, fractal_type, gen_n, prec_bits)
 
     def result(self):
-        """(first run, second run or None when the first is certified)."""
-        a = self.first.result()
-        if a[4]:
-            return a, None
-        return a, _native_orbit(self.seeds, self.lo, *self.args, True)
+        """(certified run, None), or (higher run, lower run) when neither is certified."""
+        return _certify_runs(self.first.result(), self.seeds, self.lo, self.hi, *self.args)
 
     def cancel(self):
         self.first.cancel()

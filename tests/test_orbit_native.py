@@ -184,25 +184,29 @@ def test_fixed_size_products_at_every_size(fractal_type, gen_n, int_limbs):
 @pytest.mark.parametrize("prec_bits", [256, 700])
 @pytest.mark.parametrize("formula", FORMULAS, ids=lambda f: f"type{f[0]}_n{f[2]}")
 def test_certified_runs_equal_decimal(formula, prec_bits):
-    """ap_reference_orbit_cert: wherever its error bound certifies a run, the float64 orbit,
-    the escape step and |Z|^2 at escape equal the Decimal loop's; and most seeded points
-    (non-chaotic orbits) are certified, so the second, lower-precision run is skipped."""
+    """ap_reference_orbit_cert: wherever its error bound certifies a run (64 fractional
+    bits below or above the Decimal precision), the float64 orbit, the escape step and
+    |Z|^2 at escape equal the Decimal loop's; and most seeded runs (non-chaotic orbits)
+    are certified, so the search needs one run per orbit."""
     ft, (jx, jy), n, kr, ki = formula
     lo, hi = hp.orbit_limbs(prec_bits, hp.orbit_int_limbs(ft, n))
     certified = 0
     pts = _points(prec_bits + 7 * ft + n, 8, ft)
     for cx, cy in pts:
         seeds = hp._Seeds(ft, cx, cy, jx, jy, kr, ki)
-        a = hp._first_run(seeds, hi, 3000, ft, n, prec_bits)
-        if not a[4]:
-            continue
-        certified += 1
-        b = hp.decimal_orbit_py(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
-        assert a[2] == b[2] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
-        if a[2] < 3000:
-            assert hp._smooth_escape(a[2], a[3], 3000, ft, n) == hp.decimal_escape_scalar(
-                cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
-    assert certified >= len(pts) // 2, certified
+        b = None
+        for L in (lo, hi):  # below and above the Decimal precision
+            a = hp._first_run(seeds, L, 3000, ft, n, prec_bits)
+            if not a[4]:
+                continue
+            certified += 1
+            if b is None:
+                b = hp.decimal_orbit_py(cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
+            assert a[2] == b[2] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+            if a[2] < 3000:
+                assert hp._smooth_escape(a[2], a[3], 3000, ft, n) == hp.decimal_escape_scalar(
+                    cx, cy, 3000, ft, jx, jy, prec_bits, n, kr, ki)
+    assert certified >= len(pts), certified
 
 
 def test_certification_refuses_a_run_that_differs_from_decimal():
@@ -210,9 +214,10 @@ def test_certification_refuses_a_run_that_differs_from_decimal():
     Decimal orbit before the escape, and the bound does not certify it."""
     cx, cy, bits = Decimal("-1.7692733407791943"), Decimal("0.01796380726768093"), 174
     lo, hi = hp.orbit_limbs(bits, hp.orbit_int_limbs(1, 3))
-    a = hp._first_run(hp._Seeds(1, cx, cy, 0.0, 0.0, 0.25, 1.0), hi, 6000, 1, 3, bits)
     b = hp.decimal_orbit_py(cx, cy, 6000, 1, 0.0, 0.0, bits)
-    assert not (a[2] == b[2] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]))
-    assert not a[4]
+    for L in (lo, hi):
+        a = hp._first_run(hp._Seeds(1, cx, cy, 0.0, 0.0, 0.25, 1.0), L, 6000, 1, 3, bits)
+        assert not (a[2] == b[2] and np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]))
+        assert not a[4]
     got = hp.compute_single_highprec_orbit(cx, cy, 6000, 1, 0.0, 0.0, bits)
     assert got[2] == b[2] and np.array_equal(got[0], b[0]) and np.array_equal(got[1], b[1])
