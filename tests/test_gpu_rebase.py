@@ -156,6 +156,15 @@ def test_one_pass_rejects_unserved_cases():
     with pytest.raises(NotImplementedError):
         engine.render_frame_ssaa(64, 36, 1000, Decimal("-0.75"), Decimal("0.1"), Decimal("1e-320"), None,
                                  precision_mode="1e-300 (Perturbation)", glitch_mode=ONE_PASS_REBASING)
+    # the FP32 form rebases below 1e-300 at factor 1 only, and never Julia orbits
+    with pytest.raises(NotImplementedError):
+        engine.render_frame_ssaa(64, 36, 1000, Decimal("-0.75"), Decimal("0.1"), Decimal("1e-320"), None,
+                                 ssaa_factor=2, precision_mode="1e-300 (Perturbation)",
+                                 glitch_mode=ONE_PASS_REBASING, delta_form="fp32")
+    with pytest.raises(NotImplementedError):
+        engine.render_frame_ssaa(64, 36, 1000, Decimal("-0.79"), Decimal("0.27"), Decimal("1e-14"), None,
+                                 precision_mode="1e-300 (Perturbation)", fractal_type=2, julia_cx=-0.8,
+                                 julia_cy=0.156, glitch_mode=ONE_PASS_REBASING, delta_form="fp32")
     # the C-ABI refuses the flag outside the FP64-delta tier and for Julia orbits
     import torch
     L = _lib.load()
