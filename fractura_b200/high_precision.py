@@ -171,15 +171,18 @@ def _first_run(seeds, L, max_iter, fractal_type, gen_n, prec_bits):
     return _native_orbit_cert(seeds, L, max_iter, fractal_type, gen_n, _orbit_digits(prec_bits))
 
 
-def _certify_runs(first, seeds, lo, hi, max_iter, fractal_type, gen_n, prec_bits):
-    """(run, None) for the first certified run -- the lower precision's `first`, else one
-    at the higher precision -- or (higher run, lower run) for the two-run comparison when
-    neither bound certifies.  The bound counts the run's own truncations, so the cheaper
-    run certifies whenever its bits suffice."""
-    if first[4]:
-        return first, None
-    a = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
-    return (a, None) if a[4] else (a, first)
+def _run_sequence(seeds, lo, hi, max_iter, fractal_type, gen_n, prec_bits):
+    """Certified runs from the cheaper up: the lower precision, then the higher one.
+    Returns (run, None) for the first certified run, or (higher run, lower run) for the
+    two-run comparison when no bound certifies.  The bound counts each run's own
+    truncations and the rounding of its seeds, so the cheaper run certifies whenever its
+    bits suffice.  (Fewer bits than that do not: the view's depth, which sets the
+    Decimal precision, is also what the probe candidates' orbits resolve.)"""
+    a = _first_run(seeds, lo, max_iter, fractal_type, gen_n, prec_bits)
+    if a[4]:
+        return a, None
+    b = _first_run(seeds, hi, max_iter, fractal_type, gen_n, prec_bits)
+    return (b, None) if b[4] else (b, a)
 
 
 def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_type=0,
@@ -193,8 +196,8 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     (math_core/high_precision.py:706-875).
 
     The orbit runs natively in binary fixed point, first with 64 fractional bits fewer
-    than the reference's Decimal digits carry, then, if needed, with 64 more.  Each
-    run carries a bound on its distance from the Decimal iteration
+    than the reference's Decimal digits carry, then, if needed, with 64 more.  Each run
+    carries a bound on its distance from the Decimal iteration
     (ap_reference_orbit_cert); where the bound proves every float64 value and bailout
     decision equal, that orbit is returned.  When neither run is certified, they are
     compared: when both give the same float64 orbit, the Decimal orbit, whose
@@ -204,8 +207,7 @@ def compute_single_highprec_orbit(cand_cx_dec, cand_cy_dec, max_iter, fractal_ty
     """
     lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
     seeds = _Seeds(fractal_type, cand_cx_dec, cand_cy_dec, julia_cx, julia_cy, gen_kr, gen_ki)
-    a, b = _certify_runs(_first_run(seeds, lo, max_iter, fractal_type, gen_n, prec_bits), seeds, lo, hi,
-                         max_iter, fractal_type, gen_n, prec_bits)
+    a, b = _run_sequence(seeds, lo, hi, max_iter, fractal_type, gen_n, prec_bits)
     return _certified_orbit(a, b, cand_cx_dec, cand_cy_dec, max_iter, fractal_type, julia_cx, julia_cy,
                             prec_bits, gen_n, gen_kr, gen_ki)
 
@@ -278,8 +280,7 @@ def probe_candidate(cand_cx, cand_cy, max_iter, fractal_type=0, julia_cx=0.0, ju
     disagree; the escape scalar is then the exact Decimal one)."""
     lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
     seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
-    a, b = _certify_runs(_first_run(seeds, lo, max_iter, fractal_type, gen_n, prec_bits), seeds, lo, hi,
-                         max_iter, fractal_type, gen_n, prec_bits)
+    a, b = _run_sequence(seeds, lo, hi, max_iter, fractal_type, gen_n, prec_bits)
     return _certified_probe(a, b, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits,
                             gen_n, gen_kr, gen_ki)
 
@@ -300,22 +301,20 @@ def _certified_probe(a, b, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, j
 
 
 class _Runs:
-    """The native runs of one orbit on a pool: the lower-precision one at once, with its
-    certificate; the higher one only if that run is not certified."""
+    """The certified runs of one orbit (_run_sequence) as one task of a pool."""
 
     def __init__(self, pool, cand_cx, cand_cy, max_iter, fractal_type, julia_cx, julia_cy, prec_bits, gen_n,
                  gen_kr, gen_ki):
-        self.lo, self.hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
-        self.seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
-        self.args = (max_iter, fractal_type, gen_n, prec_bits)
-        self.first = pool.submit(_first_run, self.seeds, self.lo, max_iter, fractal_type, gen_n, prec_bits)
+        lo, hi = orbit_limbs(prec_bits, orbit_int_limbs(fractal_type, gen_n))
+        seeds = _Seeds(fractal_type, cand_cx, cand_cy, julia_cx, julia_cy, gen_kr, gen_ki)
+        self.task = pool.submit(_run_sequence, seeds, lo, hi, max_iter, fractal_type, gen_n, prec_bits)
 
     def result(self):
         """(certified run, None), or (higher run, lower run) when neither is certified."""
-        return _certify_runs(self.first.result(), self.seeds, self.lo, self.hi, *self.args)
+        return self.task.result()
 
     def cancel(self):
-        self.first.cancel()
+        self.task.cancel()
 
 
 # Exact Decimal iteration in the reference's operation order: the path for orbits the
