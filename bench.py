@@ -704,6 +704,7 @@ def frame_arm(args, wl, rank, world, local_rank, steps, headline):
     # End to end through render_frame_ssaa with a pinned host RGB buffer, cold orbit search.
     e2e_steps = max(3, steps // 10)
     h_rgb = torch.empty((H, W, 3), dtype=torch.uint8).pin_memory().numpy()
+    render_call(engine, wl, stream, h_rgb_buf=h_rgb)  # warm-up: the host-buffer path's first call
     barrier(world)
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
@@ -1050,9 +1051,8 @@ def adjoint_arm(args, wl, rank, world, local_rank, steps, headline):
     # memory each step, the loss and the gradient go back
     tgt_host = [tgt.cpu().pin_memory() for _, _, tgt in cases]
     e2e_steps = max(3, steps // 10)
-    barrier(world)
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+
+    def e2e_step():
         for (case, th, _), th_host in zip(cases, tgt_host):
             theta = torch.tensor(th, dtype=torch.float64, device="cuda", requires_grad=True)
             tg = th_host.to("cuda", non_blocking=True)
@@ -1061,6 +1061,12 @@ def adjoint_arm(args, wl, rank, world, local_rank, steps, headline):
             loss = torch.where(mask, (s - tg) ** 2, torch.zeros_like(s)).mean()
             loss.backward()
             _ = float(loss.item()), theta.grad.cpu().numpy()
+
+    e2e_step()  # warm-up: the autograd path's first call is not timed
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
     e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     barrier(world)
     e2e = iters * e2e_steps * world / e2e_s / 1e9
