@@ -118,12 +118,13 @@ _PAIR_LOCK = threading.Lock()
 
 def _probe_pool():
     """Threads for the centre orbit and the probe candidates of
-    find_optimal_reference_orbit (one task per native run; the native runs release
-    the GIL)."""
+    find_optimal_reference_orbit (one task per orbit; the native runs release the
+    GIL).  At least one thread per orbit of a search (17): with fewer, the last orbit
+    waits for a whole run instead of sharing the cores."""
     global _PROBE_POOL
     with _PAIR_LOCK:
         if _PROBE_POOL is None:
-            _PROBE_POOL = ThreadPoolExecutor(max_workers=max(2, os.cpu_count() or 4),
+            _PROBE_POOL = ThreadPoolExecutor(max_workers=max(1 + len(PROBE_UV), os.cpu_count() or 4),
                                              thread_name_prefix="probe")
         return _PROBE_POOL
 
