@@ -179,6 +179,94 @@ __global__ void __launch_bounds__(kChunkThreads) cdf_chunk_kernel(const int* __r
     }
 }
 
+// The aligned form (num_bins a multiple of 4 up to kChunkMaxBins, hist and cdf 16-byte
+// aligned): blocks of 1024 threads, 4096 bins each.  Every thread reads its share of all
+// counts as at most 16 independent int4 loads (one round of memory latency, where the
+// form above walks 64 loads a thread) for the total and the sum before the block's
+// chunk, then one int4 of the chunk itself (4 consecutive bins, coalesced); the thread
+// sums are scanned across the block and each thread writes its 4 cdf values as one
+// float4.  The same exact integer prefix and float64 division as cdf_kernel.
+constexpr int kChunk4Threads = 1024;
+
+__global__ void __launch_bounds__(kChunk4Threads) cdf_chunk4_kernel(const int4* __restrict__ h4, int n4,
+                                                                    int num_bins, float4* __restrict__ cdf4) {
+    __shared__ long long red_before[kChunk4Threads / 32], red_total[kChunk4Threads / 32];
+    __shared__ long long scan_s[kChunk4Threads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int s4 = blockIdx.x * kChunk4Threads;  // the chunk's first int4
+    long long before = 0, total = 0;
+#pragma unroll
+    for (int r = 0; r < kChunkMaxBins / 4 / kChunk4Threads; ++r) {
+        const int q = t + r * kChunk4Threads;
+        if (q < n4) {
+            const int4 v = __ldg(h4 + q);
+            const long long s = (long long)v.x + v.y + v.z + v.w;
+            total += s;
+            if (q < s4) before += s;
+        }
+    }
+    before = warp_sum_ll(before);
+    total = warp_sum_ll(total);
+    if (lane == 0) {
+        red_before[warp] = before;
+        red_total[warp] = total;
+    }
+    const int q = s4 + t;
+    const int4 c = q < n4 ? __ldg(h4 + q) : make_int4(0, 0, 0, 0);
+    const long long mine = (long long)c.x + c.y + c.z + c.w;
+    long long v = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) scan_s[warp] = v;
+    __syncthreads();
+    before = total = 0;
+    long long run = v - mine;
+#pragma unroll 8
+    for (int w = 0; w < kChunk4Threads / 32; ++w) {
+        before += red_before[w];
+        total += red_total[w];
+        if (w < warp) run += scan_s[w];
+    }
+    if (q >= n4) return;
+    run += before;
+    const double tot = (double)total;
+    const int b = 4 * q;
+    auto value = [&](long long prefix, int bin) {
+        return tot > 0.0 ? (float)((double)prefix / tot) : (float)((double)bin / (double)(num_bins - 1));
+    };
+    float4 out;
+    run += c.x;
+    out.x = value(run, b);
+    run += c.y;
+    out.y = value(run, b + 1);
+    run += c.z;
+    out.z = value(run, b + 2);
+    run += c.w;
+    out.w = value(run, b + 3);
+    cdf4[q] = out;
+}
+
+// The CDF of a histogram: the aligned chunked form, the chunked form, or one block.
+static int launch_cdf(const int32_t* hist, int num_bins, float* cdf, cudaStream_t st) {
+    if (num_bins <= kChunkMaxBins && (num_bins & 3) == 0 && (reinterpret_cast<uintptr_t>(hist) & 15u) == 0 &&
+        (reinterpret_cast<uintptr_t>(cdf) & 15u) == 0) {
+        const int n4 = num_bins >> 2;
+        cdf_chunk4_kernel<<<(n4 + kChunk4Threads - 1) / kChunk4Threads, kChunk4Threads, 0, st>>>(
+            reinterpret_cast<const int4*>(hist), n4, num_bins, reinterpret_cast<float4*>(cdf));
+        return check_launch("cdf_chunk4_kernel");
+    }
+    if (num_bins <= kChunkMaxBins) {
+        const int blocks = (num_bins + kChunkBins - 1) / kChunkBins;
+        cdf_chunk_kernel<<<blocks, kChunkThreads, 0, st>>>(hist, num_bins, cdf);
+        return check_launch("cdf_chunk_kernel");
+    }
+    cdf_kernel<<<1, kScanThreads, 0, st>>>(hist, num_bins, cdf);
+    return check_launch("cdf_kernel");
+}
+
 // ----------------------------------------------------------------- colour
 // apply_histogram_equalization_kernel (math_core/cuda_kernels.py:2016) and
 // recolor_iter_map_cuda_kernel (math_core/cuda_kernels.py:3201).
@@ -274,13 +362,7 @@ extern "C" int ap_histogram_cdf(const float* iter_map, int32_t width, int32_t he
     ap::histogram_kernel<<<blocks, 256, 0, st>>>(iter_map, n, inv_max, num_bins, hist);
     int rc = ap::check_launch("histogram_kernel");
     if (rc != AP_OK) return rc;
-    if (num_bins <= ap::kChunkMaxBins) {
-        const int blocks = (num_bins + ap::kChunkBins - 1) / ap::kChunkBins;
-        ap::cdf_chunk_kernel<<<blocks, ap::kChunkThreads, 0, st>>>(hist, num_bins, cdf);
-        return ap::check_launch("cdf_chunk_kernel");
-    }
-    ap::cdf_kernel<<<1, ap::kScanThreads, 0, st>>>(hist, num_bins, cdf);
-    return ap::check_launch("cdf_kernel");
+    return ap::launch_cdf(hist, num_bins, cdf, st);
 }
 
 extern "C" int ap_histogram(const float* iter_map, int32_t width, int32_t height, int32_t max_iter,
@@ -309,14 +391,7 @@ extern "C" int ap_cdf_from_histogram(const int32_t* hist, int32_t num_bins, floa
         ap::set_error("ap_cdf_from_histogram: bad arguments");
         return AP_E_INVALID;
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (num_bins <= ap::kChunkMaxBins) {
-        const int blocks = (num_bins + ap::kChunkBins - 1) / ap::kChunkBins;
-        ap::cdf_chunk_kernel<<<blocks, ap::kChunkThreads, 0, st>>>(hist, num_bins, cdf);
-        return ap::check_launch("cdf_chunk_kernel");
-    }
-    ap::cdf_kernel<<<1, ap::kScanThreads, 0, st>>>(hist, num_bins, cdf);
-    return ap::check_launch("cdf_kernel");
+    return ap::launch_cdf(hist, num_bins, cdf, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int ap_colour(const ApFrameParams* p, const ApFrameBuffers* b, void* stream) {
