@@ -33,19 +33,29 @@ __global__ void __launch_bounds__(256) edge_kernel(const float* __restrict__ it,
 
 // -------------------------------------------------------------- histogram
 // math_core/cuda_kernels.py:1999-2013: bin = int(s / max(1, max_iter) * (bins - 1)).
+// Neighbouring pixels mostly fall into the same bins, so the lanes of a warp that count
+// into one bin add once (the lowest of them, by the number of lanes): the same counts
+// with far fewer atomics on the hot bins.  Every lane of a warp runs the same iterations
+// (the loop steps over warp-sized groups of pixels), as the full-warp match requires.
 __global__ void __launch_bounds__(256) histogram_kernel(const float* __restrict__ it, size_t n,
                                                         double inv_max, int num_bins,
                                                         int* __restrict__ hist) {
-    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n;
-         q += (size_t)gridDim.x * blockDim.x) {
-        const float s = it[q];
-        if (s >= 0.0f) {
-            const double pos = ((double)s * inv_max) * (double)(num_bins - 1);
-            int bin = (int)pos;
-            if (bin >= num_bins) bin = num_bins - 1;
-            else if (bin < 0) bin = 0;
-            atomicAdd(hist + bin, 1);
+    const int lane = threadIdx.x & 31;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t base = blockIdx.x * (size_t)blockDim.x + (threadIdx.x & ~31u); base < n; base += stride) {
+        const size_t q = base + lane;
+        int bin = -1;
+        if (q < n) {
+            const float s = it[q];
+            if (s >= 0.0f) {
+                const double pos = ((double)s * inv_max) * (double)(num_bins - 1);
+                bin = (int)pos;
+                if (bin >= num_bins) bin = num_bins - 1;
+                else if (bin < 0) bin = 0;
+            }
         }
+        const unsigned peers = __match_any_sync(0xffffffffu, bin);
+        if (bin >= 0 && lane == __ffs(peers) - 1) atomicAdd(hist + bin, __popc(peers));
     }
 }
 
